@@ -1,0 +1,270 @@
+/*
+ * vapor_b200 — C ABI of the B200-native MAC 3D smoke step.
+ *
+ * This is the drop-in boundary for Vapor's MAC 3D hot path. It replaces the
+ * OpenGL compute coordinator and the two stage plugins of the reference:
+ *
+ *   reference interface (taehwann/vapor)                      replaced by
+ *   ------------------------------------------------------    ---------------------------
+ *   GpuMacSimulation3D ctor/advance/resetState/setBoxSize/     vapor_mac3d_*      (resident)
+ *     parameters/lastProjection/upload/download/byte counters
+ *     src/solvers/mac3d/gpu/GpuMacSimulation3D.hpp:9-46
+ *   MacGridFluidSolver3D::diagnostics                          vapor_mac3d_diagnostics
+ *     src/solvers/mac3d/MacGridFluidSolver3D.cpp:332-334
+ *   Projection3D::project / reset                              vapor_stage_project
+ *     src/solvers/mac3d/Projection3D.hpp:6-11                  vapor_stage_reset
+ *   Advection3D::advectScalar / advectFace                     vapor_stage_advect_scalar
+ *     src/solvers/mac3d/Advection3D.hpp:6-14                   vapor_stage_advect_face
+ *
+ * Conventions
+ *   - Every entry point returns a vapor_status; VAPOR_OK is 0. No C++
+ *     exception crosses this boundary. vapor_last_error() returns the message
+ *     of the last failure on the calling thread.
+ *   - The reference throws std::invalid_argument for contract violations,
+ *     std::length_error for index overflow and std::runtime_error for backend
+ *     failures; these map to VAPOR_INVALID_ARGUMENT, VAPOR_LENGTH_ERROR and
+ *     VAPOR_RUNTIME_ERROR.
+ *   - Fields use the reference's MAC layout (MacGridDomain3D.hpp:22-31), FP32,
+ *     x fastest: density n^3 at x+n(y+nz); u (n+1)n^2 at x+(n+1)(y+nz);
+ *     v n(n+1)n at x+n(y+(n+1)z); w n^2(n+1) at x+n(y+nz), z in [0,n].
+ *   - Axis convention is the reference's: z is up (buoyancy acts on w).
+ *   - A handle owns one CUDA stream and all of its device buffers. A handle is
+ *     not thread-safe; distinct handles may be used concurrently.
+ *   - Host pointers passed to upload/download/stage calls may be pageable or
+ *     pinned; pinned memory makes the copies asynchronous-capable and faster.
+ */
+#ifndef VAPOR_B200_H
+#define VAPOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VAPOR_B200_ABI_VERSION 1
+
+typedef enum vapor_status {
+    VAPOR_OK = 0,
+    VAPOR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+    VAPOR_LENGTH_ERROR = 2,     /* std::length_error (index range overflow) */
+    VAPOR_RUNTIME_ERROR = 3,    /* std::runtime_error (CUDA failure, no device) */
+    VAPOR_NON_FINITE = 4,       /* non-finite divergence or velocity found on the device;
+                                   the reference throws std::invalid_argument here */
+    VAPOR_OUT_OF_MEMORY = 5
+} vapor_status;
+
+/* MacAlgorithm (src/common/MacAlgorithm.hpp:3-9). */
+typedef enum vapor_mac_algorithm {
+    VAPOR_SIMPLE_SEMI_LAGRANGIAN = 0,
+    VAPOR_SIMPLE_MACCORMACK = 1,
+    VAPOR_REFLECTION_SEMI_LAGRANGIAN = 2,
+    VAPOR_REFLECTION_MACCORMACK = 3
+} vapor_mac_algorithm;
+
+/* AdvectionMethod (src/common/MacAlgorithm.hpp:10). */
+typedef enum vapor_advection_method {
+    VAPOR_SEMI_LAGRANGIAN = 0,
+    VAPOR_MACCORMACK = 1
+} vapor_advection_method;
+
+/* FaceAxis (src/solvers/mac3d/AdvectionContext.hpp:9). */
+typedef enum vapor_face_axis { VAPOR_FACE_X = 0, VAPOR_FACE_Y = 1, VAPOR_FACE_Z = 2 } vapor_face_axis;
+
+/* Pressure solver kinds. RED_BLACK_SOR is the reference's SOR (SOR.cpp:22-64)
+ * with its red-black colour order, so iterates match it exactly. The other
+ * kinds are extensions that always finish with the same residual test. */
+typedef enum vapor_solver_kind {
+    VAPOR_SOLVER_RED_BLACK_SOR = 0,
+    VAPOR_SOLVER_MIXED_REFINEMENT = 1 /* FP32 SOR inner sweeps, FP64 residual and correction */
+} vapor_solver_kind;
+
+/* LinearSolveOptions / LinearSolveResult (src/common/LinearSolveOptions.hpp:4-24). */
+typedef struct vapor_linear_solve_options {
+    int32_t max_iterations;          /* default 200 */
+    int32_t residual_check_interval; /* default 8 */
+    double absolute_tolerance;       /* default 1e-6 */
+    double relative_tolerance;       /* default 1e-5 */
+    int32_t fixed_iterations;        /* default 0 (stop at tolerance) */
+    int32_t reserved0;
+} vapor_linear_solve_options;
+
+typedef struct vapor_linear_solve_result {
+    int32_t iterations;
+    int32_t converged;
+    double initial_residual; /* FP64 infinity norm of b - A x0 */
+    double final_residual;   /* FP64 infinity norm of b - A x after the mean gauge */
+} vapor_linear_solve_result;
+
+/* ProjectionOptions / ProjectionResult (src/common/ProjectionOptions.hpp:5-18). */
+typedef struct vapor_projection_options {
+    float dt;         /* default 1/60 */
+    float relaxation; /* SOR omega, default 1.95 */
+    vapor_linear_solve_options linear_solve;
+} vapor_projection_options;
+
+typedef struct vapor_projection_result {
+    vapor_linear_solve_result linear_solve;
+    int32_t residual_available; /* always 1: the residual is measured in FP64 */
+    float divergence_before;    /* max |div u| before projection */
+    float divergence_after;     /* max |div u| after projection */
+    int32_t reserved0;
+    double removed_rhs_mean;
+} vapor_projection_result;
+
+/* FluidDiagnostics (src/common/FluidDiagnostics.hpp:3-7). */
+typedef struct vapor_fluid_diagnostics {
+    float kinetic_energy;
+    float max_velocity;
+    float max_divergence;
+} vapor_fluid_diagnostics;
+
+/*
+ * MacGridParameters3D (src/solvers/mac3d/MacGridFluidSolver3D.hpp:14-36), field
+ * for field, followed by extensions the reference does not have. With the
+ * extensions at their defaults the step is the reference's step.
+ */
+typedef struct vapor_mac3d_params {
+    float emitter_radius;            /* .035 (fraction of box) */
+    float emitter_center_x;          /* .5 */
+    float emitter_center_y;          /* .5 */
+    float emitter_center_z;          /* .1 (z is up) */
+    float emitter_kick_multiplier;   /* 1 */
+    float emitter_kick_base;         /* .8 */
+    float emitter_kick_scale;        /* .8 */
+    float stir_strength;             /* .5 */
+    uint32_t random_seed;            /* 0x9E3779B9, applied at construction and reset */
+    float sor_omega;                 /* 1.95 */
+    float buoyancy_split;            /* .5 */
+    float cfl_mc;                    /* 3 */
+    int32_t mac_cormack_smoke;       /* 1 */
+    int32_t mac_cormack_vel;         /* 1 */
+    float smoke_decay;               /* .06 */
+    int32_t reflection;              /* 1 */
+    float buoyancy;                  /* 2.5 */
+    float source_strength;           /* 1 */
+    int32_t project_iterations;      /* 64 */
+
+    /* ---- extensions (no reference counterpart) ---- */
+    /* 0: projections run project_iterations fixed sweeps (reference semantics,
+     *    MacGridFluidSolver3D.cpp:131-138). 1: projections use `solve`. */
+    int32_t use_solve_options;
+    vapor_linear_solve_options solve;
+    int32_t solver_kind;             /* vapor_solver_kind */
+    /* 0: reference emitter (density = 1 inside the sphere, kick, stir).
+     * 1: smooth profile density = max(density, min(1, 3 s exp(-3.5 (d/r)^2))). */
+    int32_t emitter_profile;
+    int32_t emitter_count;           /* 1 or 2 */
+    float emitter2_center_x, emitter2_center_y, emitter2_center_z;
+} vapor_mac3d_params;
+
+/* Error message of the last failing call on this thread ("" if none). */
+const char *vapor_last_error(void);
+/* VAPOR_B200_ABI_VERSION of the loaded library. */
+int32_t vapor_abi_version(void);
+
+/* Defaults of MacGridParameters3D() and of MacGridParameters3D(MacAlgorithm)
+ * (MacGridFluidSolver3D.cpp:11-26). */
+vapor_status vapor_mac3d_default_params(vapor_mac3d_params *out);
+vapor_status vapor_mac3d_algorithm_params(int32_t algorithm, vapor_mac3d_params *out);
+vapor_status vapor_default_projection_options(vapor_projection_options *out);
+
+/* ------------------------------------------------------------------------ */
+/* Resident coordinator: GpuMacSimulation3D (gpu/GpuMacSimulation3D.hpp:9-46) */
+/* ------------------------------------------------------------------------ */
+typedef struct vapor_mac3d vapor_mac3d;
+
+/* GpuMacSimulation3D(int, float, MacGridParameters3D) (GpuMacSimulation3D.cpp:49-63).
+ * Validates the grid like MacGridDomain3D (MacGridDomain3D.cpp:7-22), allocates
+ * every buffer on the current device and resets the state. */
+vapor_status vapor_mac3d_create(int32_t n, float box, const vapor_mac3d_params *params,
+                                vapor_mac3d **out);
+vapor_status vapor_mac3d_destroy(vapor_mac3d *sim);
+/* resetState (GpuMacSimulation3D.cpp:89-98): zero all fields, reseed the RNG. */
+vapor_status vapor_mac3d_reset(vapor_mac3d *sim);
+/* setBoxSize (GpuMacSimulation3D.cpp:99-106): reset when the size changes. */
+vapor_status vapor_mac3d_set_box(vapor_mac3d *sim, float box);
+vapor_status vapor_mac3d_get_params(const vapor_mac3d *sim, vapor_mac3d_params *out);
+/* parameters() returns a mutable struct read on every advance. */
+vapor_status vapor_mac3d_set_params(vapor_mac3d *sim, const vapor_mac3d_params *params);
+/* advance(dt) (GpuMacSimulation3D.cpp:224-264): one step, enqueued on the
+ * handle's stream; it does not wait for the device. Parameter validation
+ * happens here (VAPOR_INVALID_ARGUMENT). Device-side failures (non-finite
+ * divergence) surface from vapor_mac3d_synchronize / last_projection. */
+vapor_status vapor_mac3d_advance(vapor_mac3d *sim, float dt);
+/* Advance `steps` times with the same dt (one graph launch per step). */
+vapor_status vapor_mac3d_advance_n(vapor_mac3d *sim, float dt, int32_t steps);
+/* Wait for the handle's stream; report a deferred device-side error. */
+vapor_status vapor_mac3d_synchronize(vapor_mac3d *sim);
+/* lastProjection(): result of the last projection of the last step (waits). */
+vapor_status vapor_mac3d_last_projection(vapor_mac3d *sim, vapor_projection_result *out);
+/* Sum of SOR iterations over all projections since reset (waits). */
+vapor_status vapor_mac3d_total_iterations(vapor_mac3d *sim, int64_t *out);
+/* diagnostics(): kinetic energy, max |velocity|, max |divergence| (waits). */
+vapor_status vapor_mac3d_diagnostics(vapor_mac3d *sim, vapor_fluid_diagnostics *out);
+/* upload/download (GpuMacSimulation3D.cpp:110-141): host snapshot <-> device.
+ * Array sizes are implied by n (see layout above). */
+vapor_status vapor_mac3d_upload(vapor_mac3d *sim, const float *density, const float *u,
+                                const float *v, const float *w);
+vapor_status vapor_mac3d_download(vapor_mac3d *sim, float *density, float *u, float *v,
+                                  float *w);
+/* uploadedBytes/downloadedBytes (GpuMacSimulation3D.hpp:25-26). */
+vapor_status vapor_mac3d_byte_counters(const vapor_mac3d *sim, uint64_t *uploaded,
+                                       uint64_t *downloaded);
+/* renderData() analogue: borrowed device pointers of the resident fields.
+ * They stay valid until the next advance/reset/destroy on this handle. */
+vapor_status vapor_mac3d_device_fields(vapor_mac3d *sim, float **density, float **u, float **v,
+                                       float **w);
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or record CUDA events against the step. */
+vapor_status vapor_mac3d_stream(vapor_mac3d *sim, void **stream);
+vapor_status vapor_mac3d_resolution(const vapor_mac3d *sim, int32_t *n, float *box);
+
+/* ------------------------------------------------------------------------ */
+/* Staged stage plugins: Projection3D / Advection3D with host spans           */
+/* (the GpuPressureSolver/GpuAdvection pattern, GpuMacBackend.cpp:91-109)     */
+/* ------------------------------------------------------------------------ */
+typedef struct vapor_stage vapor_stage;
+
+/* One workspace per concurrent operation (AdvectionContext.hpp:18-19). */
+vapor_status vapor_stage_create(int32_t n, float box, vapor_stage **out);
+vapor_status vapor_stage_destroy(vapor_stage *stage);
+/* Projection3D::reset: clear the pressure and divergence workspace. */
+vapor_status vapor_stage_reset(vapor_stage *stage);
+/* Projection3D::project (CpuPressureSolver3D.cpp:25-60) on host velocity
+ * spans, in place. diagonal_floor is the SOR relaxation floor (6 reproduces
+ * MacGridFluidSolver3D's solver, MacGridFluidSolver3D.hpp:118). pressure_out
+ * (may be NULL) receives the zero-mean pressure, n^3 floats. */
+vapor_status vapor_stage_project(vapor_stage *stage, float *u, float *v, float *w,
+                                 const vapor_projection_options *options, float diagonal_floor,
+                                 vapor_projection_result *result, float *pressure_out);
+/* Advection3D::advectFace (CpuAdvectionKernels.cpp:82-269): source and output
+ * are face arrays of `axis`; flow_u/v/w are the tracer velocity. The output
+ * must not alias the source or the flow (AdvectionContext.cpp:53-67). */
+vapor_status vapor_stage_advect_face(vapor_stage *stage, int32_t axis, float dt, float cfl_limit,
+                                     int32_t method, const float *source, const float *flow_u,
+                                     const float *flow_v, const float *flow_w, float *output);
+/* Advection3D::advectScalar (CpuAdvectionKernels.cpp:18-80), in place. */
+vapor_status vapor_stage_advect_scalar(vapor_stage *stage, float dt, float cfl_limit,
+                                       int32_t method, float *field, const float *flow_u,
+                                       const float *flow_v, const float *flow_w);
+/* Device-pointer variants: every pointer is device memory of the right size. */
+vapor_status vapor_stage_project_device(vapor_stage *stage, float *u, float *v, float *w,
+                                        const vapor_projection_options *options,
+                                        float diagonal_floor, vapor_projection_result *result,
+                                        float *pressure_out);
+vapor_status vapor_stage_advect_face_device(vapor_stage *stage, int32_t axis, float dt,
+                                            float cfl_limit, int32_t method, const float *source,
+                                            const float *flow_u, const float *flow_v,
+                                            const float *flow_w, float *output);
+vapor_status vapor_stage_advect_scalar_device(vapor_stage *stage, float dt, float cfl_limit,
+                                              int32_t method, float *field, const float *flow_u,
+                                              const float *flow_v, const float *flow_w);
+vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VAPOR_B200_H */

@@ -1,0 +1,299 @@
+"""Test-side loaders for the oracle libraries (checkers, never the product).
+
+  Oracle     oracle/_build/libvapor_oracle.so   CPU restatement (float and double)
+  Reference  oracle/_ref/libvapor_ref.so        the reference's own CPU sources
+
+Both are built by `make -C oracle` (see oracle/Makefile); __graft_entry__.build()
+runs it. Arrays are numpy, in the reference's MAC layout (z, y, x).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from vapor_b200.abi import (FluidDiagnostics, LinearSolveOptions, LinearSolveResult, MacParams,
+                            ProjectionResult, field_shapes)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libvapor_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libvapor_ref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+
+def _setup_oracle(lib):
+    for suf, T, P in (("f32", C.c_float, _f32p), ("f64", C.c_double, _f64p)):
+        def f(name, res, *args):
+            fn = getattr(lib, f"{name}_{suf}")
+            fn.restype = res
+            fn.argtypes = list(args)
+        f("vo_sample", C.c_double, C.c_int, T, C.c_int, P, T, T, T)
+        f("vo_advect", None, C.c_int, T, C.c_int, T, T, C.c_int, P, P, P, P, P)
+        f("vo_divergence", None, C.c_int, T, P, P, P, P)
+        f("vo_max_divergence", C.c_double, C.c_int, T, P, P, P)
+        f("vo_enforce_walls", None, C.c_int, P, P, P)
+        f("vo_apply_gradient", None, C.c_int, T, P, T, P, P, P)
+        f("vo_residual", C.c_double, C.c_int, P, P)
+        f("vo_sor_solve", C.c_int, C.c_int, T, T, P, P, C.POINTER(LinearSolveOptions),
+          C.POINTER(LinearSolveResult))
+        f("vo_sor_iteration", None, C.c_int, T, T, P, P)
+        f("vo_project", C.c_int, C.c_int, T, P, P, P, T, T, T, C.POINTER(LinearSolveOptions), C.c_int,
+          C.POINTER(ProjectionResult), P)
+        f("vo_sim_create", _vp, C.c_int, T)
+        f("vo_sim_destroy", None, _vp)
+        f("vo_sim_set_params", None, _vp, C.POINTER(MacParams))
+        f("vo_sim_get_params", None, _vp, C.POINTER(MacParams))
+        f("vo_sim_reset", None, _vp)
+        f("vo_sim_advance", C.c_int, _vp, T)
+        f("vo_sim_get_fields", None, _vp, P, P, P, P)
+        f("vo_sim_set_fields", None, _vp, P, P, P, P)
+        f("vo_sim_rng", C.c_uint32, _vp)
+        f("vo_sim_set_rng", None, _vp, C.c_uint32)
+        f("vo_sim_diagnostics", None, _vp, C.POINTER(FluidDiagnostics))
+        f("vo_sim_last_projection", None, _vp, C.POINTER(ProjectionResult))
+        f("vo_sim_total_iterations", C.c_longlong, _vp)
+    lib.vapor_mac3d_default_params.argtypes = [C.POINTER(MacParams)]
+    lib.vapor_mac3d_algorithm_params.argtypes = [C.c_int32, C.POINTER(MacParams)]
+    return lib
+
+
+def _setup_ref(lib):
+    def f(name, res, *args):
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = list(args)
+    P = _f32p
+    f("ref_sim_create", C.c_int, C.c_int, C.c_float, C.POINTER(_vp))
+    f("ref_sim_create_algorithm", C.c_int, C.c_int, C.POINTER(_vp))
+    f("ref_sim_create_from_fields", C.c_int, C.c_int, C.c_float, P, P, P, P, C.POINTER(_vp))
+    f("ref_sim_destroy", None, _vp)
+    f("ref_sim_set_params", C.c_int, _vp, C.POINTER(MacParams))
+    f("ref_sim_get_params", None, _vp, C.POINTER(MacParams))
+    f("ref_sim_reset", C.c_int, _vp)
+    f("ref_sim_set_box", C.c_int, _vp, C.c_float)
+    f("ref_sim_advance", C.c_int, _vp, C.c_float)
+    f("ref_sim_get_fields", None, _vp, P, P, P, P)
+    f("ref_sim_diagnostics", C.c_int, _vp, C.POINTER(FluidDiagnostics))
+    f("ref_sim_last_projection", None, _vp, C.POINTER(ProjectionResult))
+    f("ref_sim_resolution", C.c_int, _vp)
+    f("ref_sim_box", C.c_float, _vp)
+    f("ref_advect", C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, C.c_int, P, P, P, P, P)
+    f("ref_project", C.c_int, C.c_int, C.c_float, P, P, P, C.c_float, C.c_float, C.c_float,
+      C.POINTER(LinearSolveOptions), C.POINTER(ProjectionResult), P)
+    f("ref_sor_solve", C.c_int, C.c_int, C.c_float, C.c_float, P, P, P, P, P, P,
+      C.POINTER(LinearSolveOptions), C.POINTER(LinearSolveResult))
+    f("ref_sample", C.c_double, C.c_int, C.c_float, C.c_int, P, C.c_float, C.c_float, C.c_float)
+    f("ref_max_divergence", C.c_int, C.c_int, C.c_float, P, P, P, C.POINTER(C.c_float))
+    f("ref_divergence", C.c_int, C.c_int, C.c_float, P, P, P, P)
+    lib.vapor_mac3d_default_params.argtypes = [C.POINTER(MacParams)]
+    return lib
+
+
+_oracle = None
+_ref = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle)")
+        _oracle = _setup_oracle(C.CDLL(ORACLE_SO))
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise RuntimeError(f"reference library missing: {REF_SO}")
+        _ref = _setup_ref(C.CDLL(REF_SO))
+    return _ref
+
+
+def default_params():
+    p = MacParams()
+    oracle().vapor_mac3d_default_params(C.byref(p))
+    return p
+
+
+def algorithm_params(alg):
+    p = MacParams()
+    assert oracle().vapor_mac3d_algorithm_params(alg, C.byref(p)) == 0
+    return p
+
+
+def zeros_fields(n, dtype=np.float32):
+    return [np.zeros(s, dtype=dtype) for s in field_shapes(n)]
+
+
+class OracleSim:
+    """The oracle coordinator (float: reference-exact FP32; double: FP64 oracle)."""
+
+    def __init__(self, n, box=4.5, dtype=np.float32):
+        self.n, self.box, self.dtype = n, box, np.dtype(dtype)
+        self.suf = "f32" if self.dtype == np.float32 else "f64"
+        self.lib = oracle()
+        self.h = self._fn("vo_sim_create")(n, box)
+
+    def _fn(self, name):
+        return getattr(self.lib, f"{name}_{self.suf}")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._fn("vo_sim_destroy")(self.h)
+            self.h = None
+
+    @property
+    def params(self):
+        p = MacParams()
+        self._fn("vo_sim_get_params")(self.h, C.byref(p))
+        return p
+
+    @params.setter
+    def params(self, p):
+        self._fn("vo_sim_set_params")(self.h, C.byref(p))
+
+    def reset(self):
+        self._fn("vo_sim_reset")(self.h)
+
+    def advance(self, dt):
+        return self._fn("vo_sim_advance")(self.h, dt)
+
+    def fields(self):
+        out = zeros_fields(self.n, self.dtype)
+        self._fn("vo_sim_get_fields")(self.h, *out)
+        return out
+
+    def set_fields(self, d, u, v, w):
+        arrs = [np.ascontiguousarray(a, dtype=self.dtype) for a in (d, u, v, w)]
+        self._fn("vo_sim_set_fields")(self.h, *arrs)
+
+    @property
+    def rng(self):
+        return self._fn("vo_sim_rng")(self.h)
+
+    @rng.setter
+    def rng(self, s):
+        self._fn("vo_sim_set_rng")(self.h, s)
+
+    def diagnostics(self):
+        d = FluidDiagnostics()
+        self._fn("vo_sim_diagnostics")(self.h, C.byref(d))
+        return d
+
+    def last_projection(self):
+        r = ProjectionResult()
+        self._fn("vo_sim_last_projection")(self.h, C.byref(r))
+        return r
+
+    def total_iterations(self):
+        return self._fn("vo_sim_total_iterations")(self.h)
+
+
+class RefSim:
+    """The reference's MacGridFluidSolver3D, compiled from its own sources."""
+
+    def __init__(self, n=None, box=4.5, algorithm=None, fields=None):
+        self.lib = ref()
+        h = _vp()
+        if algorithm is not None:
+            st = self.lib.ref_sim_create_algorithm(algorithm, C.byref(h))
+        elif fields is not None:
+            arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in fields]
+            st = self.lib.ref_sim_create_from_fields(n, box, *arrs, C.byref(h))
+        else:
+            st = self.lib.ref_sim_create(n, box, C.byref(h))
+        if st != 0:
+            raise ValueError(f"reference construction failed with status {st}")
+        self.h = h
+        self.n = self.lib.ref_sim_resolution(h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_sim_destroy(self.h)
+            self.h = None
+
+    @property
+    def params(self):
+        p = MacParams()
+        self.lib.ref_sim_get_params(self.h, C.byref(p))
+        return p
+
+    @params.setter
+    def params(self, p):
+        st = self.lib.ref_sim_set_params(self.h, C.byref(p))
+        if st != 0:
+            raise ValueError(f"reference rejected parameters ({st})")
+
+    def reset(self):
+        return self.lib.ref_sim_reset(self.h)
+
+    def set_box(self, b):
+        return self.lib.ref_sim_set_box(self.h, b)
+
+    def advance(self, dt):
+        return self.lib.ref_sim_advance(self.h, dt)
+
+    def fields(self):
+        out = zeros_fields(self.n)
+        self.lib.ref_sim_get_fields(self.h, *out)
+        return out
+
+    def diagnostics(self):
+        d = FluidDiagnostics()
+        st = self.lib.ref_sim_diagnostics(self.h, C.byref(d))
+        return d if st == 0 else None
+
+    def last_projection(self):
+        r = ProjectionResult()
+        self.lib.ref_sim_last_projection(self.h, C.byref(r))
+        return r
+
+
+def ref_advect(n, box, loc, dt, cfl, mc, src, u, v, w):
+    out = np.zeros_like(src, dtype=np.float32)
+    st = ref().ref_advect(n, box, loc, dt, cfl, int(mc), *[np.ascontiguousarray(a, np.float32) for a in (src, u, v, w)], out)
+    if st != 0:
+        raise ValueError(st)
+    return out
+
+
+def oracle_advect(n, box, loc, dt, cfl, mc, src, u, v, w, dtype=np.float32):
+    suf = "f32" if np.dtype(dtype) == np.float32 else "f64"
+    out = np.zeros(src.shape, dtype=dtype)
+    getattr(oracle(), f"vo_advect_{suf}")(n, box, loc, dt, cfl, int(mc),
+                                          *[np.ascontiguousarray(a, dtype) for a in (src, u, v, w)], out)
+    return out
+
+
+def ref_project(n, box, u, v, w, dt, omega, floor, opts):
+    u, v, w = [np.array(a, dtype=np.float32, copy=True) for a in (u, v, w)]
+    p = np.zeros((n, n, n), np.float32)
+    r = ProjectionResult()
+    st = ref().ref_project(n, box, u, v, w, dt, omega, floor, C.byref(opts), C.byref(r), p)
+    return st, r, u, v, w, p
+
+
+def oracle_project(n, box, u, v, w, dt, omega, floor, opts, solver_kind=0, dtype=np.float32):
+    suf = "f32" if np.dtype(dtype) == np.float32 else "f64"
+    u, v, w = [np.array(a, dtype=dtype, copy=True) for a in (u, v, w)]
+    p = np.zeros((n, n, n), dtype)
+    r = ProjectionResult()
+    st = getattr(oracle(), f"vo_project_{suf}")(n, box, u, v, w, dt, omega, floor, C.byref(opts), solver_kind,
+                                               C.byref(r), p)
+    return st, r, u, v, w, p
+
+
+def random_fields(n, seed, scale=1.0, density=True):
+    """Seeded random MAC state (density in [0,1), velocities ~ N(0, scale))."""
+    rng = np.random.default_rng(seed)
+    sd, su, sv, sw = field_shapes(n)
+    d = rng.random(sd, dtype=np.float32) if density else np.zeros(sd, np.float32)
+    return [d] + [(rng.standard_normal(s) * scale).astype(np.float32) for s in (su, sv, sw)]

@@ -1,0 +1,332 @@
+"""Pins the CPU oracle before anything is compared against it.
+
+1. The float oracle reproduces the reference's golden diagnostics
+   (tests/SimulationTests.cpp:17-34) at the reference's tolerance (2e-5 rel).
+2. The float oracle is bit-identical to the reference's own CPU sources
+   (oracle/_ref) on seeded inputs: sampling, advection, projection, full steps.
+3. The reference's known-answer tests (AdvectionTests.cpp, NumericsTests.cpp)
+   hold for the oracle.
+4. The FP64 oracle agrees with the FP32 oracle to FP32 accuracy.
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle_lib import (OracleSim, RefSim, algorithm_params, default_params, oracle, oracle_advect,
+                        oracle_project, random_fields, ref, ref_advect, ref_available, ref_project)
+from vapor_b200.abi import LinearSolveOptions, field_shapes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+needs_ref = pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def load_baselines():
+    with open(os.path.join(GOLDEN, "simulation_baselines.json")) as f:
+        return json.load(f)
+
+
+def baseline_params(case):
+    p = default_params()
+    p.stir_strength, p.emitter_radius, p.emitter_center_z = 0.0, 0.18, 0.3
+    p.mac_cormack_smoke = int(case["flags"] & 1 != 0)
+    p.mac_cormack_vel = int(case["flags"] & 2 != 0)
+    p.reflection, p.project_iterations = case["reflect"], 16
+    return p
+
+
+def near(actual, expected, name):
+    tol = 2e-5 * max(1.0, abs(expected))
+    assert np.isfinite(actual) and abs(actual - expected) <= tol, f"{name}: {actual} vs {expected}"
+
+
+@pytest.mark.parametrize("case", load_baselines()["cases"],
+                         ids=lambda c: f"n{c['n']}-r{c['reflect']}-f{c['flags']}")
+def test_oracle_reproduces_reference_baselines(case):
+    sim = OracleSim(case["n"])
+    sim.params = baseline_params(case)
+    for _ in range(6):
+        assert sim.advance(1.0 / 60.0) == 0
+    d = sim.fields()[0].ravel().astype(np.float64)
+    weights = 1 + (np.arange(d.size) % 31)
+    diag = sim.diagnostics()
+    near(diag.kinetic_energy, case["energy"], "kinetic energy")
+    near(diag.max_velocity, case["max_velocity"], "max velocity")
+    near(diag.max_divergence, case["divergence"], "divergence")
+    near(d.sum(), case["density_sum"], "density sum")
+    near((d * weights).sum(), case["weighted_density"], "weighted density")
+
+
+@needs_ref
+@pytest.mark.parametrize("n", [1, 2, 4, 7])
+@pytest.mark.parametrize("loc", [0, 1, 2, 3])
+def test_sampling_bit_identical(n, loc):
+    box = 3.7
+    rng = np.random.default_rng(10 * n + loc)
+    f = rng.standard_normal(n * n * (n + (loc > 0))).astype(np.float32)
+    for _ in range(64):
+        x, y, z = (rng.random(3) * 1.6 - 0.3) * box
+        a = oracle().vo_sample_f32(n, box, loc, f, x, y, z)
+        b = ref().ref_sample(n, box, loc, f, x, y, z)
+        assert np.float32(a).view(np.uint32) == np.float32(b).view(np.uint32)
+
+
+@needs_ref
+@pytest.mark.parametrize("n", [1, 3, 6, 11])
+@pytest.mark.parametrize("mc", [0, 1])
+@pytest.mark.parametrize("dt,cfl", [(0.1, 3.0), (2.0, 3.0), (0.1, 0.001), (0.6, 1.5)])
+def test_advection_bit_identical(n, mc, dt, cfl):
+    box = 4.0
+    d, u, v, w = random_fields(n, seed=n * 7 + mc, scale=0.8)
+    for loc, src in enumerate((d, u, v, w)):
+        a = oracle_advect(n, box, loc, dt, cfl, mc, src, u, v, w)
+        b = ref_advect(n, box, loc, dt, cfl, mc, src, u, v, w)
+        assert bits_equal(a, b), f"loc {loc}"
+
+
+@needs_ref
+@pytest.mark.parametrize("n", [1, 2, 5, 10])
+@pytest.mark.parametrize("floor", [0.0, 6.0])
+@pytest.mark.parametrize("fixed,iters", [(1, 16), (0, 400)])
+def test_projection_bit_identical(n, floor, fixed, iters):
+    d, u, v, w = random_fields(n, seed=100 + n, scale=1.0)
+    opts = LinearSolveOptions.defaults(max_iterations=iters, fixed_iterations=fixed,
+                                       relative_tolerance=1e-6, absolute_tolerance=1e-7)
+    sa, ra, ua, va, wa, pa = oracle_project(n, 4.5, u, v, w, 1 / 60, 1.7, floor, opts)
+    sb, rb, ub, vb, wb, pb = ref_project(n, 4.5, u, v, w, 1 / 60, 1.7, floor, opts)
+    assert sa == sb == 0
+    for x, y in ((ua, ub), (va, vb), (wa, wb), (pa, pb)):
+        assert bits_equal(x, y)
+    assert ra.linear_solve.iterations == rb.linear_solve.iterations
+    assert ra.linear_solve.final_residual == rb.linear_solve.final_residual
+    assert ra.linear_solve.initial_residual == rb.linear_solve.initial_residual
+    assert ra.removed_rhs_mean == rb.removed_rhs_mean
+    assert ra.divergence_before == rb.divergence_before and ra.divergence_after == rb.divergence_after
+
+
+@needs_ref
+@pytest.mark.parametrize("alg", [0, 1, 2, 3])
+@pytest.mark.parametrize("n,box", [(9, 1.0), (12, 4.5), (13, 2.0)])
+def test_full_steps_bit_identical(alg, n, box):
+    p = algorithm_params(alg)
+    p.project_iterations, p.stir_strength, p.emitter_radius, p.emitter_center_z = 20, 0.5, 0.22, 0.3
+    a, r = OracleSim(n, box), RefSim(n, box)
+    a.params, r.params = p, p
+    a.reset()
+    r.reset()
+    for _ in range(8):
+        assert a.advance(1 / 60) == 0 and r.advance(1 / 60) == 0
+    for x, y in zip(a.fields(), r.fields()):
+        assert bits_equal(x, y)
+    pa, pr = a.last_projection(), r.last_projection()
+    assert pa.linear_solve.final_residual == pr.linear_solve.final_residual
+
+
+@needs_ref
+def test_tolerance_driven_steps_bit_identical():
+    """Tolerance-driven projections through the reference's setPressureSolver hook."""
+    p = algorithm_params(3)
+    p.use_solve_options = 1
+    p.solve = LinearSolveOptions.defaults(max_iterations=2000, relative_tolerance=1e-6, absolute_tolerance=0.0)
+    a, r = OracleSim(12, 1.0), RefSim(12, 1.0)
+    a.params, r.params = p, p
+    a.reset()
+    r.reset()
+    for _ in range(4):
+        assert a.advance(0.01) == 0 and r.advance(0.01) == 0
+        assert a.last_projection().linear_solve.iterations == r.last_projection().linear_solve.iterations
+    for x, y in zip(a.fields(), r.fields()):
+        assert bits_equal(x, y)
+
+
+def test_reference_step_fixtures_match_oracle():
+    """The committed reference fixtures (made from oracle/_ref) equal the oracle."""
+    data = np.load(os.path.join(GOLDEN, "reference_steps.npz"))
+    for reflection in (0, 1):
+        for mc_vel in (0, 1):
+            for mc_smoke in (0, 1):
+                p = default_params()
+                p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = reflection, mc_vel, mc_smoke
+                p.emitter_radius, p.emitter_center_z, p.stir_strength, p.project_iterations = 0.22, 0.3, 0.5, 20
+                sim = OracleSim(9, 1.0)
+                sim.params = p
+                sim.reset()
+                for _ in range(8):
+                    assert sim.advance(1 / 60) == 0
+                key = f"resident_r{reflection}_v{mc_vel}_s{mc_smoke}"
+                for name, a in zip("duvw", sim.fields()):
+                    assert bits_equal(a, data[f"{key}_{name}"]), key + name
+
+
+# ---- the reference's own known-answer tests, run against the oracle ----
+
+def test_sampling_known_answers():
+    """AdvectionTests.cpp:29-56: linear fields are sampled exactly; clamping."""
+    n, box = 4, 4.0
+    value = lambda x, y, z: x + 2 * y + 3 * z
+    sd, su, sv, sw = field_shapes(n)
+    zz, yy, xx = np.meshgrid(np.arange(n + 1), np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    d = value(xx[:n, :n, :n] + .5, yy[:n, :n, :n] + .5, zz[:n, :n, :n] + .5).astype(np.float32)
+    u = value(xx[:n, :n, :], yy[:n, :n, :] + .5, zz[:n, :n, :] + .5).astype(np.float32)
+    v = value(xx[:n, :, :n] + .5, yy[:n, :, :n], zz[:n, :, :n] + .5).astype(np.float32)
+    w = value(xx[:, :n, :n] + .5, yy[:, :n, :n] + .5, zz[:, :n, :n]).astype(np.float32)
+    o = oracle()
+    p = (1.2, 1.6, 2.1)
+    expected = value(*p)
+    for loc, f in enumerate((d, u, v, w)):
+        assert abs(o.vo_sample_f32(n, box, loc, f.ravel(), *p) - expected) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 0, d.ravel(), -1, -1, -1) - 3.0) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 1, u.ravel(), -1, -1, -1) - 2.5) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 0, d.ravel(), 9, 9, 9) - 21.0) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 1, u.ravel(), 9, 9, 9) - 21.5) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 2, v.ravel(), 9, 9, 9) - 22.0) <= 1e-5
+    assert abs(o.vo_sample_f32(n, box, 3, w.ravel(), 9, 9, 9) - 22.5) <= 1e-5
+    single = np.array([2.0], np.float32)
+    assert abs(o.vo_sample_f32(1, 4.5, 0, single, 1, 1, 1) - 2.0) <= 1e-5
+
+
+@pytest.mark.parametrize("mc", [0, 1])
+def test_uniform_translation_known_answer(mc):
+    """AdvectionTests.cpp:84-110: u=.5, dt=.5 translates a linear field by .25."""
+    n, box = 6, 6.0
+    d, u, v, w = [np.zeros(s, np.float32) for s in field_shapes(n)]
+    u[:] = 0.5
+    zz, yy, xx = np.meshgrid(np.arange(n + 1), np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    for loc, shape in enumerate(field_shapes(n)):
+        src = (xx + 2 * yy + 3 * zz)[: shape[0], : shape[1], : shape[2]].astype(np.float32)
+        out = oracle_advect(n, box, loc, 0.5, 3.0, mc, src, u, v, w)
+        assert abs(out[2, 2, 2] - (12.0 - 0.25)) <= 1e-5
+
+
+def test_projection_gradient_known_answer():
+    """NumericsTests.cpp:255-278: a discrete gradient projects to zero and the
+    pressure is recovered up to a constant."""
+    n, box, dt = 8, 4.0, 0.1
+    h = box / n
+    x = np.arange(n, dtype=np.float32)
+    zz, yy, xx = np.meshgrid(x, x, x, indexing="ij")
+    pot = (np.sin(np.float32(0.3) * xx) * np.cos(np.float32(0.4) * yy) + np.float32(0.2) * zz * zz / (n * n)).astype(np.float32)
+    f = np.float32(dt / h)
+    _, u, v, w = [np.zeros(s, np.float32) for s in field_shapes(n)]
+    u[:, :, 1:n] = f * (pot[:, :, 1:] - pot[:, :, :-1])
+    v[:, 1:n, :] = f * (pot[:, 1:, :] - pot[:, :-1, :])
+    w[1:n, :, :] = f * (pot[1:, :, :] - pot[:-1, :, :])
+    opts = LinearSolveOptions.defaults(max_iterations=4000, absolute_tolerance=1e-5, relative_tolerance=1e-6)
+    st, r, uo, vo, wo, p = oracle_project(n, box, u, v, w, dt, 1.5, 0.0, opts)
+    assert st == 0 and r.linear_solve.converged
+    for a in (uo, vo, wo):
+        assert np.abs(a).max() <= 1e-5
+    assert np.abs(p - (pot - pot.astype(np.float64).mean())).max() <= 1e-4
+
+
+def test_projection_solenoidal_known_answer():
+    """NumericsTests.cpp:311-325: a discrete curl is untouched (early exit)."""
+    n = 4
+    psi = lambda x, y: np.float32(x * (n - x) * y * (n - y))
+    _, u, v, w = [np.zeros(s, np.float32) for s in field_shapes(n)]
+    for z in range(n):
+        for y in range(n):
+            for x in range(n + 1):
+                u[z, y, x] = psi(x, y + 1) - psi(x, y)
+        for y in range(n + 1):
+            for x in range(n):
+                v[z, y, x] = -(psi(x + 1, y) - psi(x, y))
+    opts = LinearSolveOptions.defaults(max_iterations=4000, absolute_tolerance=1e-5, relative_tolerance=1e-6)
+    st, r, uo, vo, wo, _ = oracle_project(n, float(n), u, v, w, 0.02, 1.95, 0.0, opts)
+    assert st == 0 and r.linear_solve.converged and r.linear_solve.iterations == 0
+    assert np.array_equal(uo, u) and np.array_equal(vo, v) and np.array_equal(wo, w)
+
+
+def _legacy_projection(n, box, u, v, w, dt, iterations, omega):
+    """Independent restatement of the GLSL sor.comp loop (lagged Neumann ghost,
+    denominator 6), as NumericsTests.cpp:343-373 states it."""
+    o = oracle()
+    u, v, w = u.copy(), v.copy(), w.copy()
+    o.vo_enforce_walls_f32(n, u, v, w)
+    h = np.float32(np.float32(box) / np.float32(n))
+    div = np.zeros((n, n, n), np.float32)
+    hinv = np.float32(1) / h
+    for z in range(n):
+        for y in range(n):
+            for x in range(n):
+                s = (np.float32(u[z, y, x + 1]) - u[z, y, x] + v[z, y + 1, x] - v[z, y, x] + w[z + 1, y, x] - w[z, y, x])
+                div[z, y, x] = np.float32(s) * hinv
+    p = np.zeros((n, n, n), np.float32)
+    om = np.float32(omega)
+    c = h * h / np.float32(dt)
+    for _ in range(iterations):
+        for parity in range(2):
+            for z in range(n):
+                for y in range(n):
+                    for x in range((y + z + parity) & 1, n, 2):
+                        cen = p[z, y, x]
+                        s = np.float32(0)
+                        s += p[z, y, x - 1] if x > 0 else cen
+                        s += p[z, y, x + 1] if x + 1 < n else cen
+                        s += p[z, y - 1, x] if y > 0 else cen
+                        s += p[z, y + 1, x] if y + 1 < n else cen
+                        s += p[z - 1, y, x] if z > 0 else cen
+                        s += p[z + 1, y, x] if z + 1 < n else cen
+                        p[z, y, x] = (np.float32(1) - om) * cen + om * (s - div[z, y, x] * c) / np.float32(6)
+    o.vo_apply_gradient_f32(n, box, p, dt, u, v, w)
+    o.vo_enforce_walls_f32(n, u, v, w)
+    return u, v, w
+
+
+@pytest.mark.parametrize("n", [2, 3, 6])
+@pytest.mark.parametrize("iterations", [1, 8])
+def test_projection_matches_legacy_shader_formula(n, iterations):
+    """NumericsTests.cpp:375-384: floor-6 SOR equals the GLSL sor.comp formula."""
+    _, u, v, w = random_fields(n, seed=7 + n)
+    opts = LinearSolveOptions.defaults(max_iterations=iterations, fixed_iterations=1)
+    st, r, uo, vo, wo, _ = oracle_project(n, 4.5, u, v, w, 1 / 60, 1.95, 6.0, opts)
+    assert st == 0 and r.linear_solve.iterations == iterations
+    lu, lv, lw = _legacy_projection(n, 4.5, u, v, w, 1 / 60, iterations, 1.95)
+    for a, b in ((uo, lu), (vo, lv), (wo, lw)):
+        assert np.abs(a - b).max() <= 2e-5
+
+
+def test_seeded_replay():
+    """SimulationTests.cpp:44-75: seeded streams are independent; reset replays."""
+    def make(seed):
+        s = OracleSim(8)
+        p = s.params
+        p.emitter_radius, p.emitter_center_z, p.project_iterations, p.random_seed = .18, .3, 16, seed
+        s.params = p
+        s.reset()
+        return s
+    first, second, other = make(12345), make(12345), make(54321)
+    for _ in range(6):
+        first.advance(1 / 60)
+        other.advance(1 / 60)
+        second.advance(1 / 60)
+    assert all(bits_equal(a, b) for a, b in zip(first.fields(), second.fields()))
+    assert not bits_equal(first.fields()[1], other.fields()[1])
+    first.reset()
+    for _ in range(6):
+        first.advance(1 / 60)
+    assert all(bits_equal(a, b) for a, b in zip(first.fields(), second.fields()))
+
+
+@pytest.mark.parametrize("alg", [0, 3])
+def test_fp64_oracle_tracks_fp32(alg):
+    p = algorithm_params(alg)
+    p.project_iterations, p.stir_strength = 40, 0.0
+    a, b = OracleSim(10, 1.0), OracleSim(10, 1.0, dtype=np.float64)
+    a.params, b.params = p, p
+    a.reset()
+    b.reset()
+    for _ in range(4):
+        assert a.advance(1 / 60) == 0 and b.advance(1 / 60) == 0
+    for x, y in zip(a.fields(), b.fields()):
+        scale = max(1.0, float(np.abs(y).max()))
+        assert np.abs(x.astype(np.float64) - y).max() <= 1e-4 * scale
