@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MAC 3D smoke step.
+
+Workload (synthetic, seeded): the Reflection + MacCormack plume of the
+128^3 configuration, run at 256^3: box 1, dt 0.01, two profile sources
+min(1, 3 exp(-3.5 (d/r)^2)) of radius .08 at (x, y, z) = (.3, .5, .15) and
+(.7, .5, .15) (z up), buoyancy 1.5, smoke decay .995 per step, no kick or stir,
+initial velocity a seeded swirl of 8 Gaussian vortices (amplitude .5). Every
+projection solves to relative residual (= relative divergence) 1e-6 in FP64
+with the mixed-precision red-black SOR (FP32 sweeps, FP64 residual and
+pressure). Metric: steps/s (higher is better).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs under torchrun as independent replicas (one scene per GPU, no
+collective on the data path); value = N*K / max over ranks of the timed
+region. Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256^3 steps/s: learned-warm-start vs plain GPU solve at rel div 1e-6; HBM %"
+DT = 0.01
+# SOR relaxation per grid size for the floor-6 red-black sweep (chosen by
+# measured sweep counts to rel 1e-6 on this plume; larger grids want omega
+# closer to 2).
+OMEGA = {32: 1.95, 64: 1.95, 96: 1.96, 128: 1.97, 192: 1.975, 256: 1.98}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--rel", type=float, default=1e-6)
+    ap.add_argument("--max-iterations", type=int, default=20000)
+    ap.add_argument("--omega", type=float, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+def omega_for(n, override=None):
+    if override:
+        return override
+    keys = sorted(OMEGA)
+    return OMEGA[min(keys, key=lambda k: abs(k - n))]
+
+
+def scene_params(vb_params, n, rel, max_iterations, omega):
+    from vapor_b200.abi import LinearSolveOptions, SOLVER_MIXED_REFINEMENT
+    p = vb_params
+    p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = 1, 1, 1
+    p.buoyancy, p.buoyancy_split, p.cfl_mc = 1.5, 0.5, 3.0
+    p.smoke_decay = 0.5  # factor clamp(1 - .5 * .01) = .995 per step
+    p.emitter_radius, p.source_strength = 0.08, 1.0
+    p.emitter_center_x, p.emitter_center_y, p.emitter_center_z = 0.3, 0.5, 0.15
+    p.emitter_count = 2
+    p.emitter2_center_x, p.emitter2_center_y, p.emitter2_center_z = 0.7, 0.5, 0.15
+    p.emitter_profile = 1
+    p.emitter_kick_multiplier, p.stir_strength = 0.0, 0.0
+    p.sor_omega = omega
+    p.use_solve_options = 1
+    p.solver_kind = SOLVER_MIXED_REFINEMENT
+    p.solve = LinearSolveOptions.defaults(max_iterations=max_iterations, residual_check_interval=8,
+                                          relative_tolerance=rel, absolute_tolerance=0.0, fixed_iterations=0)
+    return p
+
+
+def swirl_fields(n, seed, amplitude=0.5, vortices=8, sigma=0.08):
+    """Seeded swirl: sum of Gaussian vortices (random centre and axis) on the
+    MAC faces, normal velocity zero on the walls; density zero."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.2, 0.8, size=(vortices, 3))
+    axes = rng.normal(size=(vortices, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    h = 1.0 / n
+
+    def comp(c, shape):
+        zz, yy, xx = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+        pos = [(xx + (0.0 if c == 0 else 0.5)) * h, (yy + (0.0 if c == 1 else 0.5)) * h,
+               (zz + (0.0 if c == 2 else 0.5)) * h]
+        out = np.zeros(shape)
+        for k in range(vortices):
+            r = [pos[d] - centres[k, d] for d in range(3)]
+            g = np.exp(-(r[0] ** 2 + r[1] ** 2 + r[2] ** 2) / (2 * sigma ** 2))
+            a = axes[k]
+            cross = [a[1] * r[2] - a[2] * r[1], a[2] * r[0] - a[0] * r[2], a[0] * r[1] - a[1] * r[0]]
+            out += amplitude * cross[c] / sigma * g
+        return out.astype(np.float32)
+
+    u = comp(0, (n, n, n + 1))
+    v = comp(1, (n, n + 1, n))
+    w = comp(2, (n + 1, n, n))
+    u[:, :, 0] = u[:, :, -1] = 0
+    v[:, 0, :] = v[:, -1, :] = 0
+    w[0] = w[-1] = 0
+    return [np.zeros((n, n, n), np.float32), u, v, w]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        exe = shutil.which("nvidia-smi")
+        if not exe:
+            return
+        self.proc = subprocess.Popen([exe, f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def reference_cpu_sample(n_target, sweeps_per_step, seed, n_sample=128):
+    """Times the reference's own CPU MAC 3D step (oracle/_ref) on a bounded
+    sample: one Reflection+MacCormack step at n_sample^3 of the same scene with
+    16 and then 48 fixed SOR sweeps, giving the non-solver cost and the cost per
+    sweep; both scale with the cell count to n_target^3. The reference has no
+    profile emitter or second source, so its sample uses its own emitter at the
+    first source position (the cost is dominated by transport and sweeps)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import RefSim, ref_available, default_params
+    if not ref_available():
+        return None
+    fields = swirl_fields(n_sample, seed)
+    times = {}
+    for iters in (16, 48):
+        sim = RefSim(n_sample, 1.0, fields=fields)
+        p = default_params()
+        p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = 1, 1, 1
+        p.buoyancy, p.smoke_decay, p.emitter_radius, p.source_strength = 1.5, 0.5, 0.08, 1.0
+        p.emitter_center_x, p.emitter_center_y, p.emitter_center_z = 0.3, 0.5, 0.15
+        p.emitter_kick_multiplier, p.stir_strength = 0.0, 0.0
+        p.sor_omega, p.project_iterations = omega_for(n_sample), iters
+        sim.params = p
+        t0 = time.perf_counter()
+        assert sim.advance(DT) == 0
+        times[iters] = time.perf_counter() - t0
+    per_sweep = (times[48] - times[16]) / 32.0
+    fixed = times[16] - 16 * per_sweep
+    scale = (n_target / n_sample) ** 3
+    step_s = scale * (fixed + sweeps_per_step * per_sweep)
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": 1, "kind": "reference",
+            "sample": (f"reference CPU MAC 3D step (oracle/_ref, single-threaded) at {n_sample}^3 with 16 and 48 "
+                       f"fixed sweeps: {fixed:.2f} s non-solver + {per_sweep * 1e3:.1f} ms/sweep, scaled by "
+                       f"{scale:.0f}x cells to {n_target}^3 and {sweeps_per_step:.0f} sweeps/step"),
+            "nproc": os.cpu_count()}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sweeps = REFERENCE_SWEEPS_PER_STEP
+    samples = []
+    t_start = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        s = reference_cpu_sample(args.n, sweeps, args.seed)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) missing"}))
+            return
+        samples.append(s["value"])
+    value = statistics.median(samples)
+    s["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"mac3d_reflection_maccormack_{args.n}", "n": args.n,
+                       "sweeps_per_step": sweeps, "note": "reference FP32 SOR stagnates above 1e-6; "
+                       "it is given the sweep count the GPU solve needed"},
+            "cpu_baseline": s, "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                       "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t_start}
+    print(json.dumps(line))
+
+
+# SOR sweeps per step the plain GPU solve needed on this workload at 256^3
+# (from the latest GPU run of this benchmark); the reference arm is charged
+# the same number of sweeps.
+REFERENCE_SWEEPS_PER_STEP = 6000
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import vapor_b200 as vb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    vb.set_device(local)
+    torch.cuda.set_device(local)
+
+    n = args.n
+    omega = omega_for(n, args.omega)
+    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega)
+    fields = swirl_fields(n, args.seed + rank)
+    sim = vb.MacSimulation3D(n, 1.0, params)
+    sim.upload(*fields)
+    for _ in range(args.warmup):
+        sim.advance(DT)
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it0 = sim.total_iterations()
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sim.set_timing(True)
+    launches0 = vb.kernel_launch_count()
+    clocks.start()
+    wall0 = time.perf_counter()
+    start.record(stream)
+    for _ in range(args.steps):
+        sim.advance(DT)
+    end.record(stream)
+    end.synchronize()
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop()
+    launches = vb.kernel_launch_count() - launches0
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    phases = sim.timings()
+    sim.set_timing(False)
+    sweeps = sim.total_iterations() - it0
+    result = sim.last_projection()
+    rel = result.linear_solve.final_residual / max(result.linear_solve.initial_residual, 1e-300)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # End to end through the public API: pinned host state in, step, state out.
+    pinned = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in fields]
+    for dst, src in zip(pinned, sim.download()):
+        dst[...] = src
+    out = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in fields]
+    h2d = sum(a.nbytes for a in pinned)
+    e2e_steps = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload(*pinned)
+        sim.advance(DT)
+        sim.download(out)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    cells = n ** 3
+    sor = phases["sor"]
+    sor_launch_ms = sor["ms"] / max(1, sor["launches"])
+    # One red-black iteration reads p and b and writes p once: 12 B/cell; a
+    # colour launch is half an iteration.
+    sor_bytes = 6.0 * cells
+    achieved = sor_bytes / (sor_launch_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": world * args.steps / (ms * 1e-3), "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"mac3d_reflection_maccormack_{n}", "n": n, "dt": DT, "solver": "plain GPU "
+                   "red-black SOR, FP32 sweeps + FP64 residual/pressure refinement", "omega": omega,
+                   "relative_tolerance": args.rel, "sweeps_per_step": sweeps / args.steps,
+                   "final_relative_residual": rel, "converged": bool(result.linear_solve.converged),
+                   "l2": "state (4 x 67 MB fields) and solver buffers exceed the 126 MB L2",
+                   "parallelism": f"replicas{world}"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_sor_color", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": sor_bytes, "avg_launch_us": sor_launch_ms * 1e3},
+        "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in phases.items()},
+        "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d},
+        "clocks": clock_info, "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_cpu_sample(n, sweeps / args.steps, args.seed)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -159,10 +159,36 @@ typedef struct vapor_mac3d_params {
     float emitter2_center_x, emitter2_center_y, emitter2_center_z;
 } vapor_mac3d_params;
 
+/* Per-phase device timings of a handle, accumulated between enabling timing
+ * and reading it (CUDA events on the handle's stream; the analogue of the
+ * reference's TimedAdvection/TimedPressure wrappers, tests/GpuPerformance.cpp:14-44).
+ * Index the arrays with vapor_phase. `launches` counts kernel launches and
+ * `cells` the grid cells each launch covers (for bytes-per-cell rooflines). */
+typedef enum vapor_phase {
+    VAPOR_PHASE_FORCING = 0,   /* emit, buoyancy, walls */
+    VAPOR_PHASE_ADVECT = 1,    /* velocity and smoke transport */
+    VAPOR_PHASE_RHS = 2,       /* divergence, right-hand side, mean */
+    VAPOR_PHASE_SOR = 3,       /* red-black colour sweeps */
+    VAPOR_PHASE_RESIDUAL = 4,  /* FP64 residual checks and re-centring */
+    VAPOR_PHASE_GRADIENT = 5,  /* pressure gauge, final residual, gradient, divergence after */
+    VAPOR_PHASE_COUNT = 6
+} vapor_phase;
+
+typedef struct vapor_phase_timings {
+    double milliseconds[VAPOR_PHASE_COUNT];
+    int64_t launches[VAPOR_PHASE_COUNT];
+    int64_t intervals[VAPOR_PHASE_COUNT]; /* timed event pairs */
+} vapor_phase_timings;
+
 /* Error message of the last failing call on this thread ("" if none). */
 const char *vapor_last_error(void);
 /* VAPOR_B200_ABI_VERSION of the loaded library. */
 int32_t vapor_abi_version(void);
+/* Kernels launched by this library so far (all handles, all threads). */
+int64_t vapor_kernel_launch_count(void);
+/* Select the CUDA device for handles created afterwards on this thread
+ * (one process per GPU: pass the local rank). */
+vapor_status vapor_set_device(int32_t device);
 
 /* Defaults of MacGridParameters3D() and of MacGridParameters3D(MacAlgorithm)
  * (MacGridFluidSolver3D.cpp:11-26). */
@@ -220,6 +246,10 @@ vapor_status vapor_mac3d_device_fields(vapor_mac3d *sim, float **density, float 
  * work or record CUDA events against the step. */
 vapor_status vapor_mac3d_stream(vapor_mac3d *sim, void **stream);
 vapor_status vapor_mac3d_resolution(const vapor_mac3d *sim, int32_t *n, float *box);
+/* Enable (1) or disable (0) phase timing; enabling clears the accumulators. */
+vapor_status vapor_mac3d_set_timing(vapor_mac3d *sim, int32_t enabled);
+/* Waits for the stream, folds recorded intervals into the totals and returns them. */
+vapor_status vapor_mac3d_timings(vapor_mac3d *sim, vapor_phase_timings *out);
 
 /* ------------------------------------------------------------------------ */
 /* Staged stage plugins: Projection3D / Advection3D with host spans           */
@@ -261,6 +291,9 @@ vapor_status vapor_stage_advect_face_device(vapor_stage *stage, int32_t axis, fl
 vapor_status vapor_stage_advect_scalar_device(vapor_stage *stage, float dt, float cfl_limit,
                                               int32_t method, float *field, const float *flow_u,
                                               const float *flow_v, const float *flow_w);
+/* Pressure solver used by vapor_stage_project (vapor_solver_kind); the default
+ * is VAPOR_SOLVER_RED_BLACK_SOR, the reference's SOR. */
+vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 
 #ifdef __cplusplus

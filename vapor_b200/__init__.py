@@ -1,0 +1,337 @@
+"""vapor_b200: B200-native MAC 3D smoke step (Simple and Reflection variants).
+
+Python mirror of the reference's solver interface over the C ABI in
+include/vapor_b200.h (the shared library vapor_b200/_lib/libvapor_b200.so,
+built by vapor_b200._build). Names follow the reference:
+
+  MacSimulation3D   GpuMacSimulation3D (src/solvers/mac3d/gpu/GpuMacSimulation3D.hpp:9-46):
+                    advance / reset_state / set_box_size / parameters /
+                    last_projection / upload / download / byte counters,
+                    plus diagnostics() (MacGridFluidSolver3D.cpp:332-334)
+  StageBackend      the staged Projection3D / Advection3D plugins
+                    (Projection3D.hpp:6-11, Advection3D.hpp:6-14)
+
+Errors raise the reference's exception types: ValueError for
+std::invalid_argument (VAPOR_INVALID_ARGUMENT / VAPOR_NON_FINITE),
+OverflowError for std::length_error, RuntimeError for backend failures.
+There is no CPU fallback: without the built library or a B200 device every
+call fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import (FluidDiagnostics, LinearSolveOptions, MacParams, ProjectionOptions, ProjectionResult,
+                  field_shapes, field_sizes)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "_lib", "libvapor_b200.so")
+
+_lib = None
+
+
+class VaporError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class InvalidArgument(VaporError, ValueError):
+    pass
+
+
+class LengthError(VaporError, OverflowError):
+    pass
+
+
+class NonFinite(InvalidArgument):
+    pass
+
+
+class OutOfMemory(VaporError, MemoryError):
+    pass
+
+
+_ERRORS = {abi.VAPOR_INVALID_ARGUMENT: InvalidArgument, abi.VAPOR_LENGTH_ERROR: LengthError,
+           abi.VAPOR_NON_FINITE: NonFinite, abi.VAPOR_OUT_OF_MEMORY: OutOfMemory}
+
+_vp = C.c_void_p
+_fp = C.POINTER(C.c_float)
+
+
+def _declare(lib):
+    def f(name, *args, res=C.c_int):
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = list(args)
+    f("vapor_last_error", res=C.c_char_p)
+    f("vapor_abi_version", res=C.c_int32)
+    f("vapor_kernel_launch_count", res=C.c_int64)
+    f("vapor_set_device", C.c_int32)
+    f("vapor_mac3d_default_params", C.POINTER(MacParams))
+    f("vapor_mac3d_algorithm_params", C.c_int32, C.POINTER(MacParams))
+    f("vapor_default_projection_options", C.POINTER(ProjectionOptions))
+    f("vapor_mac3d_create", C.c_int32, C.c_float, C.POINTER(MacParams), C.POINTER(_vp))
+    f("vapor_mac3d_destroy", _vp)
+    f("vapor_mac3d_reset", _vp)
+    f("vapor_mac3d_set_box", _vp, C.c_float)
+    f("vapor_mac3d_get_params", _vp, C.POINTER(MacParams))
+    f("vapor_mac3d_set_params", _vp, C.POINTER(MacParams))
+    f("vapor_mac3d_advance", _vp, C.c_float)
+    f("vapor_mac3d_advance_n", _vp, C.c_float, C.c_int32)
+    f("vapor_mac3d_synchronize", _vp)
+    f("vapor_mac3d_last_projection", _vp, C.POINTER(ProjectionResult))
+    f("vapor_mac3d_total_iterations", _vp, C.POINTER(C.c_int64))
+    f("vapor_mac3d_diagnostics", _vp, C.POINTER(FluidDiagnostics))
+    f("vapor_mac3d_upload", _vp, _vp, _vp, _vp, _vp)
+    f("vapor_mac3d_download", _vp, _vp, _vp, _vp, _vp)
+    f("vapor_mac3d_byte_counters", _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+    f("vapor_mac3d_device_fields", _vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp))
+    f("vapor_mac3d_stream", _vp, C.POINTER(_vp))
+    f("vapor_mac3d_resolution", _vp, C.POINTER(C.c_int32), C.POINTER(C.c_float))
+    f("vapor_mac3d_set_timing", _vp, C.c_int32)
+    f("vapor_mac3d_timings", _vp, C.POINTER(abi.PhaseTimings))
+    f("vapor_stage_create", C.c_int32, C.c_float, C.POINTER(_vp))
+    f("vapor_stage_destroy", _vp)
+    f("vapor_stage_reset", _vp)
+    f("vapor_stage_project", _vp, _vp, _vp, _vp, C.POINTER(ProjectionOptions), C.c_float,
+      C.POINTER(ProjectionResult), _vp)
+    f("vapor_stage_project_device", _vp, _vp, _vp, _vp, C.POINTER(ProjectionOptions), C.c_float,
+      C.POINTER(ProjectionResult), _vp)
+    f("vapor_stage_advect_face", _vp, C.c_int32, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp)
+    f("vapor_stage_advect_face_device", _vp, C.c_int32, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp, _vp)
+    f("vapor_stage_advect_scalar", _vp, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp)
+    f("vapor_stage_advect_scalar_device", _vp, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp)
+    f("vapor_stage_set_solver_kind", _vp, C.c_int32)
+    f("vapor_stage_stream", _vp, C.POINTER(_vp))
+    return lib
+
+
+def library():
+    """The loaded C library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise RuntimeError(f"vapor_b200 CUDA library not built: {LIBRARY_PATH} "
+                               "(run vapor_b200._build.build())")
+        _lib = _declare(C.CDLL(LIBRARY_PATH))
+        if _lib.vapor_abi_version() != abi.ABI_VERSION:
+            raise RuntimeError("vapor_b200 library ABI version mismatch")
+    return _lib
+
+
+def check(status):
+    if status != abi.VAPOR_OK:
+        msg = library().vapor_last_error().decode(errors="replace")
+        raise _ERRORS.get(status, VaporError)(status, msg)
+
+
+def set_device(device):
+    """Select the CUDA device for handles created afterwards on this thread."""
+    check(library().vapor_set_device(int(device)))
+
+
+def kernel_launch_count():
+    """Kernels launched by the library so far (exact counter)."""
+    return library().vapor_kernel_launch_count()
+
+
+def default_params():
+    p = MacParams()
+    check(library().vapor_mac3d_default_params(C.byref(p)))
+    return p
+
+
+def algorithm_params(algorithm):
+    p = MacParams()
+    check(library().vapor_mac3d_algorithm_params(algorithm, C.byref(p)))
+    return p
+
+
+def default_projection_options():
+    o = ProjectionOptions()
+    check(library().vapor_default_projection_options(C.byref(o)))
+    return o
+
+
+def _host(a, n_expected, writable=False):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags.c_contiguous:
+        raise TypeError("fields must be C-contiguous float32 numpy arrays")
+    if a.size != n_expected:
+        raise InvalidArgument(abi.VAPOR_INVALID_ARGUMENT, "field size does not match the grid layout")
+    if writable and not a.flags.writeable:
+        raise TypeError("output array is read-only")
+    return a.ctypes.data
+
+
+class MacSimulation3D:
+    """Resident MAC 3D simulation on one B200 (GpuMacSimulation3D's interface).
+
+    MacSimulation3D(algorithm) builds the reference's 32^3, box 4.5 preset;
+    MacSimulation3D(n, box, params) takes an explicit grid and parameters.
+    """
+
+    def __init__(self, n_or_algorithm, box=None, params=None):
+        lib = library()
+        if box is None and params is None:
+            params = algorithm_params(n_or_algorithm)
+            n, box = 32, 4.5
+        else:
+            n = n_or_algorithm
+            params = params if params is not None else default_params()
+        self.n = int(n)
+        h = _vp()
+        check(lib.vapor_mac3d_create(self.n, float(box), C.byref(params), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().vapor_mac3d_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # parameters() -> mutable copy; assign back with set_parameters
+    def parameters(self):
+        p = MacParams()
+        check(library().vapor_mac3d_get_params(self._h, C.byref(p)))
+        return p
+
+    def set_parameters(self, p):
+        check(library().vapor_mac3d_set_params(self._h, C.byref(p)))
+
+    def advance(self, dt, steps=1):
+        if steps == 1:
+            check(library().vapor_mac3d_advance(self._h, float(dt)))
+        else:
+            check(library().vapor_mac3d_advance_n(self._h, float(dt), int(steps)))
+
+    def synchronize(self):
+        check(library().vapor_mac3d_synchronize(self._h))
+
+    def reset_state(self):
+        check(library().vapor_mac3d_reset(self._h))
+
+    def set_box_size(self, box):
+        check(library().vapor_mac3d_set_box(self._h, float(box)))
+
+    @property
+    def box_size(self):
+        n, b = C.c_int32(), C.c_float()
+        check(library().vapor_mac3d_resolution(self._h, C.byref(n), C.byref(b)))
+        return b.value
+
+    def last_projection(self):
+        r = ProjectionResult()
+        check(library().vapor_mac3d_last_projection(self._h, C.byref(r)))
+        return r
+
+    def total_iterations(self):
+        v = C.c_int64()
+        check(library().vapor_mac3d_total_iterations(self._h, C.byref(v)))
+        return v.value
+
+    def diagnostics(self):
+        d = FluidDiagnostics()
+        check(library().vapor_mac3d_diagnostics(self._h, C.byref(d)))
+        return d
+
+    def upload(self, density, u, v, w):
+        sizes = field_sizes(self.n)
+        ptrs = [_host(a, s) for a, s in zip((density, u, v, w), sizes)]
+        check(library().vapor_mac3d_upload(self._h, *ptrs))
+
+    def download(self, out=None):
+        if out is None:
+            out = [np.empty(s, np.float32) for s in field_shapes(self.n)]
+        sizes = field_sizes(self.n)
+        ptrs = [_host(a, s, writable=True) for a, s in zip(out, sizes)]
+        check(library().vapor_mac3d_download(self._h, *ptrs))
+        return out
+
+    def byte_counters(self):
+        up, down = C.c_uint64(), C.c_uint64()
+        check(library().vapor_mac3d_byte_counters(self._h, C.byref(up), C.byref(down)))
+        return up.value, down.value
+
+    def device_fields(self):
+        ptrs = [_vp() for _ in range(4)]
+        check(library().vapor_mac3d_device_fields(self._h, *[C.byref(p) for p in ptrs]))
+        return [p.value for p in ptrs]
+
+    def stream(self):
+        s = _vp()
+        check(library().vapor_mac3d_stream(self._h, C.byref(s)))
+        return s.value
+
+    def set_timing(self, enabled):
+        check(library().vapor_mac3d_set_timing(self._h, int(bool(enabled))))
+
+    def timings(self):
+        t = abi.PhaseTimings()
+        check(library().vapor_mac3d_timings(self._h, C.byref(t)))
+        return t.as_dict()
+
+
+class StageBackend:
+    """Staged Projection3D / Advection3D plugins over host (numpy) spans."""
+
+    def __init__(self, n, box):
+        self.n = int(n)
+        h = _vp()
+        check(library().vapor_stage_create(self.n, float(box), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().vapor_stage_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def reset(self):
+        check(library().vapor_stage_reset(self._h))
+
+    def set_solver_kind(self, kind):
+        check(library().vapor_stage_set_solver_kind(self._h, int(kind)))
+
+    def project(self, u, v, w, options, diagonal_floor=0.0, want_pressure=False):
+        """Projection3D::project in place on (u, v, w); returns (result, pressure)."""
+        f = field_sizes(self.n)[1]
+        ptrs = [_host(a, f, writable=True) for a in (u, v, w)]
+        r = ProjectionResult()
+        p = np.empty((self.n,) * 3, np.float32) if want_pressure else None
+        check(library().vapor_stage_project(self._h, *ptrs, C.byref(options), float(diagonal_floor), C.byref(r),
+                                            p.ctypes.data if p is not None else None))
+        return r, p
+
+    def advect_face(self, axis, dt, cfl, method, source, flow, output):
+        f = field_sizes(self.n)[1]
+        ptrs = [_host(a, f) for a in (source,) + tuple(flow)]
+        out = _host(output, f, writable=True)
+        check(library().vapor_stage_advect_face(self._h, int(axis), float(dt), float(cfl), int(method), ptrs[0],
+                                                ptrs[1], ptrs[2], ptrs[3], out))
+
+    def advect_scalar(self, dt, cfl, method, field, flow):
+        c, f = field_sizes(self.n)[:2]
+        fp = _host(field, c, writable=True)
+        ptrs = [_host(a, f) for a in flow]
+        check(library().vapor_stage_advect_scalar(self._h, float(dt), float(cfl), int(method), fp, *ptrs))
+
+
+__all__ = ["MacSimulation3D", "StageBackend", "MacParams", "ProjectionOptions", "LinearSolveOptions",
+           "ProjectionResult", "FluidDiagnostics", "default_params", "algorithm_params",
+           "default_projection_options", "library", "check", "VaporError", "InvalidArgument", "LengthError",
+           "NonFinite", "OutOfMemory", "field_shapes", "field_sizes", "LIBRARY_PATH"]

@@ -126,6 +126,17 @@ class MacParams(C.Structure):
         return self
 
 
+PHASES = ("forcing", "advect", "rhs", "sor", "residual", "gradient")
+
+
+class PhaseTimings(C.Structure):
+    _fields_ = [("milliseconds", C.c_double * 6), ("launches", C.c_int64 * 6), ("intervals", C.c_int64 * 6)]
+
+    def as_dict(self):
+        return {name: {"ms": self.milliseconds[i], "launches": self.launches[i], "intervals": self.intervals[i]}
+                for i, name in enumerate(PHASES)}
+
+
 def field_sizes(n):
     """Element counts of density, u, v, w for resolution n (MacGridState3D.cpp:12-15)."""
     c = n * n * n

@@ -1,0 +1,588 @@
+// Host-side engine: buffers, projection orchestration, resident coordinator
+// (GpuMacSimulation3D's role, gpu/GpuMacSimulation3D.cpp:49-264) and staged
+// stages (GpuPressureSolver.cpp / GpuAdvection.cpp).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+
+namespace vb {
+
+void fail(vapor_status code, const std::string& message) { throw Error(code, message); }
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const vapor_status code = e == cudaErrorMemoryAllocation ? VAPOR_OUT_OF_MEMORY : VAPOR_RUNTIME_ERROR;
+    throw Error(code, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+void DevArray<T>::allocate(size_t count) {
+    release();
+    if (count == 0) return;
+    void* ptr = nullptr;
+    VB_CUDA(cudaMalloc(&ptr, count * sizeof(T)));
+    p = static_cast<T*>(ptr);
+    n = count;
+}
+template <class T>
+void DevArray<T>::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+}
+template <class T>
+void DevArray<T>::zero(cudaStream_t s) {
+    if (p) VB_CUDA(cudaMemsetAsync(p, 0, bytes(), s));
+}
+template struct DevArray<float>;
+template struct DevArray<double>;
+template struct DevArray<uint32_t>;
+
+Stream::Stream() { VB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+Stream::~Stream() {
+    if (s) cudaStreamDestroy(s);
+}
+
+void validate_grid(int n, float box) {
+    if (n <= 0) fail(VAPOR_INVALID_ARGUMENT, "MAC grid resolution must be positive");
+    const size_t nn = size_t(n);
+    const size_t limit = size_t(std::numeric_limits<int>::max());
+    if (nn > limit / nn || nn * nn > limit / (nn + 1)) fail(VAPOR_LENGTH_ERROR, "MAC grid exceeds the supported index range");
+    if (!std::isfinite(box) || box <= 0.f || box / float(n) <= 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "MAC grid requires a finite positive box size and spacing");
+}
+
+static bool valid_options(const vapor_linear_solve_options& o) {
+    return o.max_iterations >= 0 && o.residual_check_interval > 0 && std::isfinite(o.absolute_tolerance) &&
+           o.absolute_tolerance >= 0.0 && std::isfinite(o.relative_tolerance) && o.relative_tolerance >= 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// PhaseTimer
+// ---------------------------------------------------------------------------
+PhaseTimer::~PhaseTimer() {
+    for (auto& p : pending_) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : pool_) cudaEventDestroy(e);
+    for (auto e : open_)
+        if (e) cudaEventDestroy(e);
+}
+
+cudaEvent_t PhaseTimer::take() {
+    if (!pool_.empty()) {
+        cudaEvent_t e = pool_.back();
+        pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    VB_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void PhaseTimer::enable(bool on) {
+    fold(true);
+    on_ = on;
+    acc_ = vapor_phase_timings{};
+}
+
+void PhaseTimer::begin(int phase) {
+    if (!on_) return;
+    cudaEvent_t e = take();
+    VB_CUDA(cudaEventRecord(e, s_));
+    if (open_[phase]) pool_.push_back(open_[phase]);
+    open_[phase] = e;
+}
+
+void PhaseTimer::end(int phase, long long launches) {
+    if (!on_ || !open_[phase]) return;
+    cudaEvent_t e = take();
+    VB_CUDA(cudaEventRecord(e, s_));
+    pending_.push_back({phase, open_[phase], e, launches});
+    open_[phase] = nullptr;
+    if (pending_.size() > 4096) fold(true);
+}
+
+void PhaseTimer::fold(bool wait) {
+    if (pending_.empty()) return;
+    if (wait) VB_CUDA(cudaStreamSynchronize(s_));
+    size_t keep = 0;
+    for (size_t i = 0; i < pending_.size(); ++i) {
+        Pending& p = pending_[i];
+        if (!wait && cudaEventQuery(p.b) != cudaSuccess) {
+            pending_[keep++] = p;
+            continue;
+        }
+        float ms = 0.f;
+        VB_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        acc_.milliseconds[p.phase] += ms;
+        acc_.launches[p.phase] += p.launches;
+        acc_.intervals[p.phase] += 1;
+        pool_.push_back(p.a);
+        pool_.push_back(p.b);
+    }
+    pending_.resize(keep);
+    (void)cudaGetLastError();  // clear cudaErrorNotReady from queries
+}
+
+vapor_phase_timings PhaseTimer::totals() {
+    fold(true);
+    return acc_;
+}
+
+// ---------------------------------------------------------------------------
+// Workspace
+// ---------------------------------------------------------------------------
+Workspace::Workspace(int n, float box, cudaStream_t stream)
+    : n_(n), box_(box), stream_(stream), timer_(stream) {
+    validate_grid(n, box);
+    const size_t cells = size_t(n) * n * n;
+    const size_t faces = size_t(n) * n * (n + 1);
+    b_.allocate(cells);
+    p_.allocate(cells);
+    fwd_.allocate(faces);
+    partial_capacity_ = reduction_blocks(faces);
+    partials_.allocate(size_t(partial_capacity_));
+    VB_CUDA(cudaMalloc(&ctrl_, sizeof(ProjControl)));
+    VB_CUDA(cudaMalloc(&diag_, sizeof(DiagControl)));
+    VB_CUDA(cudaMallocHost(&ctrl_host_, sizeof(ProjControl)));
+    VB_CUDA(cudaMallocHost(&diag_host_, sizeof(DiagControl)));
+    VB_CUDA(cudaMallocHost(&done_host_, sizeof(int)));
+    std::memset(ctrl_host_, 0, sizeof(ProjControl));
+    reset_buffers();
+    VB_CUDA(cudaStreamSynchronize(stream_));
+}
+
+Workspace::~Workspace() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (ctrl_) cudaFree(ctrl_);
+    if (diag_) cudaFree(diag_);
+    if (ctrl_host_) cudaFreeHost(ctrl_host_);
+    if (diag_host_) cudaFreeHost(diag_host_);
+    if (done_host_) cudaFreeHost(done_host_);
+}
+
+void Workspace::reset_buffers() {
+    b_.zero(stream_);
+    p_.zero(stream_);
+    fwd_.zero(stream_);
+    VB_CUDA(cudaMemsetAsync(ctrl_, 0, sizeof(ProjControl), stream_));
+    VB_CUDA(cudaMemsetAsync(diag_, 0, sizeof(DiagControl), stream_));
+    total_iterations_ = 0;
+    sticky_errors_ = 0u;
+}
+
+void Workspace::clear_errors() { VB_CUDA(cudaMemsetAsync(&ctrl_->sticky_nonfinite, 0, sizeof(unsigned int), stream_)); }
+
+void Workspace::advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u,
+                       const float* v, const float* w, float* out, float post_scale) {
+    timer_.begin(VAPOR_PHASE_ADVECT);
+    launch_advect(grid(), loc, dt, cfl, maccormack, src, u, v, w, fwd_.p, out, post_scale, stream_);
+    timer_.end(VAPOR_PHASE_ADVECT, maccormack ? 2 : 1);
+    VB_CUDA(cudaGetLastError());
+}
+
+void Workspace::project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo,
+                        float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
+                        const vapor_linear_solve_options& o, int solver_kind) {
+    const ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
+    cudaStream_t s = stream_;
+    PhaseTimer& t = timer_;
+    t.begin(VAPOR_PHASE_RHS);
+    launch_rhs(a, ui, vi, wi, b_.p, partials_.p, partial_capacity_, ctrl_, s);
+    p_.zero(s);
+    t.end(VAPOR_PHASE_RHS, 3);
+    auto wait_done = [&]() {
+        VB_CUDA(cudaMemcpyAsync(done_host_, &ctrl_->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+        VB_CUDA(cudaStreamSynchronize(s));
+        t.fold(false);
+        return *done_host_ != 0;
+    };
+    auto sweeps = [&](int k, float* x, const float* rhs, bool guarded, bool subtract_mean) {
+        t.begin(VAPOR_PHASE_SOR);
+        for (int j = 0; j < k; ++j) {
+            launch_sor_color(a, 0, x, rhs, ctrl_, guarded, s, subtract_mean);
+            launch_sor_color(a, 1, x, rhs, ctrl_, guarded, s, subtract_mean);
+        }
+        t.end(VAPOR_PHASE_SOR, 2LL * k);
+    };
+    if (solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT) {
+        // FP32 red-black sweeps on the error equation, re-centred in FP64 at
+        // every residual check (see the oracle's refinementSolve).
+        const size_t cells = b_.n;
+        for (auto& x : x64_)
+            if (x.n != cells) x.allocate(cells);
+        if (r32_.n != cells) r32_.allocate(cells);
+        x64_[0].zero(s);
+        int cur = 0, it = 0;
+        for (;;) {
+            t.begin(VAPOR_PHASE_RESIDUAL);
+            launch_refine_residual(a, b_.p, x64_[cur].p, p_.p, x64_[1 - cur].p, r32_.p, ctrl_, s);
+            cur = 1 - cur;
+            launch_check(ctrl_, it, false, 0ull, s);
+            t.end(VAPOR_PHASE_RESIDUAL, 1);
+            if (wait_done()) break;
+            p_.zero(s);
+            const int k = std::min(o.residual_check_interval - it % o.residual_check_interval, o.max_iterations - it);
+            sweeps(k, p_.p, r32_.p, false, false);
+            it += k;
+        }
+        t.begin(VAPOR_PHASE_GRADIENT);
+        launch_pressure_mean64(a, x64_[cur].p, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
+        launch_gradient64(a, x64_[cur].p, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        t.end(VAPOR_PHASE_GRADIENT, 5);
+    } else {
+        if (o.max_iterations > 0) {
+            if (o.fixed_iterations) {
+                // Intermediate residual checks cannot change a fixed-budget
+                // solve: the final residual and convergence are recomputed
+                // after the pressure gauge (CpuPressureSolver3D.cpp:50-56).
+                sweeps(o.max_iterations, p_.p, b_.p, true, true);
+                launch_check(ctrl_, o.max_iterations, false, 0ull, s);
+            } else {
+                int it = 0;
+                bool stop = wait_done();
+                while (!stop && it < o.max_iterations) {
+                    const int to_check = o.residual_check_interval - it % o.residual_check_interval;
+                    const int k = std::min(to_check, o.max_iterations - it);
+                    sweeps(k, p_.p, b_.p, false, true);
+                    it += k;
+                    t.begin(VAPOR_PHASE_RESIDUAL);
+                    launch_residual(a, p_.p, b_.p, ctrl_, false, s);
+                    launch_check(ctrl_, it, false, 0ull, s);
+                    t.end(VAPOR_PHASE_RESIDUAL, 1);
+                    stop = wait_done();
+                }
+            }
+        }
+        t.begin(VAPOR_PHASE_GRADIENT);
+        launch_pressure_mean(a, p_.p, partials_.p, partial_capacity_, ctrl_, s);
+        launch_residual(a, p_.p, b_.p, ctrl_, true, s);
+        launch_gradient(a, p_.p, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        t.end(VAPOR_PHASE_GRADIENT, 5);
+    }
+    launch_finish_projection(ctrl_, s);
+    VB_CUDA(cudaGetLastError());
+    VB_CUDA(cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(ProjControl), cudaMemcpyDeviceToHost, s));
+}
+
+vapor_projection_result Workspace::last_result() {
+    VB_CUDA(cudaStreamSynchronize(stream_));
+    if (ctrl_host_->sticky_nonfinite & 1u) fail(VAPOR_NON_FINITE, "Non-finite divergence");
+    if (ctrl_host_->sticky_nonfinite & 6u) fail(VAPOR_NON_FINITE, "Non-finite MAC velocity");
+    return ctrl_host_->result;
+}
+
+long long Workspace::total_iterations() {
+    VB_CUDA(cudaMemcpyAsync(ctrl_host_, ctrl_, sizeof(ProjControl), cudaMemcpyDeviceToHost, stream_));
+    VB_CUDA(cudaStreamSynchronize(stream_));
+    return ctrl_host_->total_iterations;
+}
+
+void Workspace::diagnostics(const float* u, const float* v, const float* w, vapor_fluid_diagnostics* out) {
+    launch_diagnostics(grid(), u, v, w, partials_.p, partial_capacity_, diag_, stream_);
+    VB_CUDA(cudaGetLastError());
+    VB_CUDA(cudaMemcpyAsync(diag_host_, diag_, sizeof(DiagControl), cudaMemcpyDeviceToHost, stream_));
+    VB_CUDA(cudaStreamSynchronize(stream_));
+    if (diag_host_->nonfinite) fail(VAPOR_NON_FINITE, "Non-finite MAC velocity");
+    const double dx = double(grid().h);
+    out->kinetic_energy = float(0.5 * diag_host_->kinetic_sum * dx * dx * dx);
+    uint32_t bits = diag_host_->max_velocity_bits;
+    std::memcpy(&out->max_velocity, &bits, sizeof(float));
+    bits = diag_host_->max_divergence_bits;
+    std::memcpy(&out->max_divergence, &bits, sizeof(float));
+}
+
+// ---------------------------------------------------------------------------
+// Resident simulation
+// ---------------------------------------------------------------------------
+Simulation::Simulation(int n, float box, const vapor_mac3d_params& p) : params(p), ws_(n, box, stream_.s) {
+    const size_t cells = size_t(n) * n * n;
+    const size_t faces = size_t(n) * n * (n + 1);
+    for (auto& d : dens_) d.allocate(cells);
+    for (auto& set : vel_)
+        for (auto& c : set) c.allocate(faces);
+    rng_.allocate(1);
+    reset();
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+}
+
+Simulation::~Simulation() { cudaStreamSynchronize(ws_.stream()); }
+
+void Simulation::reset() {
+    cudaStream_t s = ws_.stream();
+    for (auto& d : dens_) d.zero(s);
+    for (auto& set : vel_)
+        for (auto& c : set) c.zero(s);
+    ws_.reset_buffers();
+    const uint32_t seed = params.random_seed;
+    VB_CUDA(cudaMemcpyAsync(rng_.p, &seed, sizeof(seed), cudaMemcpyHostToDevice, s));
+    // The seed is a stack value: wait so the copy has read it.
+    VB_CUDA(cudaStreamSynchronize(s));
+    std::memset(ws_.ctrl_host_, 0, sizeof(ProjControl));
+    cur_ = 0;
+    S_ = 0;
+    T_ = 1;
+    U_ = 2;
+}
+
+void Simulation::set_box(float box) {
+    if (!std::isfinite(box) || box <= 0.f || box / float(ws_.n()) <= 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "Invalid GPU box size");
+    if (box != ws_.box()) {
+        ws_.set_box(box);
+        reset();
+    }
+}
+
+vapor_linear_solve_options Simulation::solve_options(int iterations) const {
+    if (params.use_solve_options) return params.solve;
+    vapor_linear_solve_options o{};
+    o.max_iterations = iterations;
+    o.residual_check_interval = 8;
+    o.absolute_tolerance = 1e-6;
+    o.relative_tolerance = 1e-5;
+    o.fixed_iterations = 1;
+    return o;
+}
+
+// Emitter patch of MacGridFluidSolver3D::emit (MacGridFluidSolver3D.cpp:140-147),
+// computed in the same FP32 operations.
+void Simulation::emit_one(float cxf, float cyf, float czf, float dt) {
+    const Grid g = ws_.grid();
+    const float dx = g.h;
+    const float box = g.box;
+    EmitterBox e{};
+    e.ec[0] = cxf * box;
+    e.ec[1] = cyf * box;
+    e.ec[2] = czf * box;
+    e.erad = params.emitter_radius * box;
+    const int R = int(e.erad / dx + 1);
+    for (int a = 0; a < 3; ++a) {
+        const int c = int(e.ec[a] / dx);
+        e.lo[a] = std::max(0, c - R);
+        e.size[a] = std::min(g.n, c + R) - e.lo[a];
+    }
+    if (e.size[0] <= 0 || e.size[1] <= 0 || e.size[2] <= 0) return;
+    e.kick = params.emitter_kick_multiplier * (params.emitter_kick_base + params.emitter_kick_scale * params.source_strength);
+    e.apply_kick = params.emitter_kick_multiplier > 0.f;
+    e.stir = params.stir_strength;
+    e.dt_scale = dt * 60.0f;
+    e.profile = params.emitter_profile;
+    e.strength = params.source_strength;
+    const size_t patch = size_t(e.size[0]) * e.size[1] * e.size[2];
+    if (noise_.n < patch) noise_.allocate(patch);
+    launch_emit(g, e, rng_.p, noise_.p, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, ws_.stream());
+}
+
+void Simulation::emit(float dt) {
+    if (params.source_strength <= 0.f) return;
+    emit_one(params.emitter_center_x, params.emitter_center_y, params.emitter_center_z, dt);
+    if (params.emitter_count > 1)
+        emit_one(params.emitter2_center_x, params.emitter2_center_y, params.emitter2_center_z, dt);
+}
+
+void Simulation::advect_velocity(float dt, int src, int flow, int out) {
+    for (int c = 0; c < 3; ++c)
+        ws_.advect(FACE_X + c, dt, params.cfl_mc, params.mac_cormack_vel != 0, vel_[src][c].p, vel_[flow][0].p,
+                   vel_[flow][1].p, vel_[flow][2].p, vel_[out][c].p, 1.f);
+}
+
+void Simulation::advance(float dt) {
+    const auto& p = params;
+    if (!std::isfinite(p.emitter_kick_multiplier) || p.emitter_kick_multiplier < 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "Invalid emitter kick multiplier");
+    // GpuMacSimulation3D::advance validation (GpuMacSimulation3D.cpp:226-233).
+    if (!std::isfinite(dt) || dt <= 0.f || !std::isfinite(p.source_strength) || p.source_strength < 0.f ||
+        !std::isfinite(p.emitter_radius) || p.emitter_radius <= 0.f || p.emitter_radius > 1.f ||
+        !std::isfinite(p.buoyancy) || !std::isfinite(p.smoke_decay) || p.smoke_decay < 0.f ||
+        !std::isfinite(p.sor_omega) || p.sor_omega <= 0.f || p.sor_omega >= 2.f || p.project_iterations < 0 ||
+        !std::isfinite(p.stir_strength) || !std::isfinite(p.cfl_mc) || p.cfl_mc <= 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "Invalid resident GPU step parameters");
+    if (p.use_solve_options && !valid_options(p.solve)) fail(VAPOR_INVALID_ARGUMENT, "Invalid linear solve options");
+    if (p.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && p.solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
+        fail(VAPOR_INVALID_ARGUMENT, "Unknown solver kind");
+    if (p.emitter_count < 1 || p.emitter_count > 2) fail(VAPOR_INVALID_ARGUMENT, "emitter_count must be 1 or 2");
+    const float scale = ws_.grid().h * ws_.grid().h / (p.reflection ? 0.5f * dt : dt);
+    if (!std::isfinite(scale) || scale <= 0.f) fail(VAPOR_INVALID_ARGUMENT, "Projection scale is outside the supported float range");
+
+    cudaStream_t s = ws_.stream();
+    const Grid g = ws_.grid();
+    ws_.timer().begin(VAPOR_PHASE_FORCING);
+    emit(dt);
+    launch_buoyancy_walls(g, p.buoyancy, dt, p.buoyancy_split, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
+                          vel_[S_][2].p, s);
+    ws_.timer().end(VAPOR_PHASE_FORCING, 1);
+    if (p.reflection) {
+        // MacGridFluidSolver3D::step (MacGridFluidSolver3D.cpp:192-228).
+        const float half = 0.5f * dt;
+        const auto o = solve_options(std::max(1, p.project_iterations / 2));
+        advect_velocity(half, S_, S_, T_);  // T = advected (tilde)
+        ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
+                    vel_[U_][0].p, vel_[U_][1].p, vel_[U_][2].p, half, p.sor_omega, 6.f, o,
+                    p.solver_kind);  // S = projected, U = hat
+        advect_velocity(half, U_, S_, T_);
+        ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
+                    nullptr, nullptr, nullptr, half, p.sor_omega, 6.f, o, p.solver_kind);
+    } else {
+        // MacGridFluidSolver3D::stepNoReflect (MacGridFluidSolver3D.cpp:230-245).
+        advect_velocity(dt, S_, S_, T_);
+        ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
+                    nullptr, nullptr, nullptr, dt, p.sor_omega, 6.f, solve_options(p.project_iterations),
+                    p.solver_kind);
+    }
+    // Smoke transport through the projected velocity, then dissipation
+    // (MacGridFluidSolver3D.cpp:183-190) fused as a post-scale.
+    const float factor = std::clamp(1.0f - p.smoke_decay * dt, 0.0f, 1.0f);
+    ws_.advect(CELL, dt, p.cfl_mc, p.mac_cormack_smoke != 0, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
+               vel_[S_][2].p, dens_[1 - cur_].p, factor);
+    cur_ = 1 - cur_;
+    VB_CUDA(cudaGetLastError());
+}
+
+void Simulation::upload(const float* d, const float* u, const float* v, const float* w) {
+    cudaStream_t s = ws_.stream();
+    const size_t cells = dens_[0].n, faces = vel_[0][0].n;
+    VB_CUDA(cudaMemcpyAsync(dens_[cur_].p, d, cells * sizeof(float), cudaMemcpyHostToDevice, s));
+    VB_CUDA(cudaMemcpyAsync(vel_[S_][0].p, u, faces * sizeof(float), cudaMemcpyHostToDevice, s));
+    VB_CUDA(cudaMemcpyAsync(vel_[S_][1].p, v, faces * sizeof(float), cudaMemcpyHostToDevice, s));
+    VB_CUDA(cudaMemcpyAsync(vel_[S_][2].p, w, faces * sizeof(float), cudaMemcpyHostToDevice, s));
+    VB_CUDA(cudaStreamSynchronize(s));
+    uploaded += (cells + 3 * faces) * sizeof(float);
+}
+
+void Simulation::download(float* d, float* u, float* v, float* w) {
+    cudaStream_t s = ws_.stream();
+    const size_t cells = dens_[0].n, faces = vel_[0][0].n;
+    VB_CUDA(cudaMemcpyAsync(d, dens_[cur_].p, cells * sizeof(float), cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaMemcpyAsync(u, vel_[S_][0].p, faces * sizeof(float), cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaMemcpyAsync(v, vel_[S_][1].p, faces * sizeof(float), cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaMemcpyAsync(w, vel_[S_][2].p, faces * sizeof(float), cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaStreamSynchronize(s));
+    downloaded += (cells + 3 * faces) * sizeof(float);
+}
+
+void Simulation::synchronize() { (void)ws_.last_result(); }
+
+vapor_projection_result Simulation::last_projection() { return ws_.last_result(); }
+
+void Simulation::diagnostics(vapor_fluid_diagnostics* out) {
+    ws_.diagnostics(vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, out);
+}
+
+// ---------------------------------------------------------------------------
+// Staged stages
+// ---------------------------------------------------------------------------
+Stage::Stage(int n, float box) : ws_(n, box, stream_.s) {
+    const size_t faces = size_t(n) * n * (n + 1);
+    for (auto& a : in_) a.allocate(faces);
+    for (auto& a : out_) a.allocate(faces);
+    src_.allocate(faces);
+    dst_.allocate(faces);
+}
+
+Stage::~Stage() { cudaStreamSynchronize(ws_.stream()); }
+
+void Stage::reset() {
+    ws_.reset_buffers();
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+}
+
+static bool overlaps(const float* a, size_t na, const float* b, size_t nb) {
+    if (!a || !b || na == 0 || nb == 0) return false;
+    const uintptr_t a0 = uintptr_t(a), a1 = uintptr_t(a + na), b0 = uintptr_t(b), b1 = uintptr_t(b + nb);
+    return a0 < b1 && b0 < a1;
+}
+
+// Projection3D::project contract (CpuPressureSolver3D.cpp:25-33, SOR.cpp:15-27).
+void Stage::project(float* u, float* v, float* w, const vapor_projection_options& o, float floor_diag,
+                    vapor_projection_result* result, float* pressure_out, bool device_pointers) {
+    const Grid g = ws_.grid();
+    if (!u || !v || !w) fail(VAPOR_INVALID_ARGUMENT, "Velocity fields are required");
+    if (!std::isfinite(o.relaxation) || o.relaxation <= 0.f || o.relaxation >= 2.f)
+        fail(VAPOR_INVALID_ARGUMENT, "SOR relaxation factor must be between 0 and 2");
+    if (!std::isfinite(floor_diag) || floor_diag < 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "SOR diagonal floor must be finite and nonnegative");
+    if (!std::isfinite(o.dt) || o.dt <= 0.f) fail(VAPOR_INVALID_ARGUMENT, "Projection time step must be finite and positive");
+    const float scale = g.h * g.h / o.dt;
+    if (!std::isfinite(scale) || scale <= 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "Projection scale is outside the supported float range");
+    if (!valid_options(o.linear_solve)) fail(VAPOR_INVALID_ARGUMENT, "Invalid linear solve options");
+    cudaStream_t s = ws_.stream();
+    const size_t faces = in_[0].n, bytes = faces * sizeof(float);
+    float* user[3] = {u, v, w};
+    const cudaMemcpyKind in_kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (int c = 0; c < 3; ++c) VB_CUDA(cudaMemcpyAsync(in_[c].p, user[c], bytes, in_kind, s));
+    ws_.clear_errors();
+    if (solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
+        fail(VAPOR_INVALID_ARGUMENT, "Unknown solver kind");
+    ws_.project(in_[0].p, in_[1].p, in_[2].p, out_[0].p, out_[1].p, out_[2].p, nullptr, nullptr, nullptr, o.dt,
+                o.relaxation, floor_diag, o.linear_solve, solver_kind);
+    const vapor_projection_result r = ws_.last_result();  // waits; raises on non-finite input
+    for (int c = 0; c < 3; ++c) VB_CUDA(cudaMemcpyAsync(user[c], out_[c].p, bytes, out_kind, s));
+    if (pressure_out) {
+        const size_t cells = size_t(g.n) * g.n * g.n;
+        if (device_pointers) {
+            VB_CUDA(cudaMemcpyAsync(pressure_out, ws_.pressure(), cells * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        } else {
+            VB_CUDA(cudaMemcpyAsync(pressure_out, ws_.pressure(), cells * sizeof(float), cudaMemcpyDeviceToHost, s));
+        }
+    }
+    VB_CUDA(cudaStreamSynchronize(s));
+    if (pressure_out && !device_pointers) {
+        // The solver keeps the raw iterate and its mean; the zero-mean gauge
+        // is the same FP32 subtraction the reference applies in place.
+        const float pm = ws_.host_control()->p_mean_f;
+        const size_t cells = size_t(g.n) * g.n * g.n;
+        for (size_t i = 0; i < cells; ++i) pressure_out[i] = pressure_out[i] - pm;
+    }
+    if (result) *result = r;
+}
+
+// Advection3D contract (AdvectionContext.cpp:15-67).
+void Stage::advect(int loc, float dt, float cfl, int method, const float* src, const float* fu, const float* fv,
+                   const float* fw, float* out, bool device_pointers) {
+    const Grid g = ws_.grid();
+    if (!std::isfinite(dt) || dt < 0.f || !std::isfinite(cfl) || cfl <= 0.f || !fu || !fv || !fw)
+        fail(VAPOR_INVALID_ARGUMENT, "Invalid advection time step, CFL limit, or tracer field sizes");
+    if (loc < CELL || loc > FACE_Z) fail(VAPOR_INVALID_ARGUMENT, "Invalid staggered field axis");
+    if (method != VAPOR_SEMI_LAGRANGIAN && method != VAPOR_MACCORMACK)
+        fail(VAPOR_INVALID_ARGUMENT, "Invalid advection method");
+    const size_t faces = size_t(g.n) * g.n * (g.n + 1);
+    const size_t count = count_of(g.n, loc);
+    if (!src || !out) fail(VAPOR_INVALID_ARGUMENT, "Velocity fields must match their grid layout and not overlap");
+    if (loc != CELL && overlaps(src, count, out, count))
+        fail(VAPOR_INVALID_ARGUMENT, "Velocity fields must match their grid layout and not overlap");
+    if (overlaps(out, count, fu, faces) || overlaps(out, count, fv, faces) || overlaps(out, count, fw, faces))
+        fail(VAPOR_INVALID_ARGUMENT, "Advection output must not alias tracer velocities");
+    cudaStream_t s = ws_.stream();
+    const float* flow[3] = {fu, fv, fw};
+    const float* dsrc = src;
+    const float* dflow[3] = {fu, fv, fw};
+    float* dout = out;
+    if (!device_pointers) {
+        for (int c = 0; c < 3; ++c) {
+            VB_CUDA(cudaMemcpyAsync(in_[c].p, flow[c], faces * sizeof(float), cudaMemcpyHostToDevice, s));
+            dflow[c] = in_[c].p;
+        }
+        VB_CUDA(cudaMemcpyAsync(src_.p, src, count * sizeof(float), cudaMemcpyHostToDevice, s));
+        dsrc = src_.p;
+        dout = dst_.p;
+    } else if (loc == CELL && src == out) {
+        // In-place scalar transport on device memory: stage through src_.
+        VB_CUDA(cudaMemcpyAsync(src_.p, src, count * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        dsrc = src_.p;
+    }
+    ws_.advect(loc, dt, cfl, method == VAPOR_MACCORMACK, dsrc, dflow[0], dflow[1], dflow[2], dout, 1.f);
+    if (!device_pointers) VB_CUDA(cudaMemcpyAsync(out, dst_.p, count * sizeof(float), cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace vb

@@ -1,0 +1,202 @@
+// Host-side engine of the B200 MAC 3D step: device buffers, the projection
+// orchestration, the resident coordinator (GpuMacSimulation3D's role) and the
+// staged stage plugins (GpuPressureSolver / GpuAdvection's role).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.hpp"
+
+namespace vb {
+
+// Error carried to the C ABI, where it becomes a vapor_status.
+struct Error : std::runtime_error {
+    vapor_status code;
+    Error(vapor_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void fail(vapor_status code, const std::string& message);
+void cuda_check(cudaError_t e, const char* what);
+#define VB_CUDA(call) ::vb::cuda_check((call), #call)
+
+// Owning device allocation.
+template <class T>
+struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+    void allocate(size_t count);
+    void release();
+    void zero(cudaStream_t s);
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// Owning non-blocking CUDA stream.
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream();
+    ~Stream();
+    Stream(const Stream&) = delete;
+    Stream& operator=(const Stream&) = delete;
+};
+
+// Opt-in CUDA-event timing of step phases on one stream.
+class PhaseTimer {
+public:
+    explicit PhaseTimer(cudaStream_t s) : s_(s) {}
+    ~PhaseTimer();
+    PhaseTimer(const PhaseTimer&) = delete;
+    PhaseTimer& operator=(const PhaseTimer&) = delete;
+    void enable(bool on);
+    bool enabled() const { return on_; }
+    void begin(int phase);
+    void end(int phase, long long launches);
+    void fold(bool wait);  // accumulate finished intervals
+    vapor_phase_timings totals();
+
+private:
+    cudaEvent_t take();
+    struct Pending {
+        int phase;
+        cudaEvent_t a, b;
+        long long launches;
+    };
+    cudaStream_t s_;
+    bool on_ = false;
+    std::vector<cudaEvent_t> pool_;
+    std::vector<Pending> pending_;
+    cudaEvent_t open_[VAPOR_PHASE_COUNT] = {};
+    vapor_phase_timings acc_{};
+};
+
+// Validation shared by every entry point (MacGridDomain3D.cpp:7-22).
+void validate_grid(int n, float box);
+
+// Projection workspace: b, x, MacCormack scratch, reduction partials and the
+// device control block. One per concurrent operation.
+class Workspace {
+public:
+    Workspace(int n, float box, cudaStream_t stream);
+    ~Workspace();
+    Workspace(const Workspace&) = delete;
+    Workspace& operator=(const Workspace&) = delete;
+
+    Grid grid() const { return Grid{n_, box_, box_ / float(n_)}; }
+    int n() const { return n_; }
+    float box() const { return box_; }
+    void set_box(float box) { box_ = box; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Projects (ui,vi,wi) into (uo,vo,wo) (+ hat = 2 out - in when given).
+    // Fixed-iteration solves never wait for the device; tolerance-driven
+    // solves read the stop flag after each residual check.
+    void project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo, float* uh,
+                 float* vh, float* wh, float dt, float omega, float diagonal_floor,
+                 const vapor_linear_solve_options& options, int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR);
+    void advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
+                const float* w, float* out, float post_scale);
+    // Waits for the stream and returns the last projection result; raises
+    // VAPOR_NON_FINITE if a non-finite divergence or residual was seen since
+    // the last clear_errors().
+    vapor_projection_result last_result();
+    void clear_errors();
+    void reset_buffers();
+    float* pressure() { return p_.p; }
+    ProjControl* control() { return ctrl_; }
+    const ProjControl* host_control() const { return ctrl_host_; }
+    void diagnostics(const float* u, const float* v, const float* w, vapor_fluid_diagnostics* out);
+    long long total_iterations();
+    PhaseTimer& timer() { return timer_; }
+
+private:
+    int n_;
+    float box_;
+    cudaStream_t stream_;
+    DevArray<float> b_, p_, fwd_;
+    DevArray<double> partials_;
+    DevArray<double> x64_[2];           // mixed-precision pressure (ping-pong)
+    DevArray<float> r32_;               // mixed-precision inner right-hand side
+    int partial_capacity_ = 0;
+    ProjControl* ctrl_ = nullptr;       // device
+    ProjControl* ctrl_host_ = nullptr;  // pinned mirror
+    DiagControl* diag_ = nullptr;
+    DiagControl* diag_host_ = nullptr;
+    int* done_host_ = nullptr;          // pinned
+    PhaseTimer timer_;
+    long long total_iterations_ = 0;
+    unsigned int sticky_errors_ = 0u;
+    friend class Simulation;
+};
+
+// Resident coordinator: all fields on the device across steps.
+class Simulation {
+public:
+    Simulation(int n, float box, const vapor_mac3d_params& params);
+    ~Simulation();
+    Simulation(const Simulation&) = delete;
+    Simulation& operator=(const Simulation&) = delete;
+
+    void reset();
+    void set_box(float box);
+    void advance(float dt);
+    void upload(const float* d, const float* u, const float* v, const float* w);
+    void download(float* d, float* u, float* v, float* w);
+    void synchronize();
+    vapor_projection_result last_projection();
+    void diagnostics(vapor_fluid_diagnostics* out);
+    long long total_iterations() { return ws_.total_iterations(); }
+    PhaseTimer& timer() { return ws_.timer(); }
+
+    vapor_mac3d_params params;
+    uint64_t uploaded = 0, downloaded = 0;
+    int n() const { return ws_.n(); }
+    float box() const { return ws_.box(); }
+    cudaStream_t stream() const { return ws_.stream(); }
+    float* density() { return dens_[cur_].p; }
+    float* velocity(int c) { return vel_[S_][c].p; }
+
+private:
+    void emit(float dt);
+    void emit_one(float cx, float cy, float cz, float dt);
+    void advect_velocity(float dt, int src_set, int flow_set, int out_set);
+    vapor_linear_solve_options solve_options(int iterations) const;
+
+    Stream stream_;
+    Workspace ws_;
+    DevArray<float> dens_[2];
+    DevArray<float> vel_[3][3];
+    DevArray<uint32_t> rng_;
+    DevArray<float> noise_;
+    int cur_ = 0;
+    int S_ = 0, T_ = 1, U_ = 2;
+};
+
+// Staged stage plugins on caller-owned spans (host or device).
+class Stage {
+public:
+    Stage(int n, float box);
+    ~Stage();
+    Stage(const Stage&) = delete;
+    Stage& operator=(const Stage&) = delete;
+
+    void reset();
+    int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR;
+    void project(float* u, float* v, float* w, const vapor_projection_options& options, float diagonal_floor,
+                 vapor_projection_result* result, float* pressure_out, bool device_pointers);
+    void advect(int loc, float dt, float cfl, int method, const float* src, const float* fu, const float* fv,
+                const float* fw, float* out, bool device_pointers);
+    cudaStream_t stream() const { return ws_.stream(); }
+    int n() const { return ws_.n(); }
+
+private:
+    Stream stream_;
+    Workspace ws_;
+    DevArray<float> in_[3], out_[3], src_, dst_;
+};
+
+}  // namespace vb

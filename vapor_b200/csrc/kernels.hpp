@@ -1,0 +1,140 @@
+// Host-side launch wrappers of the MAC 3D kernels (kernels_*.cu). All
+// launches are asynchronous on the given stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/vapor_b200.h"
+#include "mac3d_common.cuh"
+
+namespace vb {
+
+// Per-projection device state: reduction accumulators, loop control and the
+// assembled ProjectionResult. Lives in device memory, one per workspace.
+struct ProjControl {
+    // accumulators, cleared at the start of a projection
+    unsigned int div_before_bits;   // max |div| before, float bits
+    unsigned int div_after_bits;    // max |div| after, float bits
+    int rhs_max_key, rhs_min_key;   // order keys of max/min of b = -div*h^2/dt
+    unsigned long long res_bits;    // max |b - Ax| of the last residual pass, double bits
+    unsigned int nonfinite;         // bit 0: divergence before, bit 1: after, bit 2: solve
+    unsigned int reserved0;
+    // derived values
+    float rhs_mean_f;               // (float)(sum b / C), subtracted from b on the fly
+    float p_mean_f;                 // (float)(sum x / C), subtracted from x on the fly
+    double p_mean64;                // sum x64 / C (mixed-precision solver)
+    double removed_mean;
+    double target;                  // max(abs tol, rel tol * initial residual)
+    // loop control
+    int iterations;
+    int done;                       // 1 once the solve loop must stop
+    int max_iterations;
+    int check_interval;
+    int fixed;
+    int continue_flag;              // mirror of the graph while-condition
+    vapor_projection_result result;
+    // persistent across projections (cleared only by a workspace reset)
+    unsigned int sticky_nonfinite;  // OR of `nonfinite` over finished projections
+    unsigned int reserved1;
+    long long total_iterations;     // SOR iterations over finished projections
+};
+
+// Simulation-wide reduction outputs (diagnostics).
+struct DiagControl {
+    unsigned int max_velocity_bits;
+    unsigned int max_divergence_bits;
+    unsigned int nonfinite;
+    unsigned int reserved0;
+    double kinetic_sum;
+};
+
+// ---- forcing: emit, buoyancy, walls, decay ----
+struct EmitterBox {
+    int lo[3];
+    int size[3];
+    float ec[3];       // centre in world units
+    float erad;        // radius in world units
+    float kick;        // emitterKickMultiplier * (base + scale * strength)
+    int apply_kick;    // emitterKickMultiplier > 0
+    float stir_scale;  // stirStrength * dt * 60, applied as (r - .5) * stir * dtScale
+    float stir;        // stirStrength
+    float dt_scale;    // dt * 60
+    int profile;       // 0: density = 1, 1: smooth profile
+    float strength;    // sourceStrength
+};
+// Emitter patch [lo, lo+size) per axis, as MacGridFluidSolver3D::emit bounds it.
+void launch_emit(const Grid& g, const EmitterBox& e, uint32_t* rng_state, float* noise, float* density,
+                 float* u, float* v, float* w, cudaStream_t s);
+// w += split * (buoyancy * d_below * dt); w += split * (buoyancy * d_above * dt)
+// on interior z-faces, then zero every wall face.
+void launch_buoyancy_walls(const Grid& g, float buoyancy, float dt, float split, const float* density, float* u,
+                           float* v, float* w, cudaStream_t s);
+void launch_walls(const Grid& g, float* u, float* v, float* w, cudaStream_t s);
+
+// ---- advection ----
+// Semi-Lagrangian (fwd only) or MacCormack (fwd into `fwd`, then the limiter)
+// transport of the field at `loc`; `post_scale` multiplies every output value
+// (the smoke dissipation factor; 1 for velocity).
+void launch_advect(const Grid& g, int loc, float dt, float cfl_limit, bool maccormack, const float* src,
+                   const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
+                   cudaStream_t s);
+
+// ---- projection ----
+struct ProjectionArgs {
+    Grid g;
+    float dt;
+    float omega;
+    float diagonal_floor;
+    vapor_linear_solve_options options;
+};
+// Clear accumulators, compute b = -div(walls(u_in)) h^2/dt with its sum,
+// max/min and max |div|; then derive mean, initial residual and target.
+void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const float* w, float* b,
+                double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s);
+// One red-black colour sweep over x (parity 0 updates i+j+k even). With
+// `subtract_mean` the right-hand side is b - ctrl->rhs_mean_f, else b.
+void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
+                      bool guarded, cudaStream_t s, bool subtract_mean = true);
+// Mixed precision: x_out = x_in + e (FP64), r32 = float(b' - A x_out) with the
+// FP64 residual norm into ctrl->res_bits.
+void launch_refine_residual(const ProjectionArgs& a, const float* b, const double* x_in, const float* e,
+                            double* x_out, float* r32, ProjControl* ctrl, cudaStream_t s);
+// Mixed precision epilogue: FP64 pressure mean, final FP64 residual, float
+// pressure copy (x64 - mean) into p32 with ctrl->p_mean_f = 0.
+void launch_pressure_mean64(const ProjectionArgs& a, const double* x64, const float* b, float* p32,
+                            double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s);
+// Gradient step with the FP64 pressure (x64 - mean): the difference, scaling
+// and subtraction run in FP64, then round to FP32.
+void launch_gradient64(const ProjectionArgs& a, const double* x64, const float* u_in, const float* v_in,
+                       const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat,
+                       float* w_hat, ProjControl* ctrl, cudaStream_t s);
+// FP64 infinity norm of (b - mean_b) - A (x - mean_x) into ctrl->res_bits;
+// `final_pass` subtracts the pressure mean.
+void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,
+                     cudaStream_t s);
+// Record a residual check: iterations/final residual/converged/done.
+void launch_check(ProjControl* ctrl, int iterations_done, bool graph_conditional,
+                  unsigned long long cond_handle, cudaStream_t s);
+// Pressure mean (deterministic FP64 sum) into ctrl->p_mean_f.
+void launch_pressure_mean(const ProjectionArgs& a, const float* x, double* partials, int partial_capacity,
+                          ProjControl* ctrl, cudaStream_t s);
+// u_out = walls(u_in - dt grad(x - mean)) and max |div u_out|; when hat
+// pointers are given also hat = 2 u_out - u_in (the reflection step).
+void launch_gradient(const ProjectionArgs& a, const float* x, const float* u_in, const float* v_in,
+                     const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat,
+                     float* w_hat, ProjControl* ctrl, cudaStream_t s);
+// Assemble ctrl->result from the accumulators.
+void launch_finish_projection(ProjControl* ctrl, cudaStream_t s);
+
+// ---- diagnostics ----
+void launch_diagnostics(const Grid& g, const float* u, const float* v, const float* w, double* partials,
+                        int partial_capacity, DiagControl* diag, cudaStream_t s);
+
+int reduction_blocks(size_t count);
+
+// Number of kernels this library has launched (all handles, all threads).
+void count_launch();
+long long launch_count();
+
+}  // namespace vb

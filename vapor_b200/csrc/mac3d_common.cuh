@@ -1,0 +1,191 @@
+// Device-side building blocks of the MAC 3D step: grid indexing, the clamped
+// trilinear sampler and reduction helpers.
+//
+// Exactness contract: every FP32 expression here evaluates the same IEEE
+// operations in the same order as the reference CPU code it cites, and the
+// library is compiled with --fmad=false (no FMA contraction) and IEEE division
+// and square root. With that, results are bit-identical to the reference's CPU
+// path, which is itself compiled without FMA.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vb {
+
+// Staggered locations of a MAC grid.
+enum Loc : int { CELL = 0, FACE_X = 1, FACE_Y = 2, FACE_Z = 3 };
+
+// Cubic grid: n cells per side, box size and cell size h = box / n
+// (MacGridDomain3D::cellSize, MacGridDomain3D.hpp:20).
+struct Grid {
+    int n;
+    float box;
+    float h;
+};
+
+__host__ __device__ inline int extent(int n, int loc, int dim) { return n + (loc == dim + 1 ? 1 : 0); }
+
+// idC/idX/idY/idZ (MacGridDomain3D.hpp:22-31): x fastest.
+__host__ __device__ inline size_t index_of(int n, int loc, int x, int y, int z) {
+    return size_t(x) + size_t(extent(n, loc, 0)) * (size_t(y) + size_t(extent(n, loc, 1)) * size_t(z));
+}
+
+__host__ __device__ inline size_t count_of(int n, int loc) {
+    return size_t(extent(n, loc, 0)) * size_t(extent(n, loc, 1)) * size_t(extent(n, loc, 2));
+}
+
+__device__ __forceinline__ float clampf_ref(float v, float lo, float hi) {
+    // std::clamp(v, lo, hi) == v < lo ? lo : (hi < v ? hi : v)
+    return v < lo ? lo : (hi < v ? hi : v);
+}
+__device__ __forceinline__ int clampi_ref(int v, int lo, int hi) { return v < lo ? lo : (hi < v ? hi : v); }
+__device__ __forceinline__ float minf_ref(float a, float b) { return b < a ? b : a; }  // std::min
+__device__ __forceinline__ float maxf_ref(float a, float b) { return a < b ? b : a; }  // std::max
+
+// One axis of the clamped trilinear lookup (MacGridSampler3D.cpp:6-11 and the
+// staggered variants :23-28, :42-47, :61-66).
+struct Bracket {
+    int i0, i1;
+    float t;
+};
+
+template <bool STAGGERED>
+__device__ __forceinline__ Bracket bracket(float coord, float h, int n) {
+    Bracket b;
+    if (STAGGERED) {
+        const float g = clampf_ref(coord / h, 0.f, float(n));
+        b.i0 = min(int(g), n - 1);
+        b.i1 = b.i0 + 1;
+        b.t = g - float(b.i0);
+    } else {
+        const float g = clampf_ref(coord / h - 0.5f, 0.f, float(n - 1));
+        b.i0 = int(g);
+        b.i1 = min(b.i0 + 1, n - 1);
+        b.t = g - float(b.i0);
+    }
+    return b;
+}
+
+// Trilinear sample of a field at location LOC, world position (px,py,pz), with
+// the reference's fixed 8-term order and left-to-right products.
+template <int LOC>
+__device__ __forceinline__ float sample(const float* __restrict__ f, int n, float h, float px, float py,
+                                        float pz) {
+    const Bracket bx = bracket<LOC == FACE_X>(px, h, n);
+    const Bracket by = bracket<LOC == FACE_Y>(py, h, n);
+    const Bracket bz = bracket<LOC == FACE_Z>(pz, h, n);
+    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
+    const size_t r00 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i0));
+    const size_t r10 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i0));
+    const size_t r01 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i1));
+    const size_t r11 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i1));
+    const float f000 = __ldg(f + r00 + bx.i0), f100 = __ldg(f + r00 + bx.i1);
+    const float f010 = __ldg(f + r10 + bx.i0), f110 = __ldg(f + r10 + bx.i1);
+    const float f001 = __ldg(f + r01 + bx.i0), f101 = __ldg(f + r01 + bx.i1);
+    const float f011 = __ldg(f + r11 + bx.i0), f111 = __ldg(f + r11 + bx.i1);
+    const float tx = bx.t, ty = by.t, tz = bz.t;
+    const float ux = 1.f - tx, uy = 1.f - ty, uz = 1.f - tz;
+    float s = f000 * ux * uy * uz;
+    s = s + f100 * tx * uy * uz;
+    s = s + f010 * ux * ty * uz;
+    s = s + f110 * tx * ty * uz;
+    s = s + f001 * ux * uy * tz;
+    s = s + f101 * tx * uy * tz;
+    s = s + f011 * ux * ty * tz;
+    s = s + f111 * tx * ty * tz;
+    return s;
+}
+
+struct Vel {
+    float x, y, z;
+};
+
+// MacGridSampler3D::velocity (MacGridSampler3D.cpp:73-75).
+__device__ __forceinline__ Vel velocity_at(const float* __restrict__ u, const float* __restrict__ v,
+                                           const float* __restrict__ w, int n, float h, float px, float py,
+                                           float pz) {
+    Vel r;
+    r.x = sample<FACE_X>(u, n, h, px, py, pz);
+    r.y = sample<FACE_Y>(v, n, h, px, py, pz);
+    r.z = sample<FACE_Z>(w, n, h, px, py, pz);
+    return r;
+}
+
+// ---- reductions -------------------------------------------------------------
+
+// Non-negative floats/doubles order like their bit patterns as unsigned ints,
+// so atomicMax on the bits is an exact, order-independent max.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned int* addr, float value) {
+    atomicMax(addr, __float_as_uint(value));
+}
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double value) {
+    atomicMax(addr, (unsigned long long)__double_as_longlong(value));
+}
+
+// Total order key for signed floats (for max and min of signed values).
+__device__ __forceinline__ int float_order_key(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : (i ^ 0x7fffffff);
+}
+__host__ __device__ inline float key_to_float(int k) {
+    const int i = k >= 0 ? k : (k ^ 0x7fffffff);
+#ifdef __CUDA_ARCH__
+    return __int_as_float(i);
+#else
+    float f;
+    __builtin_memcpy(&f, &i, sizeof f);
+    return f;
+#endif
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T other = __shfl_xor_sync(0xffffffffu, v, o);
+        v = v < other ? other : v;
+    }
+    return v;
+}
+
+// Deterministic block sum (fixed tree: warp shuffles, then warp 0).
+// `scratch` holds at least 32 T. Result valid in thread 0.
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = T(0);
+    if (warp == 0) {
+        r = lane < warps ? scratch[lane] : T(0);
+        r = warp_sum(r);
+    }
+    return r;
+}
+template <class T>
+__device__ __forceinline__ T block_max(T v, T* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = (blockDim.x + 31) >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = T(0);
+    if (warp == 0) {
+        r = lane < warps ? scratch[lane] : scratch[0];  // pad with a real entry, not 0
+        r = warp_max(r);
+    }
+    return r;
+}
+
+}  // namespace vb
