@@ -283,8 +283,8 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sim.set_timing(True)
-    launches0 = vb.kernel_launch_count()
+    # Timed region: every step is one CUDA-graph launch (solve loops are
+    # device-side while-nodes); the state is far larger than L2.
     clocks.start()
     wall0 = time.perf_counter()
     start.record(stream)
@@ -294,11 +294,8 @@ def main():
     end.synchronize()
     wall = time.perf_counter() - wall0
     clock_info = clocks.stop()
-    launches = vb.kernel_launch_count() - launches0
     torch.cuda.synchronize()
     ms = start.elapsed_time(end)
-    phases = sim.timings()
-    sim.set_timing(False)
     sweeps = sim.total_iterations() - it0
     result = sim.last_projection()
     rel = result.linear_solve.final_residual / max(result.linear_solve.initial_residual, 1e-300)
@@ -307,6 +304,19 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
+
+    # Roofline region: the same steps on the eager path with per-phase CUDA
+    # events on the simulation's stream; counts this library's kernel launches.
+    sim.set_timing(True)
+    launches0 = vb.kernel_launch_count()
+    roof_steps = max(1, min(args.steps, 2))
+    for _ in range(roof_steps):
+        sim.advance(DT)
+    sim.synchronize()
+    launches_per_step = (vb.kernel_launch_count() - launches0) / roof_steps
+    phases = sim.timings()
+    sim.set_timing(False)
+    launches = int(round(launches_per_step * args.steps))
 
     # End to end through the public API: pinned host state in, step, state out.
     pinned = [torch.empty(a.shape, dtype=torch.float32, pin_memory=True).numpy() for a in fields]
@@ -349,11 +359,12 @@ def main():
                    "final_relative_residual": rel, "converged": bool(result.linear_solve.converged),
                    "l2": "state (4 x 67 MB fields) and solver buffers exceed the 126 MB L2",
                    "parallelism": f"replicas{world}"},
-        "gpu_launches": int(launches),
+        "gpu_launches": launches,
+        "gpu_launches_note": "kernels per step counted on the eager replay of the same step, times steps",
         "roofline": {"bound": "hbm", "kernel": "k_sor_color", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                      "bytes_per_launch": sor_bytes, "avg_launch_us": sor_launch_ms * 1e3},
-        "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in phases.items()},
+        "phases_ms_per_step": {k: v["ms"] / roof_steps for k, v in phases.items()},
         "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},
         "clocks": clock_info, "wall_s": wall,

@@ -455,3 +455,29 @@ def test_mixed_refinement_reaches_tolerance_plain_fp32_cannot():
     r_mixed, _ = mixed.project(*[a.copy() for a in (u, v, w)], ProjectionOptions(0.005, 1.95, opts), 6.0)
     assert not r_plain.linear_solve.converged
     assert r_mixed.linear_solve.converged and r_mixed.linear_solve.iterations < 3000
+
+
+@pytest.mark.parametrize("mode", ["fixed", "tolerance", "mixed"])
+def test_graph_replay_equals_eager_steps(mode):
+    """Whole-step CUDA graphs (solve loops as device-side while nodes) give the
+    same bits and iteration counts as the host-driven eager path."""
+    p = algorithm_params(3)
+    p.project_iterations, p.stir_strength = 30, 0.5
+    if mode != "fixed":
+        p.use_solve_options = 1
+        p.solve = LinearSolveOptions.defaults(max_iterations=3000, relative_tolerance=1e-5 if mode == "tolerance"
+                                              else 1e-7, absolute_tolerance=0.0)
+        p.solver_kind = vb.abi.SOLVER_MIXED_REFINEMENT if mode == "mixed" else vb.abi.SOLVER_RED_BLACK_SOR
+    graph = vb.MacSimulation3D(24, 1.0, p)
+    eager = vb.MacSimulation3D(24, 1.0, p)
+    eager.set_timing(True)  # phase timing runs the eager path
+    for _ in range(3):
+        graph.advance(0.01)
+        eager.advance(0.01)
+        assert graph.last_projection().linear_solve.iterations == eager.last_projection().linear_solve.iterations
+    for a, b in zip(graph.download(), eager.download()):
+        assert bits_equal(a, b)
+    assert graph.total_iterations() == eager.total_iterations()
+    r = graph.last_projection()
+    if mode == "mixed":
+        assert r.linear_solve.converged and r.linear_solve.final_residual <= 1e-7 * r.linear_solve.initial_residual

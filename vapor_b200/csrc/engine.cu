@@ -142,10 +142,10 @@ vapor_phase_timings PhaseTimer::totals() {
 Workspace::Workspace(int n, float box, cudaStream_t stream)
     : n_(n), box_(box), stream_(stream), timer_(stream) {
     validate_grid(n, box);
-    const size_t cells = size_t(n) * n * n;
     const size_t faces = size_t(n) * n * (n + 1);
-    b_.allocate(cells);
-    p_.allocate(cells);
+    const size_t slots = rb_count(n);  // red-black split storage
+    b_.allocate(slots);
+    p_.allocate(slots);
     fwd_.allocate(faces);
     partial_capacity_ = reduction_blocks(faces);
     partials_.allocate(size_t(partial_capacity_));
@@ -188,77 +188,158 @@ void Workspace::advect(int loc, float dt, float cfl, bool maccormack, const floa
     VB_CUDA(cudaGetLastError());
 }
 
+void Workspace::ensure_mixed() {
+    const size_t cells = rb_count(n_);
+    for (auto& x : x64_)
+        if (x.n != cells) x.allocate(cells);
+    if (r32_.n != cells) r32_.allocate(cells);
+}
+
+// Adds a while-loop node at the current capture position of stream `s` whose
+// body is recorded by `body` on the workspace's body stream. The loop runs
+// while the handle's value (set by a kernel before the node and by the body's
+// last kernel) is nonzero.
+template <class Body>
+static void add_while_loop(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditionalHandle handle,
+                           Body&& body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    VB_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps));
+    if (status != cudaStreamCaptureStatusActive) fail(VAPOR_RUNTIME_ERROR, "stream is not capturing");
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    VB_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+    VB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body_graph = params.conditional.phGraph_out[0];
+    VB_CUDA(cudaStreamBeginCaptureToGraph(body_stream, body_graph, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    body(body_stream);
+    cudaGraph_t captured = nullptr;
+    VB_CUDA(cudaStreamEndCapture(body_stream, &captured));
+}
+
+static cudaGraphConditionalHandle new_condition(cudaStream_t s) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph;
+    VB_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, nullptr, nullptr));
+    if (status != cudaStreamCaptureStatusActive) fail(VAPOR_RUNTIME_ERROR, "stream is not capturing");
+    cudaGraphConditionalHandle h;
+    VB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    return h;
+}
+
 void Workspace::project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo,
                         float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
                         const vapor_linear_solve_options& o, int solver_kind) {
     const ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
     cudaStream_t s = stream_;
     PhaseTimer& t = timer_;
-    t.begin(VAPOR_PHASE_RHS);
-    launch_rhs(a, ui, vi, wi, b_.p, partials_.p, partial_capacity_, ctrl_, s);
-    p_.zero(s);
-    t.end(VAPOR_PHASE_RHS, 3);
+    const bool mixed = solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT;
+    const bool graph = capturing_;
+    const int interval = o.residual_check_interval;
+    if (mixed) ensure_mixed();
+    LoopCond cond;
+    cudaGraphConditionalHandle handle = 0;
+    if (graph) {
+        handle = new_condition(s);
+        cond.active = 1;
+        cond.handle = (unsigned long long)handle;
+    }
     auto wait_done = [&]() {
         VB_CUDA(cudaMemcpyAsync(done_host_, &ctrl_->done, sizeof(int), cudaMemcpyDeviceToHost, s));
         VB_CUDA(cudaStreamSynchronize(s));
         t.fold(false);
         return *done_host_ != 0;
     };
-    auto sweeps = [&](int k, float* x, const float* rhs, bool guarded, bool subtract_mean) {
+    // k guarded colour-pair sweeps on x (right-hand side rhs) on stream st.
+    auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean) {
         t.begin(VAPOR_PHASE_SOR);
         for (int j = 0; j < k; ++j) {
-            launch_sor_color(a, 0, x, rhs, ctrl_, guarded, s, subtract_mean);
-            launch_sor_color(a, 1, x, rhs, ctrl_, guarded, s, subtract_mean);
+            launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st);
+            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st);
         }
         t.end(VAPOR_PHASE_SOR, 2LL * k);
     };
-    if (solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT) {
+
+    t.begin(VAPOR_PHASE_RHS);
+    LoopCond rhs_cond = cond;
+    if (mixed) rhs_cond.active = 0;  // the mixed loop is decided by its first re-centring pass
+    launch_rhs(a, ui, vi, wi, b_.p, partials_.p, partial_capacity_, ctrl_, mixed ? x64_[0].p : nullptr,
+               mixed ? x64_[1].p : nullptr, rhs_cond, s);
+    VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), s));
+    t.end(VAPOR_PHASE_RHS, 3);
+
+    if (mixed) {
         // FP32 red-black sweeps on the error equation, re-centred in FP64 at
-        // every residual check (see the oracle's refinementSolve).
-        const size_t cells = b_.n;
-        for (auto& x : x64_)
-            if (x.n != cells) x.allocate(cells);
-        if (r32_.n != cells) r32_.allocate(cells);
-        x64_[0].zero(s);
-        int cur = 0, it = 0;
-        for (;;) {
+        // every residual check (the oracle's refinementSolve).
+        VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
+        auto recentre = [&](cudaStream_t st, int done_sweeps, bool accumulate) {
             t.begin(VAPOR_PHASE_RESIDUAL);
-            launch_refine_residual(a, b_.p, x64_[cur].p, p_.p, x64_[1 - cur].p, r32_.p, ctrl_, s);
-            cur = 1 - cur;
-            launch_check(ctrl_, it, false, 0ull, s);
-            t.end(VAPOR_PHASE_RESIDUAL, 1);
-            if (wait_done()) break;
-            p_.zero(s);
-            const int k = std::min(o.residual_check_interval - it % o.residual_check_interval, o.max_iterations - it);
-            sweeps(k, p_.p, r32_.p, false, false);
-            it += k;
+            launch_refine_residual(a, b_.p, p_.p, r32_.p, ctrl_, st);
+            launch_check(ctrl_, done_sweeps, accumulate, true, cond, st);
+            t.end(VAPOR_PHASE_RESIDUAL, 2);
+        };
+        const int chunk = std::max(1, std::min(interval, o.max_iterations));
+        if (graph) {
+            recentre(s, 0, false);
+            add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) {
+                VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), bs));
+                sweeps(bs, chunk, 0, p_.p, r32_.p, false);
+                recentre(bs, chunk, true);
+            });
+        } else {
+            int it = 0;
+            recentre(s, 0, false);
+            while (!wait_done()) {
+                VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), s));
+                const int k = std::min(interval - it % interval, o.max_iterations - it);
+                sweeps(s, k, 0, p_.p, r32_.p, false);
+                it += k;
+                recentre(s, k, true);
+            }
         }
         t.begin(VAPOR_PHASE_GRADIENT);
-        launch_pressure_mean64(a, x64_[cur].p, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
-        launch_gradient64(a, x64_[cur].p, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
+        launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
         t.end(VAPOR_PHASE_GRADIENT, 5);
     } else {
-        if (o.max_iterations > 0) {
-            if (o.fixed_iterations) {
-                // Intermediate residual checks cannot change a fixed-budget
-                // solve: the final residual and convergence are recomputed
-                // after the pressure gauge (CpuPressureSolver3D.cpp:50-56).
-                sweeps(o.max_iterations, p_.p, b_.p, true, true);
-                launch_check(ctrl_, o.max_iterations, false, 0ull, s);
+        if (o.fixed_iterations) {
+            // Intermediate residual checks cannot change a fixed-budget solve:
+            // the final residual and convergence are recomputed after the
+            // pressure gauge (CpuPressureSolver3D.cpp:50-56).
+            if (graph && o.max_iterations > interval) {
+                add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) {
+                    sweeps(bs, interval, 0, p_.p, b_.p, true);
+                    launch_check(ctrl_, interval, true, false, cond, bs);
+                });
             } else {
-                int it = 0;
-                bool stop = wait_done();
-                while (!stop && it < o.max_iterations) {
-                    const int to_check = o.residual_check_interval - it % o.residual_check_interval;
-                    const int k = std::min(to_check, o.max_iterations - it);
-                    sweeps(k, p_.p, b_.p, false, true);
-                    it += k;
-                    t.begin(VAPOR_PHASE_RESIDUAL);
-                    launch_residual(a, p_.p, b_.p, ctrl_, false, s);
-                    launch_check(ctrl_, it, false, 0ull, s);
-                    t.end(VAPOR_PHASE_RESIDUAL, 1);
-                    stop = wait_done();
-                }
+                sweeps(s, o.max_iterations, 0, p_.p, b_.p, true);
+                launch_check(ctrl_, o.max_iterations, false, false, LoopCond{}, s);
+            }
+        } else if (graph) {
+            add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) {
+                sweeps(bs, interval, 0, p_.p, b_.p, true);
+                launch_residual(a, p_.p, b_.p, ctrl_, false, bs);
+                launch_check(ctrl_, interval, true, false, cond, bs);
+            });
+        } else {
+            int it = 0;
+            bool stop = wait_done();
+            while (!stop && it < o.max_iterations) {
+                const int k = std::min(interval - it % interval, o.max_iterations - it);
+                sweeps(s, k, 0, p_.p, b_.p, true);
+                it += k;
+                t.begin(VAPOR_PHASE_RESIDUAL);
+                launch_residual(a, p_.p, b_.p, ctrl_, false, s);
+                launch_check(ctrl_, k, true, false, LoopCond{}, s);
+                t.end(VAPOR_PHASE_RESIDUAL, 2);
+                stop = wait_done();
             }
         }
         t.begin(VAPOR_PHASE_GRADIENT);
@@ -313,7 +394,10 @@ Simulation::Simulation(int n, float box, const vapor_mac3d_params& p) : params(p
     VB_CUDA(cudaStreamSynchronize(ws_.stream()));
 }
 
-Simulation::~Simulation() { cudaStreamSynchronize(ws_.stream()); }
+Simulation::~Simulation() {
+    cudaStreamSynchronize(ws_.stream());
+    release_graphs();
+}
 
 void Simulation::reset() {
     cudaStream_t s = ws_.stream();
@@ -353,12 +437,12 @@ vapor_linear_solve_options Simulation::solve_options(int iterations) const {
 }
 
 // Emitter patch of MacGridFluidSolver3D::emit (MacGridFluidSolver3D.cpp:140-147),
-// computed in the same FP32 operations.
-void Simulation::emit_one(float cxf, float cyf, float czf, float dt) {
+// computed in the same FP32 operations. Returns false for an empty patch.
+bool Simulation::emitter_box(float cxf, float cyf, float czf, float dt, EmitterBox& e) const {
     const Grid g = ws_.grid();
     const float dx = g.h;
     const float box = g.box;
-    EmitterBox e{};
+    e = EmitterBox{};
     e.ec[0] = cxf * box;
     e.ec[1] = cyf * box;
     e.ec[2] = czf * box;
@@ -369,23 +453,28 @@ void Simulation::emit_one(float cxf, float cyf, float czf, float dt) {
         e.lo[a] = std::max(0, c - R);
         e.size[a] = std::min(g.n, c + R) - e.lo[a];
     }
-    if (e.size[0] <= 0 || e.size[1] <= 0 || e.size[2] <= 0) return;
+    if (e.size[0] <= 0 || e.size[1] <= 0 || e.size[2] <= 0) return false;
     e.kick = params.emitter_kick_multiplier * (params.emitter_kick_base + params.emitter_kick_scale * params.source_strength);
     e.apply_kick = params.emitter_kick_multiplier > 0.f;
     e.stir = params.stir_strength;
     e.dt_scale = dt * 60.0f;
     e.profile = params.emitter_profile;
     e.strength = params.source_strength;
-    const size_t patch = size_t(e.size[0]) * e.size[1] * e.size[2];
-    if (noise_.n < patch) noise_.allocate(patch);
-    launch_emit(g, e, rng_.p, noise_.p, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, ws_.stream());
+    return true;
 }
 
 void Simulation::emit(float dt) {
     if (params.source_strength <= 0.f) return;
-    emit_one(params.emitter_center_x, params.emitter_center_y, params.emitter_center_z, dt);
-    if (params.emitter_count > 1)
-        emit_one(params.emitter2_center_x, params.emitter2_center_y, params.emitter2_center_z, dt);
+    const float centres[2][3] = {{params.emitter_center_x, params.emitter_center_y, params.emitter_center_z},
+                                 {params.emitter2_center_x, params.emitter2_center_y, params.emitter2_center_z}};
+    for (int k = 0; k < params.emitter_count; ++k) {
+        EmitterBox e;
+        if (!emitter_box(centres[k][0], centres[k][1], centres[k][2], dt, e)) continue;
+        const size_t patch = size_t(e.size[0]) * e.size[1] * e.size[2];
+        if (noise_.n < patch) fail(VAPOR_RUNTIME_ERROR, "emitter scratch not prepared");
+        launch_emit(ws_.grid(), e, rng_.p, noise_.p, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
+                    ws_.stream());
+    }
 }
 
 void Simulation::advect_velocity(float dt, int src, int flow, int out) {
@@ -394,7 +483,7 @@ void Simulation::advect_velocity(float dt, int src, int flow, int out) {
                    vel_[flow][1].p, vel_[flow][2].p, vel_[out][c].p, 1.f);
 }
 
-void Simulation::advance(float dt) {
+void Simulation::validate_step(float dt) const {
     const auto& p = params;
     if (!std::isfinite(p.emitter_kick_multiplier) || p.emitter_kick_multiplier < 0.f)
         fail(VAPOR_INVALID_ARGUMENT, "Invalid emitter kick multiplier");
@@ -409,9 +498,16 @@ void Simulation::advance(float dt) {
     if (p.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && p.solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
         fail(VAPOR_INVALID_ARGUMENT, "Unknown solver kind");
     if (p.emitter_count < 1 || p.emitter_count > 2) fail(VAPOR_INVALID_ARGUMENT, "emitter_count must be 1 or 2");
+    if (p.emitter_profile < 0 || p.emitter_profile > 1) fail(VAPOR_INVALID_ARGUMENT, "emitter_profile must be 0 or 1");
     const float scale = ws_.grid().h * ws_.grid().h / (p.reflection ? 0.5f * dt : dt);
-    if (!std::isfinite(scale) || scale <= 0.f) fail(VAPOR_INVALID_ARGUMENT, "Projection scale is outside the supported float range");
+    if (!std::isfinite(scale) || scale <= 0.f)
+        fail(VAPOR_INVALID_ARGUMENT, "Projection scale is outside the supported float range");
+}
 
+// One step of MacGridFluidSolver3D::step / stepNoReflect on the device,
+// reading density from dens_[cur_] and writing dens_[1 - cur_].
+void Simulation::record_step(float dt) {
+    const auto& p = params;
     cudaStream_t s = ws_.stream();
     const Grid g = ws_.grid();
     ws_.timer().begin(VAPOR_PHASE_FORCING);
@@ -442,8 +538,71 @@ void Simulation::advance(float dt) {
     const float factor = std::clamp(1.0f - p.smoke_decay * dt, 0.0f, 1.0f);
     ws_.advect(CELL, dt, p.cfl_mc, p.mac_cormack_smoke != 0, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
                vel_[S_][2].p, dens_[1 - cur_].p, factor);
+}
+
+void Simulation::release_graphs() {
+    for (auto& g : graphs_) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+}
+
+void Simulation::advance(float dt) {
+    validate_step(dt);
+    // Scratch that a captured step needs is allocated before any capture.
+    {
+        const float centres[2][3] = {{params.emitter_center_x, params.emitter_center_y, params.emitter_center_z},
+                                     {params.emitter2_center_x, params.emitter2_center_y, params.emitter2_center_z}};
+        size_t need = 0;
+        for (int k = 0; k < params.emitter_count; ++k) {
+            EmitterBox e;
+            if (emitter_box(centres[k][0], centres[k][1], centres[k][2], dt, e))
+                need = std::max(need, size_t(e.size[0]) * e.size[1] * e.size[2]);
+        }
+        if (noise_.n < need) {
+            VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+            release_graphs();
+            noise_.allocate(need);
+        }
+        if (params.solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT) ws_.ensure_mixed();
+    }
+    cudaStream_t s = ws_.stream();
+    if (!use_graphs_ || ws_.timer().enabled()) {
+        record_step(dt);
+        cur_ = 1 - cur_;
+        VB_CUDA(cudaGetLastError());
+        return;
+    }
+    CachedGraph& slot = graphs_[cur_];
+    GraphKey key{};
+    key.dt = dt;
+    key.box = ws_.box();
+    key.params = params;
+    if (!slot.exec || std::memcmp(&slot.key, &key, sizeof(GraphKey)) != 0) {
+        if (slot.exec) {
+            cudaGraphExecDestroy(slot.exec);
+            slot.exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        VB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        ws_.set_capturing(true);
+        try {
+            record_step(dt);
+        } catch (...) {
+            ws_.set_capturing(false);
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        ws_.set_capturing(false);
+        VB_CUDA(cudaStreamEndCapture(s, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        VB_CUDA(e);
+        slot.key = key;
+    }
+    VB_CUDA(cudaGraphLaunch(slot.exec, s));
     cur_ = 1 - cur_;
-    VB_CUDA(cudaGetLastError());
 }
 
 void Simulation::upload(const float* d, const float* u, const float* v, const float* w) {
@@ -528,21 +687,16 @@ void Stage::project(float* u, float* v, float* w, const vapor_projection_options
     const vapor_projection_result r = ws_.last_result();  // waits; raises on non-finite input
     for (int c = 0; c < 3; ++c) VB_CUDA(cudaMemcpyAsync(user[c], out_[c].p, bytes, out_kind, s));
     if (pressure_out) {
+        // Zero-mean pressure in natural order (the reference subtracts the
+        // mean in place; the same FP32 subtraction happens on the device).
         const size_t cells = size_t(g.n) * g.n * g.n;
-        if (device_pointers) {
-            VB_CUDA(cudaMemcpyAsync(pressure_out, ws_.pressure(), cells * sizeof(float), cudaMemcpyDeviceToDevice, s));
-        } else {
-            VB_CUDA(cudaMemcpyAsync(pressure_out, ws_.pressure(), cells * sizeof(float), cudaMemcpyDeviceToHost, s));
-        }
+        float* natural = device_pointers ? pressure_out : dst_.p;
+        launch_unsplit_pressure(g, ws_.pressure(), ws_.control(), natural, s);
+        VB_CUDA(cudaGetLastError());
+        if (!device_pointers)
+            VB_CUDA(cudaMemcpyAsync(pressure_out, natural, cells * sizeof(float), cudaMemcpyDeviceToHost, s));
     }
     VB_CUDA(cudaStreamSynchronize(s));
-    if (pressure_out && !device_pointers) {
-        // The solver keeps the raw iterate and its mean; the zero-mean gauge
-        // is the same FP32 subtraction the reference applies in place.
-        const float pm = ws_.host_control()->p_mean_f;
-        const size_t cells = size_t(g.n) * g.n * g.n;
-        for (size_t i = 0; i < cells; ++i) pressure_out[i] = pressure_out[i] - pm;
-    }
     if (result) *result = r;
 }
 

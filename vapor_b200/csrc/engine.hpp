@@ -112,6 +112,10 @@ public:
     void diagnostics(const float* u, const float* v, const float* w, vapor_fluid_diagnostics* out);
     long long total_iterations();
     PhaseTimer& timer() { return timer_; }
+    void ensure_mixed();
+    // While true, project() records CUDA-graph nodes (the solve loops become
+    // conditional while nodes) instead of driving the loop from the host.
+    void set_capturing(bool on) { capturing_ = on; }
 
 private:
     int n_;
@@ -128,6 +132,8 @@ private:
     DiagControl* diag_host_ = nullptr;
     int* done_host_ = nullptr;          // pinned
     PhaseTimer timer_;
+    Stream body_stream_;                // records conditional-loop bodies
+    bool capturing_ = false;
     long long total_iterations_ = 0;
     unsigned int sticky_errors_ = 0u;
     friend class Simulation;
@@ -138,6 +144,7 @@ class Simulation {
 public:
     Simulation(int n, float box, const vapor_mac3d_params& params);
     ~Simulation();
+    void release_graphs();
     Simulation(const Simulation&) = delete;
     Simulation& operator=(const Simulation&) = delete;
 
@@ -160,11 +167,29 @@ public:
     float* density() { return dens_[cur_].p; }
     float* velocity(int c) { return vel_[S_][c].p; }
 
+    // CUDA-graph replay of whole steps (default on; phase timing uses the
+    // eager path).
+    void set_graphs(bool on) { use_graphs_ = on; }
+
 private:
+    bool emitter_box(float cx, float cy, float cz, float dt, EmitterBox& e) const;
     void emit(float dt);
-    void emit_one(float cx, float cy, float cz, float dt);
     void advect_velocity(float dt, int src_set, int flow_set, int out_set);
+    void record_step(float dt);
+    void validate_step(float dt) const;
     vapor_linear_solve_options solve_options(int iterations) const;
+
+    struct GraphKey {
+        float dt;
+        float box;
+        vapor_mac3d_params params;
+    };
+    struct CachedGraph {
+        GraphKey key{};
+        cudaGraphExec_t exec = nullptr;
+    };
+    CachedGraph graphs_[2];
+    bool use_graphs_ = true;
 
     Stream stream_;
     Workspace ws_;

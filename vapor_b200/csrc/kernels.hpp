@@ -33,6 +33,9 @@ struct ProjControl {
     int check_interval;
     int fixed;
     int continue_flag;              // mirror of the graph while-condition
+    int x64_cur;                    // mixed precision: index of the current FP64 pressure
+    int reserved2;
+    double* x64[2];                 // mixed precision: FP64 pressure ping-pong buffers
     vapor_projection_result result;
     // persistent across projections (cleared only by a workspace reset)
     unsigned int sticky_nonfinite;  // OR of `nonfinite` over finished projections
@@ -88,34 +91,47 @@ struct ProjectionArgs {
     float diagonal_floor;
     vapor_linear_solve_options options;
 };
+// Graph while-loop control: when `active`, kernels that decide whether the
+// solve continues also set this conditional handle.
+struct LoopCond {
+    int active = 0;
+    unsigned long long handle = 0;
+};
 // Clear accumulators, compute b = -div(walls(u_in)) h^2/dt with its sum,
 // max/min and max |div|; then derive mean, initial residual and target.
+// x64a/x64b are the mixed-precision buffers (may be null).
 void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const float* w, float* b,
-                double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s);
+                double* partials, int partial_capacity, ProjControl* ctrl, double* x64a, double* x64b,
+                LoopCond cond, cudaStream_t s);
 // One red-black colour sweep over x (parity 0 updates i+j+k even). With
-// `subtract_mean` the right-hand side is b - ctrl->rhs_mean_f, else b.
+// `subtract_mean` the right-hand side is b - ctrl->rhs_mean_f, else b. A
+// guarded sweep returns at once when the solve is done or when
+// ctrl->iterations + sweep_index reaches the iteration budget.
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, cudaStream_t s, bool subtract_mean = true);
-// Mixed precision: x_out = x_in + e (FP64), r32 = float(b' - A x_out) with the
-// FP64 residual norm into ctrl->res_bits.
-void launch_refine_residual(const ProjectionArgs& a, const float* b, const double* x_in, const float* e,
-                            double* x_out, float* r32, ProjControl* ctrl, cudaStream_t s);
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s);
+// Mixed precision: x64[1-cur] = x64[cur] + e (FP64), r32 = float(b' - A x)
+// with the FP64 residual norm into ctrl->res_bits.
+void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
+                            ProjControl* ctrl, cudaStream_t s);
 // Mixed precision epilogue: FP64 pressure mean, final FP64 residual, float
 // pressure copy (x64 - mean) into p32 with ctrl->p_mean_f = 0.
-void launch_pressure_mean64(const ProjectionArgs& a, const double* x64, const float* b, float* p32,
-                            double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s);
+void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
+                            int partial_capacity, ProjControl* ctrl, cudaStream_t s);
 // Gradient step with the FP64 pressure (x64 - mean): the difference, scaling
 // and subtraction run in FP64, then round to FP32.
-void launch_gradient64(const ProjectionArgs& a, const double* x64, const float* u_in, const float* v_in,
-                       const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat,
-                       float* w_hat, ProjControl* ctrl, cudaStream_t s);
+void launch_gradient64(const ProjectionArgs& a, const float* u_in, const float* v_in, const float* w_in,
+                       float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat, float* w_hat,
+                       ProjControl* ctrl, cudaStream_t s);
 // FP64 infinity norm of (b - mean_b) - A (x - mean_x) into ctrl->res_bits;
 // `final_pass` subtracts the pressure mean.
 void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,
                      cudaStream_t s);
-// Record a residual check: iterations/final residual/converged/done.
-void launch_check(ProjControl* ctrl, int iterations_done, bool graph_conditional,
-                  unsigned long long cond_handle, cudaStream_t s);
+// Record a residual check: iterations/final residual/converged/done. With
+// `accumulate` the iteration count grows by min(iterations, budget left),
+// else it is set to `iterations`. `flip_x64` swaps the mixed-precision
+// buffers (after a re-centring pass).
+void launch_check(ProjControl* ctrl, int iterations, bool accumulate, bool flip_x64, LoopCond cond,
+                  cudaStream_t s);
 // Pressure mean (deterministic FP64 sum) into ctrl->p_mean_f.
 void launch_pressure_mean(const ProjectionArgs& a, const float* x, double* partials, int partial_capacity,
                           ProjControl* ctrl, cudaStream_t s);
@@ -124,6 +140,8 @@ void launch_pressure_mean(const ProjectionArgs& a, const float* x, double* parti
 void launch_gradient(const ProjectionArgs& a, const float* x, const float* u_in, const float* v_in,
                      const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat,
                      float* w_hat, ProjControl* ctrl, cudaStream_t s);
+// Natural-order zero-mean pressure (x - ctrl->p_mean_f) from the split iterate.
+void launch_unsplit_pressure(const Grid& g, const float* p, const ProjControl* ctrl, float* out, cudaStream_t s);
 // Assemble ctrl->result from the accumulators.
 void launch_finish_projection(ProjControl* ctrl, cudaStream_t s);
 

@@ -36,7 +36,10 @@ __device__ __forceinline__ int block_min_int(int v, int* scratch) {
     return -block_max(v == INT_MIN ? INT_MAX : -v, scratch);
 }
 
-__global__ void k_begin_projection(ProjControl* ctrl, vapor_linear_solve_options o) {
+__global__ void k_begin_projection(ProjControl* ctrl, vapor_linear_solve_options o, double* x64a, double* x64b) {
+    ctrl->x64[0] = x64a;
+    ctrl->x64[1] = x64b;
+    ctrl->x64_cur = 0;
     ctrl->div_before_bits = 0u;
     ctrl->div_after_bits = 0u;
     ctrl->rhs_max_key = INT_MIN;
@@ -68,6 +71,7 @@ __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const flo
     __shared__ float s_max[32];
     __shared__ int s_key[32];
     const int n = g.n;
+    const RBLayout L = rb_layout(n);
     const size_t cells = size_t(n) * n * n;
     double sum = 0.0;
     float div_max = 0.f;
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const flo
         if (!isfinite(div)) bad = 1u;
         div_max = maxf_ref(div_max, fabsf(div));
         const float rhs = -div * scale;
-        b[c] = rhs;
+        b[rb_index(L, x, y, z)] = rhs;
         sum += double(rhs);
         const int key = float_order_key(rhs);
         kmax = max(kmax, key);
@@ -110,7 +114,8 @@ __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const flo
 // Deterministic sum of the block partials, then the mean, the initial
 // residual and the stopping target (SOR.cpp:28-33).
 __global__ void k_rhs_finish(ProjControl* ctrl, const double* __restrict__ partials, int blocks, double cells,
-                             double abs_tol, double rel_tol) {
+                             double abs_tol, double rel_tol, int use_conditional,
+                             cudaGraphConditionalHandle handle) {
     __shared__ double s_sum[32];
     double sum = 0.0;
     for (int i = threadIdx.x; i < blocks; i += blockDim.x) sum += partials[i];
@@ -132,72 +137,137 @@ __global__ void k_rhs_finish(ProjControl* ctrl, const double* __restrict__ parti
     ctrl->result.linear_solve.converged = converged;
     ctrl->result.linear_solve.iterations = 0;
     ctrl->done = (converged && !ctrl->fixed) || ctrl->max_iterations == 0 || ctrl->nonfinite != 0u;
+    ctrl->continue_flag = !ctrl->done;
+    if (use_conditional) cudaGraphSetConditional(handle, ctrl->done ? 0u : 1u);
 }
 
-// One colour of red-black SOR (SOR.cpp:36-54) in the reference's operation
-// order: off = sum(-1 * x_nb) over existing neighbours in x-,x+,y-,y+,z-,z+
-// order; x += omega * (b - off - diag * x) / max(diag, floor).
-__global__ void __launch_bounds__(kThreads) k_sor_color(Grid g, int parity, float omega, float floor_diag,
-                                                        float* __restrict__ x, const float* __restrict__ b,
-                                                        const ProjControl* __restrict__ ctrl, int guarded,
-                                                        int subtract_mean) {
-    if (guarded && ctrl->done) return;
+// One colour of red-black SOR (SOR.cpp:36-54) on the split layout, in the
+// reference's operation order: off = sum(-1 * x_nb) over existing neighbours in
+// x-,x+,y-,y+,z-,z+ order; x += omega * (b - off - diag * x) / max(diag, floor).
+// Each thread updates VEC consecutive slots of one row (VEC = 4 uses vector
+// loads and needs hw % 4 == 0). The x-neighbours of slot i are the other
+// colour's slots i-1+s and i+s (s = (y+z+colour)&1, x = 2i+s); the y- and
+// z-neighbours are slot i of the adjacent rows of the other colour.
+template <int VEC>
+__global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float omega, float floor_diag,
+                                                     float* __restrict__ xs, const float* __restrict__ bs,
+                                                     const ProjControl* __restrict__ ctrl, int guarded,
+                                                     int sweep_index, int subtract_mean) {
+    if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
     const int n = g.n;
-    const int half = (n + 1) >> 1;
+    const RBLayout L = rb_layout(n);
+    const int hw = L.hw;
+    const int groups = hw / VEC;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.y;
-    const int y = t / half;
+    const int y = t / groups;
     if (y >= n) return;
-    const int i = 2 * (t - y * half) + ((y + z + parity) & 1);
-    if (i >= n) return;
-    const size_t nn = size_t(n) * n;
-    const size_t id = size_t(i) + size_t(n) * (size_t(y) + size_t(n) * z);
-    const float diag = float(neighbours(n, i, y, z));
-    if (diag == 0.f) return;
-    float off = 0.f;
-    if (i > 0) off += -1.f * x[id - 1];
-    if (i + 1 < n) off += -1.f * x[id + 1];
-    if (y > 0) off += -1.f * x[id - n];
-    if (y + 1 < n) off += -1.f * x[id + n];
-    if (z > 0) off += -1.f * x[id - nn];
-    if (z + 1 < n) off += -1.f * x[id + nn];
-    const float relax = maxf_ref(diag, floor_diag);
-    const float bi = subtract_mean ? b[id] - ctrl->rhs_mean_f : b[id];
-    const float xi = x[id];
-    x[id] = xi + omega * (bi - off - diag * xi) / relax;
+    const int i0 = (t - y * groups) * VEC;
+    const int s = (y + z + colour) & 1;
+    const size_t row = (size_t(z) * n + y) * hw;
+    float* __restrict__ own = xs + size_t(colour) * L.stride + row;
+    const float* __restrict__ oth = xs + size_t(1 - colour) * L.stride + row;
+    const float* __restrict__ rhs = bs + size_t(colour) * L.stride + row;
+    const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
+
+    float xo[VEC], bv[VEC], xl[VEC + 1], ym[VEC], yp[VEC], zm[VEC], zp[VEC];
+    const size_t yo = size_t(hw), zo = size_t(n) * hw;
+    if (VEC == 4) {
+        const float4 a4 = *reinterpret_cast<const float4*>(own + i0);
+        const float4 b4 = __ldg(reinterpret_cast<const float4*>(rhs + i0));
+        const float4 c4 = *reinterpret_cast<const float4*>(oth + i0);
+        xo[0] = a4.x; xo[1] = a4.y; xo[2] = a4.z; xo[3] = a4.w;
+        bv[0] = b4.x; bv[1] = b4.y; bv[2] = b4.z; bv[3] = b4.w;
+        // xl[k] = other-colour slot i0 - 1 + s + k, k = 0..VEC
+        if (s == 0) {
+            xl[0] = i0 > 0 ? oth[i0 - 1] : 0.f;
+            xl[1] = c4.x; xl[2] = c4.y; xl[3] = c4.z; xl[4] = c4.w;
+        } else {
+            xl[0] = c4.x; xl[1] = c4.y; xl[2] = c4.z; xl[3] = c4.w;
+            xl[4] = i0 + VEC < hw ? oth[i0 + VEC] : 0.f;
+        }
+        const float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 m4 = y > 0 ? *reinterpret_cast<const float4*>(oth - yo + i0) : z0;
+        const float4 p4 = y + 1 < n ? *reinterpret_cast<const float4*>(oth + yo + i0) : z0;
+        const float4 q4 = z > 0 ? *reinterpret_cast<const float4*>(oth - zo + i0) : z0;
+        const float4 r4 = z + 1 < n ? *reinterpret_cast<const float4*>(oth + zo + i0) : z0;
+        ym[0] = m4.x; ym[1] = m4.y; ym[2] = m4.z; ym[3] = m4.w;
+        yp[0] = p4.x; yp[1] = p4.y; yp[2] = p4.z; yp[3] = p4.w;
+        zm[0] = q4.x; zm[1] = q4.y; zm[2] = q4.z; zm[3] = q4.w;
+        zp[0] = r4.x; zp[1] = r4.y; zp[2] = r4.z; zp[3] = r4.w;
+    } else {
+        xo[0] = own[i0];
+        bv[0] = __ldg(rhs + i0);
+        const int lo = i0 - 1 + s;
+        xl[0] = lo >= 0 ? oth[lo] : 0.f;
+        xl[1] = lo + 1 < hw ? oth[lo + 1] : 0.f;
+        ym[0] = y > 0 ? oth[i0 - yo] : 0.f;
+        yp[0] = y + 1 < n ? oth[i0 + yo] : 0.f;
+        zm[0] = z > 0 ? oth[i0 - zo] : 0.f;
+        zp[0] = z + 1 < n ? oth[i0 + zo] : 0.f;
+    }
+    const int ny = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+    float res[VEC];
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) {
+        const int xc = 2 * (i0 + k) + s;
+        res[k] = xo[k];
+        if (xc >= n) continue;
+        const float diag = float((xc > 0) + (xc + 1 < n) + ny);
+        if (diag == 0.f) continue;
+        float off = 0.f;
+        if (xc > 0) off += -1.f * xl[k];
+        if (xc + 1 < n) off += -1.f * xl[k + 1];
+        if (y > 0) off += -1.f * ym[k];
+        if (y + 1 < n) off += -1.f * yp[k];
+        if (z > 0) off += -1.f * zm[k];
+        if (z + 1 < n) off += -1.f * zp[k];
+        const float relax = maxf_ref(diag, floor_diag);
+        const float bi = subtract_mean ? bv[k] - bm : bv[k];
+        res[k] = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
+    }
+    if (VEC == 4) {
+        *reinterpret_cast<float4*>(own + i0) = make_float4(res[0], res[1], res[2], res[3]);
+    } else {
+        if (2 * i0 + s < n) own[i0] = res[0];
+    }
 }
 
 // Mixed precision re-centring: x_out = x_in + e and r32 = float(b' - A x_out),
 // both in FP64, with the neighbour order of the reference residual.
 __global__ void __launch_bounds__(kThreads) k_refine_residual(Grid g, const float* __restrict__ b,
-                                                              const double* __restrict__ xin,
                                                               const float* __restrict__ e,
-                                                              double* __restrict__ xout, float* __restrict__ r32,
-                                                              ProjControl* ctrl) {
+                                                              float* __restrict__ r32, ProjControl* ctrl) {
     __shared__ double s_max[32];
+    const double* __restrict__ xin = ctrl->x64[ctrl->x64_cur];
+    double* __restrict__ xout = ctrl->x64[1 - ctrl->x64_cur];
     const int n = g.n;
+    const RBLayout L = rb_layout(n);
     const size_t cells = size_t(n) * n * n;
-    const size_t nn = size_t(n) * n;
     const float bm = ctrl->rhs_mean_f;
     double r = 0.0;
     unsigned int bad = 0u;
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int i, j, k;
         decode_cell(c, n, i, j, k);
-        auto xv = [&](size_t id) { return xin[id] + double(e[id]); };
-        const double xc = xv(c);
+        auto xv = [&](int a, int bb, int cc) {
+            const size_t id = rb_index(L, a, bb, cc);
+            return xin[id] + double(e[id]);
+        };
+        const size_t me = rb_index(L, i, j, k);
+        const double xc = xin[me] + double(e[me]);
         double ax = double(neighbours(n, i, j, k)) * xc;
-        if (i > 0) ax -= xv(c - 1);
-        if (i + 1 < n) ax -= xv(c + 1);
-        if (j > 0) ax -= xv(c - n);
-        if (j + 1 < n) ax -= xv(c + n);
-        if (k > 0) ax -= xv(c - nn);
-        if (k + 1 < n) ax -= xv(c + nn);
-        const float bi = b[c] - bm;
+        if (i > 0) ax -= xv(i - 1, j, k);
+        if (i + 1 < n) ax -= xv(i + 1, j, k);
+        if (j > 0) ax -= xv(i, j - 1, k);
+        if (j + 1 < n) ax -= xv(i, j + 1, k);
+        if (k > 0) ax -= xv(i, j, k - 1);
+        if (k + 1 < n) ax -= xv(i, j, k + 1);
+        const float bi = b[me] - bm;
         const double res = double(bi) - ax;
         if (!isfinite(res)) bad = 1u;
-        xout[c] = xc;
-        r32[c] = float(res);
+        xout[me] = xc;
+        r32[me] = float(res);
         const double a = fabs(res);
         r = r < a ? a : r;
     }
@@ -209,13 +279,19 @@ __global__ void __launch_bounds__(kThreads) k_refine_residual(Grid g, const floa
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_psum64(Grid g, const double* __restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_psum64(Grid g, const ProjControl* __restrict__ ctrl,
                                                      double* __restrict__ partials) {
     __shared__ double s_sum[32];
-    const size_t cells = size_t(g.n) * g.n * g.n;
+    const double* __restrict__ x = ctrl->x64[ctrl->x64_cur];
+    const int n = g.n;
+    const RBLayout L = rb_layout(n);
+    const size_t cells = size_t(n) * n * n;
     double sum = 0.0;
-    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x)
-        sum += x[c];
+    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+        int i, j, k;
+        decode_cell(c, n, i, j, k);
+        sum += x[rb_index(L, i, j, k)];
+    }
     const double bs = block_sum(sum, s_sum);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
 }
@@ -232,14 +308,14 @@ __global__ void k_psum64_finish(ProjControl* ctrl, const double* __restrict__ pa
 }
 
 // Final FP64 residual of x64 - mean (StencilLinearSystem.cpp:53-70 order) and
-// the float pressure copy.
-__global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const double* __restrict__ x,
-                                                         const float* __restrict__ b, float* __restrict__ p32,
-                                                         ProjControl* ctrl) {
+// the float pressure copy (split layout).
+__global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const float* __restrict__ b,
+                                                         float* __restrict__ p32, ProjControl* ctrl) {
     __shared__ double s_max[32];
+    const double* __restrict__ x = ctrl->x64[ctrl->x64_cur];
     const int n = g.n;
+    const RBLayout L = rb_layout(n);
     const size_t cells = size_t(n) * n * n;
-    const size_t nn = size_t(n) * n;
     const float bm = ctrl->rhs_mean_f;
     const double pm = ctrl->p_mean64;
     double r = 0.0;
@@ -247,18 +323,19 @@ __global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const double* _
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int i, j, k;
         decode_cell(c, n, i, j, k);
-        auto xv = [&](size_t id) { return x[id] - pm; };
-        const double xc = xv(c);
+        auto xv = [&](int a, int bb, int cc) { return x[rb_index(L, a, bb, cc)] - pm; };
+        const size_t me = rb_index(L, i, j, k);
+        const double xc = x[me] - pm;
         double ax = double(float(neighbours(n, i, j, k))) * xc;
-        if (i > 0) ax += -1.0 * xv(c - 1);
-        if (i + 1 < n) ax += -1.0 * xv(c + 1);
-        if (j > 0) ax += -1.0 * xv(c - n);
-        if (j + 1 < n) ax += -1.0 * xv(c + n);
-        if (k > 0) ax += -1.0 * xv(c - nn);
-        if (k + 1 < n) ax += -1.0 * xv(c + nn);
-        const float bi = b[c] - bm;
+        if (i > 0) ax += -1.0 * xv(i - 1, j, k);
+        if (i + 1 < n) ax += -1.0 * xv(i + 1, j, k);
+        if (j > 0) ax += -1.0 * xv(i, j - 1, k);
+        if (j + 1 < n) ax += -1.0 * xv(i, j + 1, k);
+        if (k > 0) ax += -1.0 * xv(i, j, k - 1);
+        if (k + 1 < n) ax += -1.0 * xv(i, j, k + 1);
+        const float bi = b[me] - bm;
         if (!isfinite(xc)) bad = 1u;
-        p32[c] = float(xc);
+        p32[me] = float(xc);
         const double a = fabs(double(bi) - ax);
         r = r < a ? a : r;
     }
@@ -271,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const double* _
 }
 
 // Gradient with an FP64 pressure: u_out = float(u - dt (p1 - p0) / h) in FP64.
-__global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt, const double* __restrict__ p,
+__global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt,
                                                          const float* __restrict__ u, const float* __restrict__ v,
                                                          const float* __restrict__ w, float* __restrict__ uo,
                                                          float* __restrict__ vo, float* __restrict__ wo,
@@ -283,21 +360,24 @@ __global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt, const
     const size_t nn = size_t(n) * n;
     const double hInv = 1.0 / double(g.h), dtd = double(dt);
     const double pm = ctrl->p_mean64;
+    const double* __restrict__ p = ctrl->x64[ctrl->x64_cur];
+    const RBLayout L = rb_layout(n);
     float div_max = 0.f;
     unsigned int bad = 0u;
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode_cell(c, n, x, y, z);
-        const double pc = p[c] - pm;
+        auto pv = [&](int a, int bb, int cc) { return p[rb_index(L, a, bb, cc)] - pm; };
+        const double pc = pv(x, y, z);
         const size_t ix0 = index_of(n, FACE_X, x, y, z), ix1 = ix0 + 1;
         const size_t iy0 = index_of(n, FACE_Y, x, y, z), iy1 = iy0 + n;
         const size_t iz0 = c, iz1 = c + nn;
-        const float ux0 = x == 0 ? 0.f : float(double(u[ix0]) - dtd * (pc - (p[c - 1] - pm)) * hInv);
-        const float ux1 = x + 1 == n ? 0.f : float(double(u[ix1]) - dtd * ((p[c + 1] - pm) - pc) * hInv);
-        const float vy0 = y == 0 ? 0.f : float(double(v[iy0]) - dtd * (pc - (p[c - n] - pm)) * hInv);
-        const float vy1 = y + 1 == n ? 0.f : float(double(v[iy1]) - dtd * ((p[c + n] - pm) - pc) * hInv);
-        const float wz0 = z == 0 ? 0.f : float(double(w[iz0]) - dtd * (pc - (p[c - nn] - pm)) * hInv);
-        const float wz1 = z + 1 == n ? 0.f : float(double(w[iz1]) - dtd * ((p[c + nn] - pm) - pc) * hInv);
+        const float ux0 = x == 0 ? 0.f : float(double(u[ix0]) - dtd * (pc - pv(x - 1, y, z)) * hInv);
+        const float ux1 = x + 1 == n ? 0.f : float(double(u[ix1]) - dtd * (pv(x + 1, y, z) - pc) * hInv);
+        const float vy0 = y == 0 ? 0.f : float(double(v[iy0]) - dtd * (pc - pv(x, y - 1, z)) * hInv);
+        const float vy1 = y + 1 == n ? 0.f : float(double(v[iy1]) - dtd * (pv(x, y + 1, z) - pc) * hInv);
+        const float wz0 = z == 0 ? 0.f : float(double(w[iz0]) - dtd * (pc - pv(x, y, z - 1)) * hInv);
+        const float wz1 = z + 1 == n ? 0.f : float(double(w[iz1]) - dtd * (pv(x, y, z + 1) - pc) * hInv);
         uo[ix0] = ux0;
         vo[iy0] = vy0;
         wo[iz0] = wz0;
@@ -332,24 +412,27 @@ __global__ void __launch_bounds__(kThreads) k_residual(Grid g, const float* __re
     __shared__ double s_max[32];
     const int n = g.n;
     const size_t cells = size_t(n) * n * n;
-    const size_t nn = size_t(n) * n;
     const float bm = ctrl->rhs_mean_f;
     const float pm = final_pass ? ctrl->p_mean_f : 0.f;
+    const RBLayout L = rb_layout(n);
     double r = 0.0;
     unsigned int bad = 0u;
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int i, j, k;
         decode_cell(c, n, i, j, k);
-        auto xv = [&](size_t id) { return final_pass ? x[id] - pm : x[id]; };
-        const float xc = xv(c);
+        auto xv = [&](int a, int bb, int cc) {
+            const float v = x[rb_index(L, a, bb, cc)];
+            return final_pass ? v - pm : v;
+        };
+        const float xc = xv(i, j, k);
         double ax = double(float(neighbours(n, i, j, k))) * double(xc);
-        if (i > 0) ax += -1.0 * double(xv(c - 1));
-        if (i + 1 < n) ax += -1.0 * double(xv(c + 1));
-        if (j > 0) ax += -1.0 * double(xv(c - n));
-        if (j + 1 < n) ax += -1.0 * double(xv(c + n));
-        if (k > 0) ax += -1.0 * double(xv(c - nn));
-        if (k + 1 < n) ax += -1.0 * double(xv(c + nn));
-        const float bi = b[c] - bm;
+        if (i > 0) ax += -1.0 * double(xv(i - 1, j, k));
+        if (i + 1 < n) ax += -1.0 * double(xv(i + 1, j, k));
+        if (j > 0) ax += -1.0 * double(xv(i, j - 1, k));
+        if (j + 1 < n) ax += -1.0 * double(xv(i, j + 1, k));
+        if (k > 0) ax += -1.0 * double(xv(i, j, k - 1));
+        if (k + 1 < n) ax += -1.0 * double(xv(i, j, k + 1));
+        const float bi = b[rb_index(L, i, j, k)] - bm;
         if (!isfinite(xc) || !isfinite(bi)) bad = 1u;
         const double e = fabs(double(bi) - ax);
         r = r < e ? e : r;
@@ -365,10 +448,11 @@ __global__ void __launch_bounds__(kThreads) k_residual(Grid g, const float* __re
 // Records one residual check (SOR.cpp:56-61): iterations, final residual,
 // converged, and whether the loop stops. Optionally sets the CUDA graph
 // while-condition so the loop can run on the device without the host.
-__global__ void k_check(ProjControl* ctrl, int iterations_done, int use_conditional,
-                        cudaGraphConditionalHandle handle, int add_to_iterations) {
-    if (add_to_iterations) ctrl->iterations += iterations_done;
-    else ctrl->iterations = iterations_done;
+__global__ void k_check(ProjControl* ctrl, int iterations, int accumulate, int flip_x64, int use_conditional,
+                        cudaGraphConditionalHandle handle) {
+    if (accumulate) ctrl->iterations = min(ctrl->iterations + iterations, ctrl->max_iterations);
+    else ctrl->iterations = iterations;
+    if (flip_x64) ctrl->x64_cur = 1 - ctrl->x64_cur;
     const double res = __longlong_as_double((long long)ctrl->res_bits);
     ctrl->res_bits = 0ull;
     const int converged = res <= ctrl->target;
@@ -385,10 +469,15 @@ __global__ void k_check(ProjControl* ctrl, int iterations_done, int use_conditio
 __global__ void __launch_bounds__(kThreads) k_psum(Grid g, const float* __restrict__ x,
                                                    double* __restrict__ partials) {
     __shared__ double s_sum[32];
-    const size_t cells = size_t(g.n) * g.n * g.n;
+    const int n = g.n;
+    const RBLayout L = rb_layout(n);
+    const size_t cells = size_t(n) * n * n;
     double sum = 0.0;
-    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x)
-        sum += double(x[c]);
+    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+        int i, j, k;
+        decode_cell(c, n, i, j, k);
+        sum += double(x[rb_index(L, i, j, k)]);
+    }
     const double bs = block_sum(sum, s_sum);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
 }
@@ -426,21 +515,23 @@ __global__ void __launch_bounds__(kThreads) k_gradient(Grid g, float dt, const f
     const size_t nn = size_t(n) * n;
     const float hInv = 1.f / g.h;
     const float pm = ctrl->p_mean_f;
+    const RBLayout L = rb_layout(n);
     float div_max = 0.f;
     unsigned int bad = 0u;
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode_cell(c, n, x, y, z);
-        const float pc = p[c] - pm;
+        auto pv = [&](int a, int bb, int cc) { return p[rb_index(L, a, bb, cc)] - pm; };
+        const float pc = pv(x, y, z);
         const size_t ix0 = index_of(n, FACE_X, x, y, z), ix1 = ix0 + 1;
         const size_t iy0 = index_of(n, FACE_Y, x, y, z), iy1 = iy0 + n;
         const size_t iz0 = c, iz1 = c + nn;
-        const float ux0 = x == 0 ? 0.f : u[ix0] - dt * (pc - (p[c - 1] - pm)) * hInv;
-        const float ux1 = x + 1 == n ? 0.f : u[ix1] - dt * ((p[c + 1] - pm) - pc) * hInv;
-        const float vy0 = y == 0 ? 0.f : v[iy0] - dt * (pc - (p[c - n] - pm)) * hInv;
-        const float vy1 = y + 1 == n ? 0.f : v[iy1] - dt * ((p[c + n] - pm) - pc) * hInv;
-        const float wz0 = z == 0 ? 0.f : w[iz0] - dt * (pc - (p[c - nn] - pm)) * hInv;
-        const float wz1 = z + 1 == n ? 0.f : w[iz1] - dt * ((p[c + nn] - pm) - pc) * hInv;
+        const float ux0 = x == 0 ? 0.f : u[ix0] - dt * (pc - pv(x - 1, y, z)) * hInv;
+        const float ux1 = x + 1 == n ? 0.f : u[ix1] - dt * (pv(x + 1, y, z) - pc) * hInv;
+        const float vy0 = y == 0 ? 0.f : v[iy0] - dt * (pc - pv(x, y - 1, z)) * hInv;
+        const float vy1 = y + 1 == n ? 0.f : v[iy1] - dt * (pv(x, y + 1, z) - pc) * hInv;
+        const float wz0 = z == 0 ? 0.f : w[iz0] - dt * (pc - pv(x, y, z - 1)) * hInv;
+        const float wz1 = z + 1 == n ? 0.f : w[iz1] - dt * (pv(x, y, z + 1) - pc) * hInv;
         uo[ix0] = ux0;
         vo[iy0] = vy0;
         wo[iz0] = wz0;
@@ -464,6 +555,21 @@ __global__ void __launch_bounds__(kThreads) k_gradient(Grid g, float dt, const f
     if (threadIdx.x == 0) {
         atomic_max_nonneg(&ctrl->div_after_bits, bm);
         if (any_bad) atomicOr(&ctrl->nonfinite, 2u);
+    }
+}
+
+// Natural-order copy of the zero-mean pressure (x - pressure mean) for callers.
+__global__ void __launch_bounds__(kThreads) k_unsplit_pressure(Grid g, const float* __restrict__ p,
+                                                               const ProjControl* __restrict__ ctrl,
+                                                               float* __restrict__ out) {
+    const int n = g.n;
+    const RBLayout L = rb_layout(n);
+    const size_t cells = size_t(n) * n * n;
+    const float pm = ctrl->p_mean_f;
+    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode_cell(c, n, x, y, z);
+        out[c] = p[rb_index(L, x, y, z)] - pm;
     }
 }
 
@@ -548,57 +654,71 @@ int reduction_blocks(size_t count) {
 }
 
 void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const float* w, float* b,
-                double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s) {
+                double* partials, int partial_capacity, ProjControl* ctrl, double* x64a, double* x64b,
+                LoopCond cond, cudaStream_t s) {
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     const int blocks = std::min(reduction_blocks(cells), partial_capacity);
     const float scale = a.g.h * a.g.h / a.dt;
     count_launch();
-    k_begin_projection<<<1, 1, 0, s>>>(ctrl, a.options);
+    k_begin_projection<<<1, 1, 0, s>>>(ctrl, a.options, x64a, x64b);
     count_launch();
     k_rhs<<<blocks, kThreads, 0, s>>>(a.g, scale, u, v, w, b, partials, ctrl);
     count_launch();
     k_rhs_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, double(cells), a.options.absolute_tolerance,
-                                    a.options.relative_tolerance);
+                                    a.options.relative_tolerance, cond.active,
+                                    (cudaGraphConditionalHandle)cond.handle);
 }
 
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, cudaStream_t s, bool subtract_mean) {
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s) {
     const int n = a.g.n;
-    const int half = (n + 1) / 2;
-    const dim3 grid((half * n + kThreads - 1) / kThreads, n);
+    const RBLayout L = rb_layout(n);
     count_launch();
-    k_sor_color<<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, x, b, ctrl, guarded ? 1 : 0,
-                                          subtract_mean ? 1 : 0);
+    if (L.hw % 4 == 0) {
+        const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n);
+        k_sor_rb<4><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, x, b, ctrl, guarded ? 1 : 0,
+                                              sweep_index, subtract_mean ? 1 : 0);
+    } else {
+        const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n);
+        k_sor_rb<1><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, x, b, ctrl, guarded ? 1 : 0,
+                                              sweep_index, subtract_mean ? 1 : 0);
+    }
 }
 
-void launch_refine_residual(const ProjectionArgs& a, const float* b, const double* x_in, const float* e,
-                            double* x_out, float* r32, ProjControl* ctrl, cudaStream_t s) {
+void launch_unsplit_pressure(const Grid& g, const float* p, const ProjControl* ctrl, float* out, cudaStream_t s) {
+    const size_t cells = size_t(g.n) * g.n * g.n;
+    count_launch();
+    k_unsplit_pressure<<<reduction_blocks(cells), kThreads, 0, s>>>(g, p, ctrl, out);
+}
+
+void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
+                            ProjControl* ctrl, cudaStream_t s) {
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     count_launch();
-    k_refine_residual<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, x_in, e, x_out, r32, ctrl);
+    k_refine_residual<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
 }
 
-void launch_pressure_mean64(const ProjectionArgs& a, const double* x64, const float* b, float* p32,
-                            double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s) {
+void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
+                            int partial_capacity, ProjControl* ctrl, cudaStream_t s) {
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     const int blocks = std::min(reduction_blocks(cells), partial_capacity);
     count_launch();
-    k_psum64<<<blocks, kThreads, 0, s>>>(a.g, x64, partials);
+    k_psum64<<<blocks, kThreads, 0, s>>>(a.g, ctrl, partials);
     count_launch();
     k_psum64_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, double(cells));
     count_launch();
-    k_residual64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, x64, b, p32, ctrl);
+    k_residual64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, p32, ctrl);
     count_launch();
     k_final_check<<<1, 1, 0, s>>>(ctrl);
 }
 
-void launch_gradient64(const ProjectionArgs& a, const double* x64, const float* u_in, const float* v_in,
-                       const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat,
-                       float* w_hat, ProjControl* ctrl, cudaStream_t s) {
+void launch_gradient64(const ProjectionArgs& a, const float* u_in, const float* v_in, const float* w_in,
+                       float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat, float* w_hat,
+                       ProjControl* ctrl, cudaStream_t s) {
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     count_launch();
-    k_gradient64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, a.dt, x64, u_in, v_in, w_in, u_out, v_out,
-                                                              w_out, u_hat, v_hat, w_hat, ctrl);
+    k_gradient64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, a.dt, u_in, v_in, w_in, u_out, v_out, w_out,
+                                                              u_hat, v_hat, w_hat, ctrl);
 }
 
 void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,
@@ -612,11 +732,11 @@ void launch_residual(const ProjectionArgs& a, const float* x, const float* b, Pr
     }
 }
 
-void launch_check(ProjControl* ctrl, int iterations_done, bool graph_conditional, unsigned long long cond_handle,
+void launch_check(ProjControl* ctrl, int iterations, bool accumulate, bool flip_x64, LoopCond cond,
                   cudaStream_t s) {
     count_launch();
-    k_check<<<1, 1, 0, s>>>(ctrl, iterations_done, graph_conditional ? 1 : 0,
-                            (cudaGraphConditionalHandle)cond_handle, graph_conditional ? 1 : 0);
+    k_check<<<1, 1, 0, s>>>(ctrl, iterations, accumulate ? 1 : 0, flip_x64 ? 1 : 0, cond.active,
+                            (cudaGraphConditionalHandle)cond.handle);
 }
 
 void launch_pressure_mean(const ProjectionArgs& a, const float* x, double* partials, int partial_capacity,

@@ -97,6 +97,27 @@ __device__ __forceinline__ float sample(const float* __restrict__ f, int n, floa
     return s;
 }
 
+// Red-black split storage of the projection's cell arrays (b, p, e, r32,
+// x64): the cells of colour c = (x+y+z)&1 in row (y,z) lie contiguously at
+// c*stride + (z*n + y)*hw + (x>>1), with hw = (n+1)/2 slots per row. A colour
+// sweep then reads and writes only dense, coalesced runs: its own half of the
+// iterate and of b, and the other colour's half for the neighbours.
+struct RBLayout {
+    int n, hw;
+    size_t stride;  // elements per colour
+};
+__host__ __device__ inline RBLayout rb_layout(int n) {
+    RBLayout L;
+    L.n = n;
+    L.hw = (n + 1) / 2;
+    L.stride = size_t(n) * n * L.hw;
+    return L;
+}
+__host__ __device__ inline size_t rb_count(int n) { return 2 * rb_layout(n).stride; }
+__host__ __device__ inline size_t rb_index(const RBLayout& L, int x, int y, int z) {
+    return size_t((x + y + z) & 1) * L.stride + (size_t(z) * L.n + y) * L.hw + size_t(x >> 1);
+}
+
 struct Vel {
     float x, y, z;
 };
