@@ -296,6 +296,45 @@ vapor_status vapor_stage_advect_scalar_device(vapor_stage *stage, float dt, floa
 vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 
+/* ---- Learned warm start for the pressure solve ----
+ * No counterpart in the reference, whose projection starts every solve from
+ * zero pressure (CpuPressureSolver3D.cpp:46). The model is a fixed 3-level 3D
+ * U-Net (16/32/64 channels, about 0.35 M parameters, BF16 weights and
+ * activations, FP32 accumulation on tcgen05 tensor cores) that maps the normalized right-hand side to the normalized
+ * zero-mean pressure; the projection then runs its usual solver from that
+ * guess, so convergence criteria and results keep their meaning. Parameters
+ * are one FP32 vector: for each of the 10 convolutions its weights
+ * [27][cout][cin] then its bias [cout], then the 1x1 head's 16 weights and
+ * its bias. Grids must have n divisible by 4. */
+typedef struct vapor_unet vapor_unet;
+int64_t vapor_unet_parameter_count(void);
+vapor_status vapor_unet_create(vapor_unet **out);
+vapor_status vapor_unet_destroy(vapor_unet *net);
+/* He-uniform weights from `seed`, zero biases, Adam state cleared. */
+vapor_status vapor_unet_init(vapor_unet *net, uint32_t seed);
+vapor_status vapor_unet_set_parameters(vapor_unet *net, const float *host, int64_t count);
+vapor_status vapor_unet_get_parameters(vapor_unet *net, float *host, int64_t count);
+/* Raw network on device buffers: input is n^3 voxels x 16 BF16 channels
+ * (channels-last; channel 0 the normalized RHS, channel 1 the solid mask,
+ * the rest zero), output n^3 FP32. Synchronizes. */
+vapor_status vapor_unet_forward_features(vapor_unet *net, int32_t n, const void *input_bf16,
+                                         float *output);
+/* Gradient of sum(output * grad_output) with respect to the parameters after
+ * vapor_unet_forward_features on the same n; grad_output is device memory,
+ * grad_params host memory of vapor_unet_parameter_count() floats. */
+vapor_status vapor_unet_backward(vapor_unet *net, int32_t n, const float *grad_output,
+                                 float *grad_params);
+/* Use `net` (NULL: none) for the initial guess of every later projection of
+ * `sim`. The network must outlive the simulation or be detached first. */
+vapor_status vapor_mac3d_set_warm_start(vapor_mac3d *sim, vapor_unet *net);
+/* One Adam step on the simulation's last projection (its right-hand side and
+ * converged pressure); *loss (may be NULL) receives the relative squared error
+ * of the prediction before the step. */
+vapor_status vapor_mac3d_train_warm_start(vapor_mac3d *sim, vapor_unet *net, float learning_rate,
+                                          double *loss);
+/* The same loss without an update. */
+vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d *sim, vapor_unet *net, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

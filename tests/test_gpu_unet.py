@@ -1,0 +1,153 @@
+"""The learned warm start's network against a plain PyTorch FP32 reference.
+
+The CUDA U-Net (tcgen05 implicit-GEMM 3x3x3 convolutions, BF16 weights and
+activations, FP32 accumulation) is compared with the same network written in
+PyTorch FP32 on the CPU with the same parameters. The reference rounds weights
+and stored activations to BF16 where the CUDA path stores BF16, so the
+remaining differences are FP32 accumulation order and occasional BF16 rounding
+flips; the tolerances are stated per check.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import vapor_b200 as vb
+
+pytestmark = pytest.mark.gpu
+
+LAYERS = [(16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32), (32, 32), (48, 16), (16, 16)]
+
+
+def _lib():
+    lib = vb.library()
+    for name, args, res in (
+            ("vapor_unet_create", [C.POINTER(C.c_void_p)], C.c_int),
+            ("vapor_unet_destroy", [C.c_void_p], C.c_int),
+            ("vapor_unet_init", [C.c_void_p, C.c_uint32], C.c_int),
+            ("vapor_unet_parameter_count", [], C.c_int64),
+            ("vapor_unet_get_parameters", [C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+            ("vapor_unet_set_parameters", [C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+            ("vapor_unet_forward_features", [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
+            ("vapor_unet_backward", [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int)):
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = args, res
+    return lib
+
+
+class Net:
+    def __init__(self, seed=7):
+        self.lib = _lib()
+        h = C.c_void_p()
+        vb.check(self.lib.vapor_unet_create(C.byref(h)))
+        self.h = h
+        vb.check(self.lib.vapor_unet_init(h, seed))
+        self.P = self.lib.vapor_unet_parameter_count()
+
+    def params(self):
+        p = np.zeros(self.P, np.float32)
+        vb.check(self.lib.vapor_unet_get_parameters(self.h, p.ctypes.data, self.P))
+        return p
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vapor_unet_destroy(self.h)
+
+
+def split(params):
+    """Parameter vector -> list of (W[cout,cin,3,3,3], b[cout]) and the head."""
+    out, off = [], 0
+    for cin, cout in LAYERS:
+        w = params[off:off + 27 * cout * cin].reshape(27, cout, cin)
+        off += 27 * cout * cin
+        b = params[off:off + cout]
+        off += cout
+        out.append((np.ascontiguousarray(w.transpose(1, 2, 0).reshape(cout, cin, 3, 3, 3)), b))
+    return out, params[off:off + 16], params[off + 16]
+
+
+def torch_reference(params, x16, requires_grad=False):
+    """Same U-Net in FP32 with BF16 rounding where the CUDA path stores BF16."""
+    import torch
+    import torch.nn.functional as F
+    convs, hw, hb = split(params)
+    q = lambda t: t.to(torch.bfloat16).to(torch.float32)
+    ws = [torch.tensor(w, requires_grad=requires_grad) for w, _ in convs]
+    bs = [torch.tensor(b, requires_grad=requires_grad) for _, b in convs]
+    hw_t = torch.tensor(hw, requires_grad=requires_grad)
+    hb_t = torch.tensor(np.array([hb], np.float32), requires_grad=requires_grad)
+
+    def conv(i, x):
+        y = F.conv3d(x, ws[i].to(torch.bfloat16).to(torch.float32) if not requires_grad else ws[i], bs[i], padding=1)
+        return q(F.relu(y)) if not requires_grad else F.relu(y)
+    x = torch.tensor(x16).permute(3, 0, 1, 2).unsqueeze(0)
+    e1a = conv(0, x)
+    s1 = conv(1, e1a)
+    e2in = q(F.avg_pool3d(s1, 2)) if not requires_grad else F.avg_pool3d(s1, 2)
+    e2a = conv(2, e2in)
+    s2 = conv(3, e2a)
+    e3in = q(F.avg_pool3d(s2, 2)) if not requires_grad else F.avg_pool3d(s2, 2)
+    e3a = conv(4, e3in)
+    e3b = conv(5, e3a)
+    dec2 = torch.cat([F.interpolate(e3b, scale_factor=2, mode="nearest"), s2], 1)
+    d2a = conv(6, dec2)
+    d2b = conv(7, d2a)
+    dec1 = torch.cat([F.interpolate(d2b, scale_factor=2, mode="nearest"), s1], 1)
+    d1a = conv(8, dec1)
+    d1b = conv(9, d1a)
+    out = (d1b * hw_t.view(1, 16, 1, 1, 1)).sum(1) + hb_t
+    return out[0], ws, bs, hw_t, hb_t
+
+
+def features(n, seed):
+    rng = np.random.default_rng(seed)
+    x = np.zeros((n, n, n, 16), np.float32)
+    x[..., 0] = rng.standard_normal((n, n, n))
+    x[..., 1] = (rng.random((n, n, n)) < 0.1).astype(np.float32)
+    return x
+
+
+@pytest.mark.parametrize("n", [8, 16, 32])
+def test_forward_matches_torch_reference(n):
+    import torch
+    net = Net(seed=11)
+    p = net.params()
+    x = features(n, 3)
+    xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+    out = torch.zeros(n * n * n, dtype=torch.float32, device="cuda")
+    vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+    got = out.cpu().numpy().reshape(n, n, n)
+    ref, *_ = torch_reference(p, xin.float().cpu().numpy())
+    ref = ref.detach().numpy()
+    err = np.abs(got - ref).max() / max(1e-6, np.abs(ref).max())
+    assert err < 2e-2, err  # BF16 activations: a few rounding flips propagate
+
+
+def test_gradients_match_torch_autograd():
+    """dL/dparams for L = sum(out * g) against PyTorch autograd in FP32."""
+    import torch
+    n = 16
+    net = Net(seed=5)
+    p = net.params()
+    x = features(n, 9)
+    xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+    out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+    vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+    g = np.random.default_rng(1).standard_normal(n ** 3).astype(np.float32) / n ** 3
+    gdev = torch.tensor(g).cuda()
+    grads = np.zeros(net.P, np.float32)
+    vb.check(net.lib.vapor_unet_backward(net.h, n, gdev.data_ptr(), grads.ctypes.data))
+    # reference with BF16-rounded weights and inputs, FP32 everywhere else
+    pq = torch.tensor(p).to(torch.bfloat16).float().numpy()
+    ref, ws, bs, hw, hb = torch_reference(pq, xin.float().cpu().numpy(), requires_grad=True)
+    (ref.reshape(-1) * torch.tensor(g)).sum().backward()
+    convs, _, _ = split(grads)
+    for i, (w_g, b_g) in enumerate(convs):
+        rw = ws[i].grad.numpy()
+        cos = float((w_g * rw).sum() / (np.linalg.norm(w_g) * np.linalg.norm(rw) + 1e-30))
+        rel = float(np.linalg.norm(w_g - rw) / (np.linalg.norm(rw) + 1e-30))
+        assert cos > 0.99 and rel < 0.1, (i, cos, rel)
+        rb = bs[i].grad.numpy()
+        assert np.linalg.norm(b_g - rb) <= 0.1 * np.linalg.norm(rb) + 1e-7, i
+    head = grads[-17:-1]
+    assert np.linalg.norm(head - hw.grad.numpy()) <= 0.05 * np.linalg.norm(hw.grad.numpy())

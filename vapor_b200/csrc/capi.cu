@@ -1,11 +1,13 @@
 // extern "C" boundary of include/vapor_b200.h. Every entry point catches all
 // C++ exceptions and turns them into a vapor_status plus a per-thread message.
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
 #include <string>
 
 #include "engine.hpp"
+#include "unet.hpp"
 
 struct vapor_mac3d {
     vb::Simulation sim;
@@ -14,6 +16,11 @@ struct vapor_mac3d {
 struct vapor_stage {
     vb::Stage stage;
     vapor_stage(int n, float box) : stage(n, box) {}
+};
+struct vapor_unet {
+    vb::Stream stream;
+    vb::unet::UNet net;
+    vapor_unet() : net(stream.s) {}
 };
 
 namespace {
@@ -53,6 +60,10 @@ void require_device() {
     if (prop.major != 10) vb::fail(VAPOR_RUNTIME_ERROR, "vapor_b200 requires an sm_100 (B200) device");
 }
 }  // namespace
+
+namespace vb {
+vapor_status guard(const std::function<void()>& f) { return guarded(f); }
+}  // namespace vb
 
 #define VB_API extern "C" __attribute__((visibility("default")))
 
@@ -269,4 +280,69 @@ VB_API vapor_status vapor_stage_set_solver_kind(vapor_stage* stage, int32_t kind
 }
 VB_API vapor_status vapor_stage_stream(vapor_stage* stage, void** stream) {
     STAGE_GUARD(require(stream != nullptr, "null output"); *stream = (void*)stage->stage.stream());
+}
+
+// ---- learned warm start ----
+VB_API int64_t vapor_unet_parameter_count(void) { return vb::unet::parameter_count(); }
+
+VB_API vapor_status vapor_unet_create(vapor_unet** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output");
+        *out = nullptr;
+        require_device();
+        *out = new vapor_unet();
+    });
+}
+VB_API vapor_status vapor_unet_destroy(vapor_unet* net) {
+    return guarded([&] { delete net; });
+}
+
+#define NET_GUARD(body)                                      \
+    return guarded([&] {                                     \
+        require(net != nullptr, "null network handle");     \
+        body;                                                \
+    })
+
+VB_API vapor_status vapor_unet_init(vapor_unet* net, uint32_t seed) {
+    NET_GUARD(net->net.set_stream(net->stream.s); net->net.init_parameters(seed));
+}
+VB_API vapor_status vapor_unet_set_parameters(vapor_unet* net, const float* host, int64_t count) {
+    NET_GUARD(require(host && count == vb::unet::parameter_count(), "parameter count mismatch");
+              net->net.set_stream(net->stream.s); net->net.set_parameters(host));
+}
+VB_API vapor_status vapor_unet_get_parameters(vapor_unet* net, float* host, int64_t count) {
+    NET_GUARD(require(host && count == vb::unet::parameter_count(), "parameter count mismatch");
+              net->net.get_parameters(host));
+}
+VB_API vapor_status vapor_unet_forward_features(vapor_unet* net, int32_t n, const void* input_bf16, float* output) {
+    NET_GUARD(require(input_bf16 && output, "null buffer"); net->net.set_stream(net->stream.s);
+              net->net.forward_features(n, static_cast<const __nv_bfloat16*>(input_bf16), output);
+              VB_CUDA(cudaStreamSynchronize(net->stream.s));
+              if (net->net.error_flag()) vb::fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out"));
+}
+VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float* grad_output, float* grad_params) {
+    NET_GUARD(require(grad_output && grad_params, "null buffer"); net->net.set_stream(net->stream.s);
+              net->net.backward_from_output(n, grad_output);
+              VB_CUDA(cudaMemcpyAsync(grad_params, net->net.gradient(),
+                                      vb::unet::parameter_count() * sizeof(float), cudaMemcpyDeviceToHost,
+                                      net->stream.s));
+              VB_CUDA(cudaStreamSynchronize(net->stream.s));
+              if (net->net.error_flag()) vb::fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out"));
+}
+VB_API vapor_status vapor_mac3d_set_warm_start(vapor_mac3d* sim, vapor_unet* net) {
+    SIM_GUARD(sim->sim.set_warm_start(net ? &net->net : nullptr));
+}
+VB_API vapor_status vapor_mac3d_train_warm_start(vapor_mac3d* sim, vapor_unet* net, float learning_rate,
+                                                 double* loss) {
+    SIM_GUARD(require(net != nullptr, "null network handle");
+              require(std::isfinite(learning_rate) && learning_rate > 0.f, "invalid learning rate");
+              vb::Workspace& ws = sim->sim.workspace(); net->net.set_stream(ws.stream());
+              const double l = net->net.train_step(ws.n(), ws.rhs(), ws.pressure(), ws.control(), learning_rate);
+              if (loss) *loss = l);
+}
+VB_API vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d* sim, vapor_unet* net, double* loss) {
+    SIM_GUARD(require(net != nullptr, "null network handle"); vb::Workspace& ws = sim->sim.workspace();
+              net->net.set_stream(ws.stream());
+              const double l = net->net.evaluate(ws.n(), ws.rhs(), ws.pressure(), ws.control());
+              if (loss) *loss = l);
 }

@@ -2,6 +2,7 @@
 // (GpuMacSimulation3D's role, gpu/GpuMacSimulation3D.cpp:49-264) and staged
 // stages (GpuPressureSolver.cpp / GpuAdvection.cpp).
 #include "engine.hpp"
+#include "unet.hpp"
 
 #include <algorithm>
 #include <climits>
@@ -42,6 +43,7 @@ void DevArray<T>::zero(cudaStream_t s) {
 template struct DevArray<float>;
 template struct DevArray<double>;
 template struct DevArray<uint32_t>;
+template struct DevArray<uint16_t>;
 
 Stream::Stream() { VB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
 Stream::~Stream() {
@@ -236,7 +238,7 @@ static cudaGraphConditionalHandle new_condition(cudaStream_t s) {
 
 void Workspace::project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo,
                         float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
-                        const vapor_linear_solve_options& o, int solver_kind) {
+                        const vapor_linear_solve_options& o, int solver_kind, unet::UNet* warm) {
     const ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
     cudaStream_t s = stream_;
     PhaseTimer& t = timer_;
@@ -244,9 +246,12 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     const bool graph = capturing_;
     const int interval = o.residual_check_interval;
     if (mixed) ensure_mixed();
+    // A device-side while loop is recorded only when the solve has one; a
+    // conditional handle that no node uses makes graph instantiation fail.
+    const bool loop = graph && (mixed || !o.fixed_iterations || o.max_iterations > interval);
     LoopCond cond;
     cudaGraphConditionalHandle handle = 0;
-    if (graph) {
+    if (loop) {
         handle = new_condition(s);
         cond.active = 1;
         cond.handle = (unsigned long long)handle;
@@ -258,11 +263,12 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
         return *done_host_ != 0;
     };
     // k guarded colour-pair sweeps on x (right-hand side rhs) on stream st.
+    // Inner sweeps of the mixed solver use the divide-free relaxation.
     auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean) {
         t.begin(VAPOR_PHASE_SOR);
         for (int j = 0; j < k; ++j) {
-            launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st);
-            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st);
+            launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
+            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
         }
         t.end(VAPOR_PHASE_SOR, 2LL * k);
     };
@@ -278,7 +284,8 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     if (mixed) {
         // FP32 red-black sweeps on the error equation, re-centred in FP64 at
         // every residual check (the oracle's refinementSolve).
-        VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
+        if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);  // x0 = network prediction
+        else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
         auto recentre = [&](cudaStream_t st, int done_sweeps, bool accumulate) {
             t.begin(VAPOR_PHASE_RESIDUAL);
             launch_refine_residual(a, b_.p, p_.p, r32_.p, ctrl_, st);
@@ -309,11 +316,12 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
         launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
         t.end(VAPOR_PHASE_GRADIENT, 5);
     } else {
+        if (warm) warm->infer_into(n_, b_.p, ctrl_, p_.p, nullptr);  // x0 = network prediction
         if (o.fixed_iterations) {
             // Intermediate residual checks cannot change a fixed-budget solve:
             // the final residual and convergence are recomputed after the
             // pressure gauge (CpuPressureSolver3D.cpp:50-56).
-            if (graph && o.max_iterations > interval) {
+            if (loop) {
                 add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) {
                     sweeps(bs, interval, 0, p_.p, b_.p, true);
                     launch_check(ctrl_, interval, true, false, cond, bs);
@@ -522,22 +530,34 @@ void Simulation::record_step(float dt) {
         advect_velocity(half, S_, S_, T_);  // T = advected (tilde)
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
                     vel_[U_][0].p, vel_[U_][1].p, vel_[U_][2].p, half, p.sor_omega, 6.f, o,
-                    p.solver_kind);  // S = projected, U = hat
+                    p.solver_kind, warm_);  // S = projected, U = hat
         advect_velocity(half, U_, S_, T_);
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
-                    nullptr, nullptr, nullptr, half, p.sor_omega, 6.f, o, p.solver_kind);
+                    nullptr, nullptr, nullptr, half, p.sor_omega, 6.f, o, p.solver_kind, warm_);
     } else {
         // MacGridFluidSolver3D::stepNoReflect (MacGridFluidSolver3D.cpp:230-245).
         advect_velocity(dt, S_, S_, T_);
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
                     nullptr, nullptr, nullptr, dt, p.sor_omega, 6.f, solve_options(p.project_iterations),
-                    p.solver_kind);
+                    p.solver_kind, warm_);
     }
     // Smoke transport through the projected velocity, then dissipation
     // (MacGridFluidSolver3D.cpp:183-190) fused as a post-scale.
     const float factor = std::clamp(1.0f - p.smoke_decay * dt, 0.0f, 1.0f);
     ws_.advect(CELL, dt, p.cfl_mc, p.mac_cormack_smoke != 0, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
                vel_[S_][2].p, dens_[1 - cur_].p, factor);
+}
+
+void Simulation::set_warm_start(unet::UNet* net) {
+    if (net && (ws_.n() % 4 != 0 || ws_.n() < 8))
+        fail(VAPOR_INVALID_ARGUMENT, "the warm-start network needs n divisible by 4 (n >= 8)");
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+    release_graphs();
+    warm_ = net;
+    if (warm_) {
+        warm_->set_stream(ws_.stream());
+        warm_->prepare(ws_.n());
+    }
 }
 
 void Simulation::release_graphs() {
@@ -565,6 +585,10 @@ void Simulation::advance(float dt) {
             noise_.allocate(need);
         }
         if (params.solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT) ws_.ensure_mixed();
+        if (warm_) {
+            warm_->set_stream(ws_.stream());
+            warm_->prepare(ws_.n());
+        }
     }
     cudaStream_t s = ws_.stream();
     if (!use_graphs_ || ws_.timer().enabled()) {
@@ -598,7 +622,11 @@ void Simulation::advance(float dt) {
         VB_CUDA(cudaStreamEndCapture(s, &graph));
         const cudaError_t e = cudaGraphInstantiate(&slot.exec, graph, 0);
         cudaGraphDestroy(graph);
-        VB_CUDA(e);
+        if (e != cudaSuccess) {
+            slot.exec = nullptr;
+            (void)cudaGetLastError();  // do not leave the failure as the runtime's last error
+            VB_CUDA(e);
+        }
         slot.key = key;
     }
     VB_CUDA(cudaGraphLaunch(slot.exec, s));

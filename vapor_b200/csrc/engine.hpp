@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -11,6 +12,9 @@
 #include "kernels.hpp"
 
 namespace vb {
+namespace unet {
+class UNet;
+}
 
 // Error carried to the C ABI, where it becomes a vapor_status.
 struct Error : std::runtime_error {
@@ -18,6 +22,9 @@ struct Error : std::runtime_error {
     Error(vapor_status c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 [[noreturn]] void fail(vapor_status code, const std::string& message);
+// Runs f, turning exceptions into a vapor_status and the per-thread message
+// returned by vapor_last_error (the C ABI's guard, capi.cu).
+vapor_status guard(const std::function<void()>& f);
 void cuda_check(cudaError_t e, const char* what);
 #define VB_CUDA(call) ::vb::cuda_check((call), #call)
 
@@ -97,7 +104,9 @@ public:
     // solves read the stop flag after each residual check.
     void project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo, float* uh,
                  float* vh, float* wh, float dt, float omega, float diagonal_floor,
-                 const vapor_linear_solve_options& options, int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR);
+                 const vapor_linear_solve_options& options, int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR,
+                 unet::UNet* warm_start = nullptr);
+    float* rhs() { return b_.p; }
     void advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
                 const float* w, float* out, float post_scale);
     // Waits for the stream and returns the last projection result; raises
@@ -170,6 +179,11 @@ public:
     // CUDA-graph replay of whole steps (default on; phase timing uses the
     // eager path).
     void set_graphs(bool on) { use_graphs_ = on; }
+    // Learned warm start for every projection (null: start from zero, the
+    // reference's x = 0). The network is bound to this simulation's stream.
+    void set_warm_start(unet::UNet* net);
+    unet::UNet* warm_start() const { return warm_; }
+    Workspace& workspace() { return ws_; }
 
 private:
     bool emitter_box(float cx, float cy, float cz, float dt, EmitterBox& e) const;
@@ -190,6 +204,7 @@ private:
     };
     CachedGraph graphs_[2];
     bool use_graphs_ = true;
+    unet::UNet* warm_ = nullptr;
 
     Stream stream_;
     Workspace ws_;

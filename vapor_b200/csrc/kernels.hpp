@@ -107,8 +107,10 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
 // `subtract_mean` the right-hand side is b - ctrl->rhs_mean_f, else b. A
 // guarded sweep returns at once when the solve is done or when
 // ctrl->iterations + sweep_index reaches the iteration budget.
+// `exact` = false selects the mixed solver's divide-free relaxation
+// x += (b - off - diag x) * (omega / max(diag, floor)).
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s);
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true);
 // Mixed precision: x64[1-cur] = x64[cur] + e (FP64), r32 = float(b' - A x)
 // with the FP64 residual norm into ctrl->res_bits.
 void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,

@@ -148,9 +148,17 @@ __global__ void k_rhs_finish(ProjControl* ctrl, const double* __restrict__ parti
 // loads and needs hw % 4 == 0). The x-neighbours of slot i are the other
 // colour's slots i-1+s and i+s (s = (y+z+colour)&1, x = 2i+s); the y- and
 // z-neighbours are slot i of the adjacent rows of the other colour.
-template <int VEC>
+// EXACT = false is the mixed solver's inner sweep: the relaxation is a
+// multiplication by wr[diag] = omega / max(diag, floor) (FP32, from the host)
+// instead of omega * t / max(diag, floor); the oracle's refinement uses the
+// same formula.
+struct RelaxTable {
+    float w[7];
+};
+template <int VEC, bool EXACT>
 __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float omega, float floor_diag,
-                                                     float* __restrict__ xs, const float* __restrict__ bs,
+                                                     RelaxTable wr, float* __restrict__ xs,
+                                                     const float* __restrict__ bs,
                                                      const ProjControl* __restrict__ ctrl, int guarded,
                                                      int sweep_index, int subtract_mean) {
     if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
@@ -222,9 +230,13 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
         if (y + 1 < n) off += -1.f * yp[k];
         if (z > 0) off += -1.f * zm[k];
         if (z + 1 < n) off += -1.f * zp[k];
-        const float relax = maxf_ref(diag, floor_diag);
         const float bi = subtract_mean ? bv[k] - bm : bv[k];
-        res[k] = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
+        if (EXACT) {
+            const float relax = maxf_ref(diag, floor_diag);
+            res[k] = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
+        } else {
+            res[k] = xo[k] + (bi - off - diag * xo[k]) * wr.w[int(diag)];
+        }
     }
     if (VEC == 4) {
         *reinterpret_cast<float4*>(own + i0) = make_float4(res[0], res[1], res[2], res[3]);
@@ -233,45 +245,71 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
     }
 }
 
-// Mixed precision re-centring: x_out = x_in + e and r32 = float(b' - A x_out),
-// both in FP64, with the neighbour order of the reference residual.
-__global__ void __launch_bounds__(kThreads) k_refine_residual(Grid g, const float* __restrict__ b,
-                                                              const float* __restrict__ e,
-                                                              float* __restrict__ r32, ProjControl* ctrl) {
+// Mixed precision re-centring on the split layout: x_out = x_in + e and
+// r32 = float(b' - A x_out), both in FP64 with the neighbour order of the
+// reference residual. One thread per VEC consecutive slots of one row of one
+// colour (blockIdx.z); neighbours are the other colour's x_in + e.
+template <int VEC>
+__global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __restrict__ bs,
+                                                        const float* __restrict__ es, float* __restrict__ r32,
+                                                        ProjControl* ctrl) {
     __shared__ double s_max[32];
     const double* __restrict__ xin = ctrl->x64[ctrl->x64_cur];
     double* __restrict__ xout = ctrl->x64[1 - ctrl->x64_cur];
     const int n = g.n;
     const RBLayout L = rb_layout(n);
-    const size_t cells = size_t(n) * n * n;
+    const int hw = L.hw, groups = hw / VEC;
+    const int colour = blockIdx.z;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y;
+    const int y = t / groups;
+    const bool active = y < n;
     const float bm = ctrl->rhs_mean_f;
-    double r = 0.0;
+    double rmax = 0.0;
     unsigned int bad = 0u;
-    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
-        int i, j, k;
-        decode_cell(c, n, i, j, k);
-        auto xv = [&](int a, int bb, int cc) {
-            const size_t id = rb_index(L, a, bb, cc);
-            return xin[id] + double(e[id]);
-        };
-        const size_t me = rb_index(L, i, j, k);
-        const double xc = xin[me] + double(e[me]);
-        double ax = double(neighbours(n, i, j, k)) * xc;
-        if (i > 0) ax -= xv(i - 1, j, k);
-        if (i + 1 < n) ax -= xv(i + 1, j, k);
-        if (j > 0) ax -= xv(i, j - 1, k);
-        if (j + 1 < n) ax -= xv(i, j + 1, k);
-        if (k > 0) ax -= xv(i, j, k - 1);
-        if (k + 1 < n) ax -= xv(i, j, k + 1);
-        const float bi = b[me] - bm;
-        const double res = double(bi) - ax;
-        if (!isfinite(res)) bad = 1u;
-        xout[me] = xc;
-        r32[me] = float(res);
-        const double a = fabs(res);
-        r = r < a ? a : r;
+    if (active) {
+        const int i0 = (t - y * groups) * VEC;
+        const int s = (y + z + colour) & 1;
+        const size_t row = (size_t(z) * n + y) * hw;
+        const size_t own = size_t(colour) * L.stride + row, oth = size_t(1 - colour) * L.stride + row;
+        const size_t yo = size_t(hw), zo = size_t(n) * hw;
+        auto nb = [&](size_t idx) { return xin[oth + idx] + double(es[oth + idx]); };
+        double xo[VEC], xl[VEC + 1], ym[VEC], yp[VEC], zm[VEC], zp[VEC];
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            xo[k] = xin[own + i0 + k] + double(es[own + i0 + k]);
+            ym[k] = y > 0 ? nb(i0 + k - yo) : 0.0;
+            yp[k] = y + 1 < n ? nb(i0 + k + yo) : 0.0;
+            zm[k] = z > 0 ? nb(i0 + k - zo) : 0.0;
+            zp[k] = z + 1 < n ? nb(i0 + k + zo) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k <= VEC; ++k) {
+            const int slot = i0 - 1 + s + k;
+            xl[k] = (slot >= 0 && slot < hw) ? nb(size_t(slot)) : 0.0;
+        }
+        const int ny = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            const int xc = 2 * (i0 + k) + s;
+            if (xc >= n) continue;
+            double ax = double((xc > 0) + (xc + 1 < n) + ny) * xo[k];
+            if (xc > 0) ax -= xl[k];
+            if (xc + 1 < n) ax -= xl[k + 1];
+            if (y > 0) ax -= ym[k];
+            if (y + 1 < n) ax -= yp[k];
+            if (z > 0) ax -= zm[k];
+            if (z + 1 < n) ax -= zp[k];
+            const float bi = bs[own + i0 + k] - bm;
+            const double res = double(bi) - ax;
+            if (!isfinite(res)) bad = 1u;
+            xout[own + i0 + k] = xo[k];
+            r32[own + i0 + k] = float(res);
+            const double aa = fabs(res);
+            rmax = rmax < aa ? aa : rmax;
+        }
     }
-    const double br = block_max(r, s_max);
+    const double br = block_max(rmax, s_max);
     const int any_bad = __syncthreads_or(int(bad));
     if (threadIdx.x == 0) {
         atomic_max_nonneg(&ctrl->res_bits, br);
@@ -670,18 +708,21 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
 }
 
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s) {
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact) {
     const int n = a.g.n;
     const RBLayout L = rb_layout(n);
+    RelaxTable wr;
+    for (int d = 0; d < 7; ++d) wr.w[d] = a.omega / std::max(float(d), a.diagonal_floor);
+    const int g = guarded ? 1 : 0, m = subtract_mean ? 1 : 0;
     count_launch();
     if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n);
-        k_sor_rb<4><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, x, b, ctrl, guarded ? 1 : 0,
-                                              sweep_index, subtract_mean ? 1 : 0);
+        if (exact) k_sor_rb<4, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
+        else k_sor_rb<4, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
     } else {
         const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n);
-        k_sor_rb<1><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, x, b, ctrl, guarded ? 1 : 0,
-                                              sweep_index, subtract_mean ? 1 : 0);
+        if (exact) k_sor_rb<1, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
+        else k_sor_rb<1, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
     }
 }
 
@@ -693,9 +734,16 @@ void launch_unsplit_pressure(const Grid& g, const float* p, const ProjControl* c
 
 void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
                             ProjControl* ctrl, cudaStream_t s) {
-    const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
+    const int n = a.g.n;
+    const RBLayout L = rb_layout(n);
     count_launch();
-    k_refine_residual<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
+    if (L.hw % 4 == 0) {
+        const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n, 2);
+        k_refine_rb<4><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
+    } else {
+        const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n, 2);
+        k_refine_rb<1><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
+    }
 }
 
 void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,

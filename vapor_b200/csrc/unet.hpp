@@ -1,0 +1,156 @@
+// Learned warm start for the pressure solve: a 3-level 3D U-Net mapping the
+// normalized divergence (and a solid mask) to the normalized pressure.
+//
+//   level 1 (n^3):      conv 16->16, conv 16->16          (input: 2 real channels padded to 16)
+//   level 2 ((n/2)^3):  avgpool, conv 16->32, conv 32->32
+//   level 3 ((n/4)^3):  avgpool, conv 32->64, conv 64->64
+//   decoder 2:          upsample 64 ++ skip 32 = 96 -> conv 96->32, conv 32->32
+//   decoder 1:          upsample 32 ++ skip 16 = 48 -> conv 48->16, conv 16->16
+//   head:               1x1 conv 16->1 (FP32 output)
+// ReLU after every 3x3x3 convolution; about 0.35 M parameters; BF16 weights
+// and activations, FP32 accumulation, FP32 master weights and Adam state.
+// The problem is linear in the divergence, so inputs and targets are divided
+// by the RMS of the mean-free right-hand side and outputs multiplied back.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <vector>
+
+#include "engine.hpp"
+
+namespace vb {
+namespace unet {
+
+struct ConvArgs {
+    int D, H, W;                  // grid (z, y, x)
+    const __nv_bfloat16* in;      // channels-last, in_stride channels per voxel
+    int in_stride;
+    int cin;                      // multiple of 16
+    const __nv_bfloat16* w;       // [27][cout][cin], tap = (dz+1)*9 + (dy+1)*3 + (dx+1)
+    const float* bias;            // [cout] or null
+    void* out;                    // BF16 or FP32, out_stride channels per voxel
+    int out_stride;
+    int out_offset;
+    int out_fp32;
+    int relu;
+    unsigned int* error;          // set when a bounded wait timed out
+};
+
+struct WGradArgs {
+    int D, H, W;
+    const __nv_bfloat16* g;  // output gradient, channels-last
+    int g_stride, g_offset;
+    const __nv_bfloat16* x;  // layer input, channels-last
+    int x_stride;
+    int cout, cin;           // multiples of 16
+    float* dw;               // [27][cout][cin], accumulated
+};
+
+// Sets the kernels' shared-memory limits (once per device, before use).
+void configure_conv_kernels();
+void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
+void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
+void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,
+                       __nv_bfloat16* out, cudaStream_t s);
+void launch_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* in, int in_stride, __nv_bfloat16* out,
+                     cudaStream_t s);
+void launch_upsample2(int d, int h, int w, int C, const __nv_bfloat16* in, __nv_bfloat16* out, int out_stride,
+                      cudaStream_t s);
+void launch_head(long V, int C, const __nv_bfloat16* act, const float* w, const float* bias, float* out,
+                 cudaStream_t s);
+void launch_mean(long V, const float* a, double* partial, double* mean, cudaStream_t s);
+void launch_store_warm_start(int n, const float* p, const float* scale, const double* mean, float* x_split,
+                             double* x64_split, cudaStream_t s);
+void launch_target(int n, const float* p_split, const ProjControl* ctrl, const float* scale, float* target,
+                   cudaStream_t s);
+void launch_loss_grad(long V, const float* p, const float* t, float* diff, double* partial, double* mean_e,
+                      float* grad, cudaStream_t s);
+void launch_head_backward(long V, int C, const __nv_bfloat16* act, const float* w, const float* g,
+                          __nv_bfloat16* dact, float* dw, float* db, cudaStream_t s);
+void launch_relu_mask(long V, int C, const __nv_bfloat16* act, int act_stride, int act_offset, __nv_bfloat16* g,
+                      int g_stride, int g_offset, cudaStream_t s);
+void launch_bias_grad(long V, int C, const __nv_bfloat16* g, int g_stride, int g_offset, float* db, cudaStream_t s);
+void launch_flip_weights(int cout, int cin, const __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s);
+void launch_avgpool2_backward(int D, int H, int W, int C, const __nv_bfloat16* dout, __nv_bfloat16* din,
+                              int din_stride, int din_offset, bool add, cudaStream_t s);
+void launch_upsample2_backward(int d, int h, int w, int C, const __nv_bfloat16* dfine, int fine_stride,
+                               __nv_bfloat16* dcoarse, cudaStream_t s);
+void launch_adam(long count, float* w, float* m, float* v, const float* g, __nv_bfloat16* wb, float lr, int step,
+                 cudaStream_t s);
+void launch_to_bf16(long count, const float* a, __nv_bfloat16* b, cudaStream_t s);
+
+// Parameter block layout: 10 convolutions (3x3x3) then the head.
+struct LayerShape {
+    int cin, cout;
+};
+constexpr int kConvLayers = 10;
+constexpr LayerShape kLayers[kConvLayers] = {{16, 16}, {16, 16}, {16, 32}, {32, 32}, {32, 64},
+                                             {64, 64}, {96, 32}, {32, 32}, {48, 16}, {16, 16}};
+constexpr int kHeadIn = 16;
+
+// All trainable parameters in one FP32 vector: for each conv layer its
+// weights [27][cout][cin] then its bias [cout]; then head weights [16] and
+// head bias [1].
+long parameter_count();
+long weight_offset(int layer);
+long bias_offset(int layer);
+long head_offset();
+
+class UNet {
+public:
+    explicit UNet(cudaStream_t stream);
+    ~UNet();
+    // The stream all later work is ordered on (the owning simulation's).
+    void set_stream(cudaStream_t s) { s_ = s; }
+    cudaStream_t stream() const { return s_; }
+    // Allocates the activation buffers for n (outside any stream capture).
+    void prepare(int n) { ensure(n); }
+    UNet(const UNet&) = delete;
+    UNet& operator=(const UNet&) = delete;
+
+    void set_parameters(const float* host);  // parameter_count() floats
+    void get_parameters(float* host);
+    void init_parameters(unsigned seed);      // He-uniform weights, zero biases
+
+    // Forward on an n^3 grid (n divisible by 4) from the solver's split RHS;
+    // writes the warm start x = scale * (p - mean p) into x_split (FP32) or
+    // x64_split (FP64). Returns nothing; errors raise.
+    void infer_into(int n, const float* b_split, const ProjControl* ctrl, float* x_split, double* x64_split);
+    // One training step on (b, p*) from a finished projection: forward,
+    // loss, backward, Adam. Returns the loss (waits for the device).
+    double train_step(int n, const float* b_split, const float* p_split, const ProjControl* ctrl, float lr);
+    // Forward only and the loss against p* (no update); waits.
+    double evaluate(int n, const float* b_split, const float* p_split, const ProjControl* ctrl);
+    unsigned int error_flag();
+    int adam_steps() const { return step_; }
+    // Raw forward on device channels-last input [n^3][16] -> FP32 output.
+    void forward_features(int n, const __nv_bfloat16* input16, float* out);
+    void backward_from_output(int n, const float* grad_out);  // after forward_features
+    float* gradient() { return grad_.p; }
+
+private:
+    void ensure(int n);
+    void forward(int n);
+    void backward(int n);
+    void conv(int layer, int D, int H, int W, const __nv_bfloat16* in, int in_stride, void* out, int out_stride,
+              int out_offset, bool relu, bool fp32_out = false);
+
+    cudaStream_t s_;
+    int n_ = 0;
+    int step_ = 0;
+    DevArray<float> params_, grad_, m_, v_;
+    DevArray<uint16_t> wbf_;   // BF16 copy of the parameters
+    DevArray<uint16_t> wflip_;  // flipped/transposed weights of one layer
+    // activations (BF16, channels-last)
+    DevArray<uint16_t> in0_, e1a_, dec1_, e2in_, e2a_, dec2_, e3in_, e3a_, e3b_, d2a_, d2b_, d1a_, d1b_;
+    // gradients (BF16)
+    DevArray<uint16_t> g1_, g2_, g3_, g4_;
+    DevArray<float> out_, target_, diff_, gout_;
+    DevArray<double> partial_, scalars_;
+    DevArray<float> scale_;
+    DevArray<uint32_t> error_;
+};
+
+}  // namespace unet
+}  // namespace vb

@@ -1,0 +1,629 @@
+// Kernels of the learned pressure warm start: a 3-level 3D U-Net
+// (16/32/64 channels, 3x3x3 convolutions, BF16 weights and activations, FP32
+// accumulation) and its training (backward + Adam).
+//
+// The 3x3x3 convolutions - forward, and backward with respect to the input
+// (a convolution with the spatially flipped, channel-transposed weights) - run
+// on the tensor cores through k_conv3_tc (tc_conv.cuh). Weight gradients,
+// pooling, upsampling, the 1x1 output head, the loss and Adam are memory-bound
+// or small and run on CUDA cores.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "kernels.hpp"
+#include "tc_conv.cuh"
+#include "unet.hpp"
+
+namespace vb {
+namespace unet {
+namespace {
+
+constexpr int kWaitLimit = 1 << 22;
+
+__device__ __forceinline__ void decode(long v, int H, int W, int& x, int& y, int& z) {
+    x = int(v % W);
+    const long r = v / W;
+    y = int(r % H);
+    z = int(r / H);
+}
+
+template <int N>
+struct TmemColumns {
+    static constexpr int value = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+};
+
+// Implicit-GEMM 3x3x3 convolution on tcgen05 (see tc_conv.cuh for the layout).
+template <int N>
+__global__ void __launch_bounds__(128) k_conv3_tc(ConvArgs a) {
+    constexpr int kStage = 128 * 32 + N * 32;  // A then B, bytes
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const long V = long(a.D) * a.H * a.W;
+    const long v = long(blockIdx.x) * 128 + tid;
+    const bool vin = v < V;
+    int x = 0, y = 0, z = 0;
+    if (vin) decode(v, a.H, a.W, x, y, z);
+
+    constexpr uint32_t kCols = TmemColumns<N>::value;
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), kCols);
+    const uint32_t bar0 = tc::smem_addr(&bars[0]), bar1 = tc::smem_addr(&bars[1]);
+    if (tid == 0) {
+        tc::mbar_init(bar0, 1);
+        tc::mbar_init(bar1, 1);
+        tc::fence_mbarrier_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    const int chunks = a.cin / 16;
+    const int steps = 27 * chunks;
+    constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
+    const uint32_t sbase = tc::smem_addr(smem);
+    const uint32_t arow = uint32_t((tid >> 3) * 256 + (tid & 7) * 16);
+    bool ok = true;
+    for (int s = 0; s < steps; ++s) {
+        const int st = s & 1;
+        const uint32_t bar = st ? bar1 : bar0;
+        if (s >= 2) {
+            const bool mine = tc::mbar_wait(bar, uint32_t((s - 2) >> 1) & 1u, kWaitLimit);
+            if (!__syncthreads_and(mine)) {
+                ok = false;
+                break;
+            }
+        }
+        const int tap = s / chunks, cc = s - tap * chunks;
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        const int xs = x + dx, ys = y + dy, zs = z + dz;
+        const bool valid = vin && xs >= 0 && xs < a.W && ys >= 0 && ys < a.H && zs >= 0 && zs < a.D;
+        const __nv_bfloat16* src =
+            valid ? a.in + ((long(zs) * a.H + ys) * a.W + xs) * a.in_stride + cc * 16 : a.in;
+        const uint32_t abase = sbase + uint32_t(st * kStage);
+        const uint32_t bbase = abase + 128 * 32;
+        tc::cp_async16(abase + arow, src, valid);
+        tc::cp_async16(abase + arow + 128, src + 8, valid);
+        for (int i = tid; i < 2 * N; i += 128) {
+            const int co = i >> 1, kc = i & 1;
+            const __nv_bfloat16* wsrc = a.w + (long(tap) * N + co) * a.cin + cc * 16 + kc * 8;
+            tc::cp_async16(bbase + uint32_t((co >> 3) * 256 + kc * 128 + (co & 7) * 16), wsrc, true);
+        }
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            tc::mma_bf16(tmem, tc::smem_desc(abase, 128, 256), tc::smem_desc(bbase, 128, 256), idesc, s > 0);
+            tc::mma_commit(bar);
+        }
+    }
+    if (ok && steps > 0) {
+        const int last = steps - 1;
+        const bool mine = tc::mbar_wait((last & 1) ? bar1 : bar0, uint32_t(last >> 1) & 1u, kWaitLimit);
+        ok = __syncthreads_and(mine);
+    }
+    tc::tc_fence_after();
+    if (ok) {
+        const uint32_t lane_base = uint32_t(warp * 32) << 16;
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float acc[16];
+            tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
+            if (vin) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    float val = acc[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                    if (a.relu) val = fmaxf(val, 0.f);
+                    const long o = v * a.out_stride + a.out_offset + c0 + i;
+                    if (a.out_fp32) static_cast<float*>(a.out)[o] = val;
+                    else static_cast<__nv_bfloat16*>(a.out)[o] = __float2bfloat16_rn(val);
+                }
+            }
+        }
+    } else {
+        // Drain: wait (bounded) for anything still in flight before freeing TMEM.
+        if (tid == 0) atomicOr(a.error, 1u);
+        tc::mbar_wait(bar0, 0u, kWaitLimit);
+        tc::mbar_wait(bar1, 0u, kWaitLimit);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+}
+
+// ---- CUDA-core kernels -------------------------------------------------------
+
+// Input features: channel 0 = b / scale (from the solver's red-black split RHS,
+// minus the RHS mean), channel 1 = solid mask (0: fluid), channels 2..15 = 0.
+__global__ void k_prep_input(int n, const float* __restrict__ b_split, const ProjControl* __restrict__ ctrl,
+                             const float* __restrict__ scale, __nv_bfloat16* __restrict__ out) {
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const float inv = 1.f / fmaxf(*scale, 1e-30f);
+    const float bm = ctrl ? ctrl->rhs_mean_f : 0.f;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        const float bv = (b_split[rb_index(L, x, y, z)] - bm) * inv;
+        __nv_bfloat16* o = out + v * 16;
+        o[0] = __float2bfloat16_rn(bv);
+#pragma unroll
+        for (int c = 1; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+    }
+}
+
+// Root-mean-square of the mean-free RHS (FP64), the normalization scale.
+__global__ void k_rms(int n, const float* __restrict__ b_split, const ProjControl* __restrict__ ctrl,
+                      double* __restrict__ partial) {
+    __shared__ double s_sum[32];
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const float bm = ctrl ? ctrl->rhs_mean_f : 0.f;
+    double acc = 0.0;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        const double bv = double(b_split[rb_index(L, x, y, z)] - bm);
+        acc += bv * bv;
+    }
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+__global__ void k_rms_finish(const double* __restrict__ partial, int blocks, double count, float* scale) {
+    __shared__ double s_sum[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x) acc += partial[i];
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) *scale = float(sqrt(s / count));
+}
+
+// 2x average pooling, channels-last BF16 (input dims even).
+__global__ void k_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* __restrict__ in, int in_stride,
+                           __nv_bfloat16* __restrict__ out) {
+    const int d = D / 2, h = H / 2, w = W / 2;
+    const long total = long(d) * h * w * C;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i % C);
+        const long v = i / C;
+        int x, y, z;
+        decode(v, h, w, x, y, z);
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int xx = 2 * x + (k & 1), yy = 2 * y + ((k >> 1) & 1), zz = 2 * z + (k >> 2);
+            s += __bfloat162float(in[((long(zz) * H + yy) * W + xx) * in_stride + c]);
+        }
+        out[v * C + c] = __float2bfloat16_rn(s * 0.125f);
+    }
+}
+
+// Nearest 2x upsampling of a coarse tensor into channels [0, C) of a fine
+// buffer with channel stride out_stride.
+__global__ void k_upsample2(int d, int h, int w, int C, const __nv_bfloat16* __restrict__ in,
+                            __nv_bfloat16* __restrict__ out, int out_stride) {
+    const int D = 2 * d, H = 2 * h, W = 2 * w;
+    const long total = long(D) * H * W * C;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i % C);
+        const long v = i / C;
+        int x, y, z;
+        decode(v, H, W, x, y, z);
+        out[v * out_stride + c] = in[((long(z / 2) * h + y / 2) * w + x / 2) * C + c];
+    }
+}
+
+// 1x1 output head: p[v] = bias + sum_c w[c] * act[v, c] (FP32 out).
+__global__ void k_head(long V, int C, const __nv_bfloat16* __restrict__ act, const float* __restrict__ w,
+                       const float* __restrict__ bias, float* __restrict__ out) {
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        float s = bias[0];
+        for (int c = 0; c < C; ++c) s += w[c] * __bfloat162float(act[v * C + c]);
+        out[v] = s;
+    }
+}
+
+// Warm start into the solver's split iterate: x = scale * (p - mean p).
+__global__ void k_store_warm_start(int n, const float* __restrict__ p, const float* __restrict__ scale,
+                                   const double* __restrict__ mean, float* __restrict__ x_split) {
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const float s = *scale, m = float(*mean);
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        x_split[rb_index(L, x, y, z)] = s * (p[v] - m);
+    }
+}
+__global__ void k_store_warm_start64(int n, const float* __restrict__ p, const float* __restrict__ scale,
+                                     const double* __restrict__ mean, double* __restrict__ x_split) {
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const double s = double(*scale), m = *mean;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        x_split[rb_index(L, x, y, z)] = s * (double(p[v]) - m);
+    }
+}
+
+// Deterministic FP64 mean of an FP32 array (partials then one block).
+__global__ void k_sum(long V, const float* __restrict__ a, double* __restrict__ partial) {
+    __shared__ double s_sum[32];
+    double acc = 0.0;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x)
+        acc += double(a[v]);
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+__global__ void k_mean_finish(const double* __restrict__ partial, int blocks, double count, double* mean) {
+    __shared__ double s_sum[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x) acc += partial[i];
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) *mean = s / count;
+}
+
+// Training target: zero-mean pressure / scale from the solver's split iterate.
+__global__ void k_target(int n, const float* __restrict__ p_split, const ProjControl* __restrict__ ctrl,
+                         const float* __restrict__ scale, float* __restrict__ target) {
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const float pm = ctrl->p_mean_f;
+    const float inv = 1.f / fmaxf(*scale, 1e-30f);
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        target[v] = (p_split[rb_index(L, x, y, z)] - pm) * inv;
+    }
+}
+
+// Loss L = mean(((p - mean p) - t)^2) and dL/dp = 2/V * (e - mean e) with
+// e = p - t (t has zero mean). Writes per-block partial losses.
+__global__ void k_loss_grad(long V, const float* __restrict__ p, const float* __restrict__ t,
+                            const double* __restrict__ mean_e, float* __restrict__ grad,
+                            double* __restrict__ partial) {
+    __shared__ double s_sum[32];
+    const double me = *mean_e;
+    double acc = 0.0;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        const double e = double(p[v]) - double(t[v]) - me;
+        acc += e * e;
+        grad[v] = float(2.0 * e / double(V));
+    }
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+__global__ void k_diff(long V, const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out) {
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x)
+        out[v] = a[v] - b[v];
+}
+
+// Head backward: d_act[v,c] = g[v] * w[c] (BF16, masked by act > 0 for the
+// ReLU before the head), dw[c] += sum g*act, db += sum g.
+__global__ void k_head_backward(long V, int C, const __nv_bfloat16* __restrict__ act, const float* __restrict__ w,
+                                const float* __restrict__ g, __nv_bfloat16* __restrict__ dact,
+                                float* __restrict__ dw, float* __restrict__ db) {
+    float lw[64], lb = 0.f;
+    for (int c = 0; c < C; ++c) lw[c] = 0.f;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        const float gv = g[v];
+        lb += gv;
+        for (int c = 0; c < C; ++c) {
+            const float a = __bfloat162float(act[v * C + c]);
+            lw[c] += gv * a;
+            dact[v * C + c] = __float2bfloat16_rn(a > 0.f ? gv * w[c] : 0.f);
+        }
+    }
+    for (int c = 0; c < C; ++c) atomicAdd(&dw[c], lw[c]);
+    atomicAdd(db, lb);
+}
+
+// ReLU backward in place on a gradient with channel stride: g *= (act > 0).
+__global__ void k_relu_mask(long V, int C, const __nv_bfloat16* __restrict__ act, int act_stride, int act_offset,
+                            __nv_bfloat16* __restrict__ g, int g_stride, int g_offset) {
+    const long total = V * C;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i % C);
+        const long v = i / C;
+        if (!(__bfloat162float(act[v * act_stride + act_offset + c]) > 0.f))
+            g[v * g_stride + g_offset + c] = __float2bfloat16_rn(0.f);
+    }
+}
+
+// Bias gradient: db[co] += sum_v g[v, co].
+__global__ void k_bias_grad(long V, int C, const __nv_bfloat16* __restrict__ g, int g_stride, int g_offset,
+                            float* __restrict__ db) {
+    __shared__ float s_acc[128];
+    if (threadIdx.x < C) s_acc[threadIdx.x] = 0.f;
+    __syncthreads();
+    const int c = threadIdx.x % C;
+    const int lanes = blockDim.x / C;
+    const int l = threadIdx.x / C;
+    float acc = 0.f;
+    if (l < lanes)
+        for (long v = long(blockIdx.x) * lanes + l; v < V; v += long(gridDim.x) * lanes)
+            acc += __bfloat162float(g[v * g_stride + g_offset + c]);
+    if (l < lanes) atomicAdd(&s_acc[c], acc);
+    __syncthreads();
+    if (threadIdx.x < C) atomicAdd(&db[threadIdx.x], s_acc[threadIdx.x]);
+}
+
+// Weight gradient of a 3x3x3 convolution on CUDA cores:
+// dw[tap][co][ci] += sum_v g[v, co] * x[v + tap, ci]. One block per
+// (tap, 16-co block, 16-ci block, voxel chunk); thread (co, ci) accumulates.
+__global__ void __launch_bounds__(256) k_conv3_wgrad(WGradArgs a) {
+    __shared__ float sg[64][17];
+    __shared__ float sx[64][17];
+    const int tap = blockIdx.y;
+    const int cob = blockIdx.z % (a.cout / 16), cib = blockIdx.z / (a.cout / 16);
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const long V = long(a.D) * a.H * a.W;
+    const long chunk = (V + gridDim.x - 1) / gridDim.x;
+    const long v_begin = long(blockIdx.x) * chunk, v_end = min(V, v_begin + chunk);
+    const int tco = threadIdx.x >> 4, tci = threadIdx.x & 15;
+    float acc = 0.f;
+    for (long v0 = v_begin; v0 < v_end; v0 += 64) {
+        // stage 64 voxels x 16 channels of g and of the shifted input
+        for (int i = threadIdx.x; i < 64 * 16; i += 256) {
+            const int r = i >> 4, c = i & 15;
+            const long v = v0 + r;
+            float gv = 0.f, xv = 0.f;
+            if (v < v_end) {
+                gv = __bfloat162float(a.g[v * a.g_stride + a.g_offset + cob * 16 + c]);
+                int x, y, z;
+                decode(v, a.H, a.W, x, y, z);
+                const int xs = x + dx, ys = y + dy, zs = z + dz;
+                if (xs >= 0 && xs < a.W && ys >= 0 && ys < a.H && zs >= 0 && zs < a.D)
+                    xv = __bfloat162float(a.x[((long(zs) * a.H + ys) * a.W + xs) * a.x_stride + cib * 16 + c]);
+            }
+            sg[r][c] = gv;
+            sx[r][c] = xv;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int r = 0; r < 64; ++r) acc += sg[r][tco] * sx[r][tci];
+        __syncthreads();
+    }
+    atomicAdd(&a.dw[(long(tap) * a.cout + cob * 16 + tco) * a.cin + cib * 16 + tci], acc);
+}
+
+// Flip and transpose 3x3x3 weights for the input-gradient convolution:
+// wt[26 - tap][ci][co] = w[tap][co][ci] (BF16).
+__global__ void k_flip_weights(int cout, int cin, const __nv_bfloat16* __restrict__ w,
+                               __nv_bfloat16* __restrict__ wt) {
+    const long total = 27L * cout * cin;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int ci = int(i % cin);
+        const long r = i / cin;
+        const int co = int(r % cout);
+        const int tap = int(r / cout);
+        wt[(long(26 - tap) * cin + ci) * cout + co] = w[i];
+    }
+}
+
+// avgpool backward: d_in[fine] = d_out[coarse] / 8 (into channels with stride).
+__global__ void k_avgpool2_backward(int D, int H, int W, int C, const __nv_bfloat16* __restrict__ dout,
+                                    __nv_bfloat16* __restrict__ din, int din_stride, int din_offset, int add) {
+    const long total = long(D) * H * W * C;
+    const int h = H / 2, w = W / 2;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i % C);
+        const long v = i / C;
+        int x, y, z;
+        decode(v, H, W, x, y, z);
+        float g = __bfloat162float(dout[((long(z / 2) * h + y / 2) * w + x / 2) * C + c]) * 0.125f;
+        __nv_bfloat16& o = din[v * din_stride + din_offset + c];
+        if (add) g += __bfloat162float(o);
+        o = __float2bfloat16_rn(g);
+    }
+}
+
+// upsample backward: d_coarse[c] = sum of the 8 fine gradients of channel c.
+__global__ void k_upsample2_backward(int d, int h, int w, int C, const __nv_bfloat16* __restrict__ dfine,
+                                     int fine_stride, __nv_bfloat16* __restrict__ dcoarse) {
+    const long total = long(d) * h * w * C;
+    const int H = 2 * h, W = 2 * w;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i % C);
+        const long v = i / C;
+        int x, y, z;
+        decode(v, h, w, x, y, z);
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int xx = 2 * x + (k & 1), yy = 2 * y + ((k >> 1) & 1), zz = 2 * z + (k >> 2);
+            s += __bfloat162float(dfine[((long(zz) * H + yy) * W + xx) * fine_stride + c]);
+        }
+        dcoarse[v * C + c] = __float2bfloat16_rn(s);
+    }
+}
+
+// Adam (decoupled weight decay off), FP32 master weights, BF16 copy.
+__global__ void k_adam(long count, float* __restrict__ w, float* __restrict__ m, float* __restrict__ vv,
+                       const float* __restrict__ g, __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += long(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * vv[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        vv[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        if (wb) wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+__global__ void k_to_bf16(long count, const float* __restrict__ a, __nv_bfloat16* __restrict__ b) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += long(gridDim.x) * blockDim.x)
+        b[i] = __float2bfloat16_rn(a[i]);
+}
+
+int blocks_for(long count) { return int(std::max<long>(1, std::min<long>((count + 255) / 256, 148L * 16))); }
+
+// Dynamic shared memory per block: enough that at most 512 / columns blocks
+// share an SM, so tensor-memory allocation never waits on another block.
+template <int N>
+int conv_smem_bytes() {
+    constexpr int stage = 128 * 32 + N * 32;
+    constexpr int per_sm = 512 / TmemColumns<N>::value;
+    const int cap = (227 * 1024) / (per_sm + 1) + 1024;
+    return std::max(2 * stage, std::min(cap, 227 * 1024 - 1024));
+}
+
+template <int N>
+void configure_n() {
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem_bytes<N>()));
+}
+
+template <int N>
+void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
+    const long V = long(a.D) * a.H * a.W;
+    count_launch();
+    k_conv3_tc<N><<<unsigned((V + 127) / 128), 128, conv_smem_bytes<N>(), s>>>(a);
+}
+
+}  // namespace
+
+void configure_conv_kernels() {
+    configure_n<16>();
+    configure_n<32>();
+    configure_n<48>();
+    configure_n<64>();
+    configure_n<96>();
+}
+
+void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s) {
+    switch (cout) {
+        case 16: launch_conv_n<16>(a, s); break;
+        case 32: launch_conv_n<32>(a, s); break;
+        case 48: launch_conv_n<48>(a, s); break;
+        case 64: launch_conv_n<64>(a, s); break;
+        case 96: launch_conv_n<96>(a, s); break;
+        default: fail(VAPOR_INVALID_ARGUMENT, "unsupported convolution output width");
+    }
+}
+
+void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s) {
+    const long V = long(a.D) * a.H * a.W;
+    const int chunks = int(std::max<long>(1, std::min<long>(V / 4096, 256)));
+    const dim3 grid(chunks, 27, (a.cout / 16) * (a.cin / 16));
+    count_launch();
+    k_conv3_wgrad<<<grid, 256, 0, s>>>(a);
+}
+
+void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,
+                       __nv_bfloat16* out, cudaStream_t s) {
+    const long V = long(n) * n * n;
+    const int blocks = std::min(blocks_for(V), 1184);
+    count_launch();
+    k_rms<<<blocks, 256, 0, s>>>(n, b_split, ctrl, partial);
+    count_launch();
+    k_rms_finish<<<1, 1024, 0, s>>>(partial, blocks, double(V), scale);
+    count_launch();
+    k_prep_input<<<blocks_for(V), 256, 0, s>>>(n, b_split, ctrl, scale, out);
+}
+
+void launch_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* in, int in_stride, __nv_bfloat16* out,
+                     cudaStream_t s) {
+    count_launch();
+    k_avgpool2<<<blocks_for(long(D) * H * W * C / 8), 256, 0, s>>>(D, H, W, C, in, in_stride, out);
+}
+
+void launch_upsample2(int d, int h, int w, int C, const __nv_bfloat16* in, __nv_bfloat16* out, int out_stride,
+                      cudaStream_t s) {
+    count_launch();
+    k_upsample2<<<blocks_for(8L * d * h * w * C), 256, 0, s>>>(d, h, w, C, in, out, out_stride);
+}
+
+void launch_head(long V, int C, const __nv_bfloat16* act, const float* w, const float* bias, float* out,
+                 cudaStream_t s) {
+    count_launch();
+    k_head<<<blocks_for(V), 256, 0, s>>>(V, C, act, w, bias, out);
+}
+
+void launch_mean(long V, const float* a, double* partial, double* mean, cudaStream_t s) {
+    const int blocks = std::min(blocks_for(V), 1184);
+    count_launch();
+    k_sum<<<blocks, 256, 0, s>>>(V, a, partial);
+    count_launch();
+    k_mean_finish<<<1, 1024, 0, s>>>(partial, blocks, double(V), mean);
+}
+
+void launch_store_warm_start(int n, const float* p, const float* scale, const double* mean, float* x_split,
+                             double* x64_split, cudaStream_t s) {
+    const long V = long(n) * n * n;
+    count_launch();
+    if (x64_split) k_store_warm_start64<<<blocks_for(V), 256, 0, s>>>(n, p, scale, mean, x64_split);
+    else k_store_warm_start<<<blocks_for(V), 256, 0, s>>>(n, p, scale, mean, x_split);
+}
+
+void launch_target(int n, const float* p_split, const ProjControl* ctrl, const float* scale, float* target,
+                   cudaStream_t s) {
+    count_launch();
+    k_target<<<blocks_for(long(n) * n * n), 256, 0, s>>>(n, p_split, ctrl, scale, target);
+}
+
+void launch_loss_grad(long V, const float* p, const float* t, float* diff, double* partial, double* mean_e,
+                      float* grad, cudaStream_t s) {
+    const int blocks = std::min(blocks_for(V), 1184);
+    count_launch();
+    k_diff<<<blocks_for(V), 256, 0, s>>>(V, p, t, diff);
+    launch_mean(V, diff, partial, mean_e, s);
+    count_launch();
+    k_loss_grad<<<blocks, 256, 0, s>>>(V, p, t, mean_e, grad, partial);
+}
+
+void launch_head_backward(long V, int C, const __nv_bfloat16* act, const float* w, const float* g,
+                          __nv_bfloat16* dact, float* dw, float* db, cudaStream_t s) {
+    count_launch();
+    k_head_backward<<<std::min(blocks_for(V), 592), 256, 0, s>>>(V, C, act, w, g, dact, dw, db);
+}
+
+void launch_relu_mask(long V, int C, const __nv_bfloat16* act, int act_stride, int act_offset, __nv_bfloat16* g,
+                      int g_stride, int g_offset, cudaStream_t s) {
+    count_launch();
+    k_relu_mask<<<blocks_for(V * C), 256, 0, s>>>(V, C, act, act_stride, act_offset, g, g_stride, g_offset);
+}
+
+void launch_bias_grad(long V, int C, const __nv_bfloat16* g, int g_stride, int g_offset, float* db, cudaStream_t s) {
+    count_launch();
+    k_bias_grad<<<std::min(blocks_for(V), 1184), 256, 0, s>>>(V, C, g, g_stride, g_offset, db);
+}
+
+void launch_flip_weights(int cout, int cin, const __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s) {
+    count_launch();
+    k_flip_weights<<<blocks_for(27L * cout * cin), 256, 0, s>>>(cout, cin, w, wt);
+}
+
+void launch_avgpool2_backward(int D, int H, int W, int C, const __nv_bfloat16* dout, __nv_bfloat16* din,
+                              int din_stride, int din_offset, bool add, cudaStream_t s) {
+    count_launch();
+    k_avgpool2_backward<<<blocks_for(long(D) * H * W * C), 256, 0, s>>>(D, H, W, C, dout, din, din_stride,
+                                                                         din_offset, add ? 1 : 0);
+}
+
+void launch_upsample2_backward(int d, int h, int w, int C, const __nv_bfloat16* dfine, int fine_stride,
+                               __nv_bfloat16* dcoarse, cudaStream_t s) {
+    count_launch();
+    k_upsample2_backward<<<blocks_for(long(d) * h * w * C), 256, 0, s>>>(d, h, w, C, dfine, fine_stride, dcoarse);
+}
+
+void launch_adam(long count, float* w, float* m, float* v, const float* g, __nv_bfloat16* wb, float lr, int step,
+                 cudaStream_t s) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
+    count_launch();
+    k_adam<<<blocks_for(count), 256, 0, s>>>(count, w, m, v, g, wb, lr, b1, b2, eps, c1, c2);
+}
+
+void launch_to_bf16(long count, const float* a, __nv_bfloat16* b, cudaStream_t s) {
+    count_launch();
+    k_to_bf16<<<blocks_for(count), 256, 0, s>>>(count, a, b);
+}
+
+}  // namespace unet
+}  // namespace vb
