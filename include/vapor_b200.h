@@ -296,6 +296,28 @@ vapor_status vapor_stage_advect_scalar_device(vapor_stage *stage, float dt, floa
 vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 
+/* Advection of one staggered field that allocates no device memory. No
+ * counterpart in the reference: it is for callers that may not allocate at
+ * the call site (a frame loop that cannot absorb cudaFree's device-wide
+ * synchronization, a host that owns all device memory and hands plugins only
+ * their buffers, a stream that another component is recording into). Same
+ * arithmetic as vapor_stage_advect_face_device / _scalar_device (results are
+ * bit-identical), with the MacCormack forward pass kept in a fixed 4 MiB
+ * array inside this library's device image instead of an allocated buffer.
+ *   loc: 0 cell (smoke), 1/2/3 faces of x/y/z; every pointer is device memory
+ *   on the current device, of the reference's MAC sizes for n; output must not
+ *   alias source or the flow; stream may be NULL (the default stream).
+ * Limit: the field may have at most 1048576 values (faces: n <= 101); larger
+ * fields return VAPOR_LENGTH_ERROR. The first call on each device looks up the
+ * array's address; make that first call before any stream capture begins.
+ * All calls share the array, so calls that can overlap on the GPU (different
+ * streams, unordered threads) race and must be serialized by the caller.
+ * Nothing needs to start at zero. */
+vapor_status vapor_advect_noalloc(int32_t n, float box, int32_t loc, float dt, float cfl_limit,
+                                  int32_t method, const float *source, const float *flow_u,
+                                  const float *flow_v, const float *flow_w, float *output,
+                                  void *stream);
+
 /* ---- Learned warm start for the pressure solve ----
  * No counterpart in the reference, whose projection starts every solve from
  * zero pressure (CpuPressureSolver3D.cpp:46). The model is a fixed 3-level 3D
