@@ -31,12 +31,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from vapor_b200.plume import DT, omega_for, scene_params, swirl_fields  # noqa: E402
+
 METRIC = "256^3 steps/s: learned-warm-start vs plain GPU solve at rel div 1e-6; HBM %"
-DT = 0.01
-# SOR relaxation per grid size for the floor-6 red-black sweep (chosen by
-# measured sweep counts to rel 1e-6 on this plume; larger grids want omega
-# closer to 2).
-OMEGA = {32: 1.95, 64: 1.95, 96: 1.96, 128: 1.97, 192: 1.975, 256: 1.98}
 
 
 def parse():
@@ -49,68 +46,11 @@ def parse():
     ap.add_argument("--rel", type=float, default=1e-6)
     ap.add_argument("--max-iterations", type=int, default=20000)
     ap.add_argument("--omega", type=float, default=None)
+    ap.add_argument("--interval", type=int, default=8, help="residual check interval (sweeps)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
     return ap.parse_args()
-
-
-def omega_for(n, override=None):
-    if override:
-        return override
-    keys = sorted(OMEGA)
-    return OMEGA[min(keys, key=lambda k: abs(k - n))]
-
-
-def scene_params(vb_params, n, rel, max_iterations, omega):
-    from vapor_b200.abi import LinearSolveOptions, SOLVER_MIXED_REFINEMENT
-    p = vb_params
-    p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = 1, 1, 1
-    p.buoyancy, p.buoyancy_split, p.cfl_mc = 1.5, 0.5, 3.0
-    p.smoke_decay = 0.5  # factor clamp(1 - .5 * .01) = .995 per step
-    p.emitter_radius, p.source_strength = 0.08, 1.0
-    p.emitter_center_x, p.emitter_center_y, p.emitter_center_z = 0.3, 0.5, 0.15
-    p.emitter_count = 2
-    p.emitter2_center_x, p.emitter2_center_y, p.emitter2_center_z = 0.7, 0.5, 0.15
-    p.emitter_profile = 1
-    p.emitter_kick_multiplier, p.stir_strength = 0.0, 0.0
-    p.sor_omega = omega
-    p.use_solve_options = 1
-    p.solver_kind = SOLVER_MIXED_REFINEMENT
-    p.solve = LinearSolveOptions.defaults(max_iterations=max_iterations, residual_check_interval=8,
-                                          relative_tolerance=rel, absolute_tolerance=0.0, fixed_iterations=0)
-    return p
-
-
-def swirl_fields(n, seed, amplitude=0.5, vortices=8, sigma=0.08):
-    """Seeded swirl: sum of Gaussian vortices (random centre and axis) on the
-    MAC faces, normal velocity zero on the walls; density zero."""
-    rng = np.random.default_rng(seed)
-    centres = rng.uniform(0.2, 0.8, size=(vortices, 3))
-    axes = rng.normal(size=(vortices, 3))
-    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
-    h = 1.0 / n
-
-    def comp(c, shape):
-        zz, yy, xx = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
-        pos = [(xx + (0.0 if c == 0 else 0.5)) * h, (yy + (0.0 if c == 1 else 0.5)) * h,
-               (zz + (0.0 if c == 2 else 0.5)) * h]
-        out = np.zeros(shape)
-        for k in range(vortices):
-            r = [pos[d] - centres[k, d] for d in range(3)]
-            g = np.exp(-(r[0] ** 2 + r[1] ** 2 + r[2] ** 2) / (2 * sigma ** 2))
-            a = axes[k]
-            cross = [a[1] * r[2] - a[2] * r[1], a[2] * r[0] - a[0] * r[2], a[0] * r[1] - a[1] * r[0]]
-            out += amplitude * cross[c] / sigma * g
-        return out.astype(np.float32)
-
-    u = comp(0, (n, n, n + 1))
-    v = comp(1, (n, n + 1, n))
-    w = comp(2, (n + 1, n, n))
-    u[:, :, 0] = u[:, :, -1] = 0
-    v[:, 0, :] = v[:, -1, :] = 0
-    w[0] = w[-1] = 0
-    return [np.zeros((n, n, n), np.float32), u, v, w]
 
 
 class ClockSampler:
@@ -269,7 +209,7 @@ def main():
 
     n = args.n
     omega = omega_for(n, args.omega)
-    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega)
+    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega, interval=args.interval)
     fields = swirl_fields(n, args.seed + rank)
     sim = vb.MacSimulation3D(n, 1.0, params)
     sim.upload(*fields)

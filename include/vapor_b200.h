@@ -350,8 +350,12 @@ vapor_status vapor_unet_backward(vapor_unet *net, int32_t n, const float *grad_o
  * `sim`. The network must outlive the simulation or be detached first. */
 vapor_status vapor_mac3d_set_warm_start(vapor_mac3d *sim, vapor_unet *net);
 /* One Adam step on the simulation's last projection (its right-hand side and
- * converged pressure); *loss (may be NULL) receives the relative squared error
- * of the prediction before the step. */
+ * converged pressure); *loss (may be NULL) receives the loss before the step:
+ * the relative squared error of the mean-free prediction after its best
+ * scaling, 1 - cos^2 against the converged pressure. The warm start applies
+ * that scaling itself: x0 = alpha q with q the mean-free prediction and
+ * alpha = (q.b)/(q.Aq), the Galerkin condition on span{q}, so the guess is
+ * never worse than zero in the A-norm. */
 vapor_status vapor_mac3d_train_warm_start(vapor_mac3d *sim, vapor_unet *net, float learning_rate,
                                           double *loss);
 /* The same loss without an update. */

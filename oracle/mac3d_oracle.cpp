@@ -367,14 +367,24 @@ bool sorSolve(int n, T omega, T floorDiag, T* x, const T* b, const vapor_linear_
     return true;
 }
 
-// Mixed-precision refinement (extension). The pressure x64 is FP64. At every
-// residual check (every `residual_check_interval` sweeps, as in SOR.cpp:56-61)
-// the FP64 residual r = b - A x64 is formed; if it is not below the target,
-// `interval` FP32 red-black SOR sweeps run on A e = float(r) from e = 0 and
-// x64 += e. For a stationary iteration this equals continuing SOR on x in
-// exact arithmetic, but the iterate no longer stagnates at FP32 rounding
-// (plain FP32 SOR stops near 1e-5 relative residual on a 32^3 plume).
-// `iterations` counts FP32 sweeps.
+// Mixed-precision refinement (extension). The pressure x64 is FP64; FP32
+// red-black SOR sweeps run on the error equation A e = float(b - A x64) from
+// e = 0. Every `residual_check_interval` sweeps (SOR.cpp:56-61) the FP32
+// residual of the error equation is measured on the colour-1 cells (those
+// the sweep updates last; the GPU measures it inside that sweep); the solver
+// re-centres
+// (x64 += e, new FP64 residual, e = 0) when that residual reaches the target,
+// drops below kRecentreDrop times the FP64 residual of the last re-centring,
+// after kRecentreSweeps sweeps, or at the iteration budget, and stops when the
+// FP64 residual meets the target. For a stationary iteration this equals
+// continuing SOR on x in exact arithmetic, but the iterate no longer stagnates
+// at FP32 rounding (plain FP32 SOR stops near 1e-5 relative residual on a 32^3
+// plume). The FP32 measure loses accuracy once the residual is ~1e3 below the
+// last re-centring, which the 1e-2 threshold stays well clear of. `iterations`
+// counts FP32 sweeps.
+constexpr float kRecentreDrop = 1e-2f;
+constexpr int kRecentreSweeps = 1024;
+
 inline bool refinementSolve(int n, float omega, float floorDiag, std::vector<double>& x64,
                             const float* b, const vapor_linear_solve_options& o, vapor_linear_solve_result& r) {
     if (!validOptions(o)) return false;
@@ -404,20 +414,50 @@ inline bool refinementSolve(int n, float omega, float floorDiag, std::vector<dou
     const double target = std::max(o.absolute_tolerance, o.relative_tolerance * r.initial_residual);
     r.converged = r.final_residual <= target;
     if (r.converged && !o.fixed_iterations) return true;
-    std::vector<float> e(count), rf(count);
-    while (r.iterations < o.max_iterations) {
-        for (size_t i = 0; i < count; ++i) {
-            rf[i] = float(res[i]);
-            e[i] = 0.f;
-        }
+    // FP32 sweeps on the error equation A e = rf; every check interval the FP32
+    // residual max |rf - A e| (operation order: count * e, minus x-, x+, y-, y+,
+    // z-, z+) decides whether to re-centre in FP64 and test the FP64 residual.
+    std::vector<float> e(count, 0.f), rf(count);
+    for (size_t i = 0; i < count; ++i) rf[i] = float(res[i]);
+    double r0 = r.final_residual;
+    int since = 0;
+    const size_t nn = size_t(n) * n;
+    while (true) {
         const int sweeps = std::min(o.residual_check_interval - r.iterations % o.residual_check_interval,
                                     o.max_iterations - r.iterations);
         for (int k = 0; k < sweeps; ++k) sorIterationFast(n, omega, floorDiag, e.data(), rf.data());
         r.iterations += sweeps;
+        since += sweeps;
+        // FP32 residual over the colour-1 cells ((i + j + k) odd, the colour a
+        // sweep updates last), in the sweep's operation order.
+        float rho = 0.f;
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    if (((i + j + k) & 1) == 0) continue;
+                    const size_t id = size_t(i) + size_t(n) * (size_t(j) + size_t(n) * k);
+                    const float diag = float(neighbourCount(n, i, j, k));
+                    float off = 0.f;
+                    if (i > 0) off += -1.f * e[id - 1];
+                    if (i + 1 < n) off += -1.f * e[id + 1];
+                    if (j > 0) off += -1.f * e[id - n];
+                    if (j + 1 < n) off += -1.f * e[id + n];
+                    if (k > 0) off += -1.f * e[id - nn];
+                    if (k + 1 < n) off += -1.f * e[id + nn];
+                    rho = std::max(rho, std::abs(rf[id] - off - diag * e[id]));
+                }
+        const bool recentre = double(rho) <= target || double(rho) <= double(kRecentreDrop) * r0 ||
+                              since >= kRecentreSweeps || r.iterations >= o.max_iterations;
+        if (!recentre) continue;
         for (size_t i = 0; i < count; ++i) x64[i] += double(e[i]);
-        r.final_residual = residual();
+        r.final_residual = r0 = residual();
+        since = 0;
         r.converged = r.final_residual <= target;
-        if (r.converged && !o.fixed_iterations) break;
+        if ((r.converged && !o.fixed_iterations) || r.iterations >= o.max_iterations) break;
+        for (size_t i = 0; i < count; ++i) {
+            rf[i] = float(res[i]);
+            e[i] = 0.f;
+        }
     }
     return true;
 }

@@ -67,27 +67,31 @@ def split(params):
 
 
 def torch_reference(params, x16, requires_grad=False):
-    """Same U-Net in FP32 with BF16 rounding where the CUDA path stores BF16."""
+    """Same U-Net in FP32, rounding to BF16 where the CUDA path stores BF16:
+    weights, every stored activation and (with requires_grad) the gradient of
+    every stored activation, which the CUDA backward pass also keeps in BF16."""
     import torch
     import torch.nn.functional as F
     convs, hw, hb = split(params)
-    q = lambda t: t.to(torch.bfloat16).to(torch.float32)
     ws = [torch.tensor(w, requires_grad=requires_grad) for w, _ in convs]
     bs = [torch.tensor(b, requires_grad=requires_grad) for _, b in convs]
     hw_t = torch.tensor(hw, requires_grad=requires_grad)
     hb_t = torch.tensor(np.array([hb], np.float32), requires_grad=requires_grad)
 
+    def q(t):
+        t = t.to(torch.bfloat16).to(torch.float32)
+        if requires_grad:
+            t.register_hook(lambda g: g.to(torch.bfloat16).to(torch.float32))
+        return t
+
     def conv(i, x):
-        y = F.conv3d(x, ws[i].to(torch.bfloat16).to(torch.float32) if not requires_grad else ws[i], bs[i], padding=1)
-        return q(F.relu(y)) if not requires_grad else F.relu(y)
+        return q(F.relu(F.conv3d(x, ws[i].to(torch.bfloat16).to(torch.float32), bs[i], padding=1)))
     x = torch.tensor(x16).permute(3, 0, 1, 2).unsqueeze(0)
     e1a = conv(0, x)
     s1 = conv(1, e1a)
-    e2in = q(F.avg_pool3d(s1, 2)) if not requires_grad else F.avg_pool3d(s1, 2)
-    e2a = conv(2, e2in)
+    e2a = conv(2, q(F.avg_pool3d(s1, 2)))
     s2 = conv(3, e2a)
-    e3in = q(F.avg_pool3d(s2, 2)) if not requires_grad else F.avg_pool3d(s2, 2)
-    e3a = conv(4, e3in)
+    e3a = conv(4, q(F.avg_pool3d(s2, 2)))
     e3b = conv(5, e3a)
     dec2 = torch.cat([F.interpolate(e3b, scale_factor=2, mode="nearest"), s2], 1)
     d2a = conv(6, dec2)
@@ -146,8 +150,51 @@ def test_gradients_match_torch_autograd():
         rw = ws[i].grad.numpy()
         cos = float((w_g * rw).sum() / (np.linalg.norm(w_g) * np.linalg.norm(rw) + 1e-30))
         rel = float(np.linalg.norm(w_g - rw) / (np.linalg.norm(rw) + 1e-30))
-        assert cos > 0.99 and rel < 0.1, (i, cos, rel)
+        assert cos > 0.995 and rel < 0.1, (i, cos, rel)  # BF16 storage: ~1e-2 per layer
         rb = bs[i].grad.numpy()
         assert np.linalg.norm(b_g - rb) <= 0.1 * np.linalg.norm(rb) + 1e-7, i
     head = grads[-17:-1]
     assert np.linalg.norm(head - hw.grad.numpy()) <= 0.05 * np.linalg.norm(hw.grad.numpy())
+
+
+def _plume(n, rel=1e-6):
+    from vapor_b200.plume import scene_params, swirl_fields
+    p = scene_params(vb.default_params(), n, rel=rel, max_iterations=20000)
+    sim = vb.MacSimulation3D(n, 1.0, p)
+    sim.upload(*swirl_fields(n, 4))
+    return sim
+
+
+def test_warm_start_keeps_the_tolerance_and_the_solution():
+    """An untrained network only changes the initial guess: every projection
+    still reaches the FP64 relative residual, and the fields agree with the
+    plain solve to within what that tolerance allows."""
+    from vapor_b200.learned import WarmStartNet
+    n = 32
+    plain, warm = _plume(n), _plume(n)
+    net = WarmStartNet(seed=3)
+    warm.set_warm_start(net)
+    for _ in range(4):
+        plain.advance(0.01)
+        warm.advance(0.01)
+        r = warm.last_projection().linear_solve
+        assert r.converged and r.final_residual <= 1e-6 * r.initial_residual
+    for a, b in zip(warm.download(), plain.download()):
+        assert np.abs(a - b).max() <= 1e-3 * max(1.0, float(np.abs(b).max()))
+
+
+def test_training_reduces_the_loss_on_one_scene():
+    """A few Adam steps on the same projection lower the scale-invariant loss."""
+    from vapor_b200.learned import WarmStartNet
+    sim = _plume(32)
+    for _ in range(3):
+        sim.advance(0.01)
+    net = WarmStartNet(seed=1)
+    first = sim.evaluate_warm_start(net)
+    for _ in range(30):
+        sim.train_warm_start(net, 1e-3)
+    last = sim.evaluate_warm_start(net)
+    assert 0.0 <= last < 0.7 * first, (first, last)
+    # the network handle stays usable after its simulation is gone
+    sim.close()
+    assert np.isfinite(net.parameters()).all()

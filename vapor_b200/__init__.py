@@ -106,6 +106,19 @@ def _declare(lib):
     f("vapor_stage_advect_scalar_device", _vp, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp)
     f("vapor_stage_set_solver_kind", _vp, C.c_int32)
     f("vapor_stage_stream", _vp, C.POINTER(_vp))
+    f("vapor_advect_noalloc", C.c_int32, C.c_float, C.c_int32, C.c_float, C.c_float, C.c_int32,
+      _vp, _vp, _vp, _vp, _vp, _vp)
+    f("vapor_unet_parameter_count", res=C.c_int64)
+    f("vapor_unet_create", C.POINTER(_vp))
+    f("vapor_unet_destroy", _vp)
+    f("vapor_unet_init", _vp, C.c_uint32)
+    f("vapor_unet_set_parameters", _vp, _vp, C.c_int64)
+    f("vapor_unet_get_parameters", _vp, _vp, C.c_int64)
+    f("vapor_unet_forward_features", _vp, C.c_int32, _vp, _vp)
+    f("vapor_unet_backward", _vp, C.c_int32, _vp, _vp)
+    f("vapor_mac3d_set_warm_start", _vp, _vp)
+    f("vapor_mac3d_train_warm_start", _vp, _vp, C.c_float, C.POINTER(C.c_double))
+    f("vapor_mac3d_evaluate_warm_start", _vp, _vp, C.POINTER(C.c_double))
     return lib
 
 
@@ -283,6 +296,24 @@ class MacSimulation3D:
         t = abi.PhaseTimings()
         check(library().vapor_mac3d_timings(self._h, C.byref(t)))
         return t.as_dict()
+
+    # ---- learned warm start (vapor_b200.learned.WarmStartNet) ----
+    def set_warm_start(self, net):
+        """Initial guess of every later projection from `net` (None: zero)."""
+        check(library().vapor_mac3d_set_warm_start(self._h, net.handle if net is not None else None))
+        self._warm = net  # the network must outlive its use here
+
+    def train_warm_start(self, net, learning_rate):
+        """One Adam step of `net` on the last projection; returns the loss
+        (relative squared error of the mean-free prediction) before it."""
+        loss = C.c_double()
+        check(library().vapor_mac3d_train_warm_start(self._h, net.handle, float(learning_rate), C.byref(loss)))
+        return loss.value
+
+    def evaluate_warm_start(self, net):
+        loss = C.c_double()
+        check(library().vapor_mac3d_evaluate_warm_start(self._h, net.handle, C.byref(loss)))
+        return loss.value
 
 
 class StageBackend:

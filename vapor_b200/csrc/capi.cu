@@ -283,6 +283,21 @@ VB_API vapor_status vapor_stage_stream(vapor_stage* stage, void** stream) {
 }
 
 // ---- learned warm start ----
+namespace {
+// Orders the network's work on the simulation's stream for one call; after it
+// the network goes back to its own stream unless the simulation uses it as
+// its warm start.
+struct StreamBinding {
+    vb::Simulation& sim;
+    vb::unet::UNet& net;
+    StreamBinding(vb::Simulation& s, vb::unet::UNet& n, cudaStream_t stream) : sim(s), net(n) {
+        net.set_stream(stream);
+    }
+    ~StreamBinding() {
+        if (sim.warm_start() != &net) net.use_own_stream();
+    }
+};
+}  // namespace
 VB_API int64_t vapor_unet_parameter_count(void) { return vb::unet::parameter_count(); }
 
 VB_API vapor_status vapor_unet_create(vapor_unet** out) {
@@ -300,28 +315,29 @@ VB_API vapor_status vapor_unet_destroy(vapor_unet* net) {
 #define NET_GUARD(body)                                      \
     return guarded([&] {                                     \
         require(net != nullptr, "null network handle");     \
+        net->net.use_own_stream();                           \
         body;                                                \
     })
 
 VB_API vapor_status vapor_unet_init(vapor_unet* net, uint32_t seed) {
-    NET_GUARD(net->net.set_stream(net->stream.s); net->net.init_parameters(seed));
+    NET_GUARD(net->net.init_parameters(seed));
 }
 VB_API vapor_status vapor_unet_set_parameters(vapor_unet* net, const float* host, int64_t count) {
     NET_GUARD(require(host && count == vb::unet::parameter_count(), "parameter count mismatch");
-              net->net.set_stream(net->stream.s); net->net.set_parameters(host));
+              net->net.set_parameters(host));
 }
 VB_API vapor_status vapor_unet_get_parameters(vapor_unet* net, float* host, int64_t count) {
     NET_GUARD(require(host && count == vb::unet::parameter_count(), "parameter count mismatch");
               net->net.get_parameters(host));
 }
 VB_API vapor_status vapor_unet_forward_features(vapor_unet* net, int32_t n, const void* input_bf16, float* output) {
-    NET_GUARD(require(input_bf16 && output, "null buffer"); net->net.set_stream(net->stream.s);
+    NET_GUARD(require(input_bf16 && output, "null buffer");
               net->net.forward_features(n, static_cast<const __nv_bfloat16*>(input_bf16), output);
               VB_CUDA(cudaStreamSynchronize(net->stream.s));
               if (net->net.error_flag()) vb::fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out"));
 }
 VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float* grad_output, float* grad_params) {
-    NET_GUARD(require(grad_output && grad_params, "null buffer"); net->net.set_stream(net->stream.s);
+    NET_GUARD(require(grad_output && grad_params, "null buffer");
               net->net.backward_from_output(n, grad_output);
               VB_CUDA(cudaMemcpyAsync(grad_params, net->net.gradient(),
                                       vb::unet::parameter_count() * sizeof(float), cudaMemcpyDeviceToHost,
@@ -336,13 +352,13 @@ VB_API vapor_status vapor_mac3d_train_warm_start(vapor_mac3d* sim, vapor_unet* n
                                                  double* loss) {
     SIM_GUARD(require(net != nullptr, "null network handle");
               require(std::isfinite(learning_rate) && learning_rate > 0.f, "invalid learning rate");
-              vb::Workspace& ws = sim->sim.workspace(); net->net.set_stream(ws.stream());
+              vb::Workspace& ws = sim->sim.workspace(); StreamBinding bind(sim->sim, net->net, ws.stream());
               const double l = net->net.train_step(ws.n(), ws.rhs(), ws.pressure(), ws.control(), learning_rate);
               if (loss) *loss = l);
 }
 VB_API vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d* sim, vapor_unet* net, double* loss) {
     SIM_GUARD(require(net != nullptr, "null network handle"); vb::Workspace& ws = sim->sim.workspace();
-              net->net.set_stream(ws.stream());
+              StreamBinding bind(sim->sim, net->net, ws.stream());
               const double l = net->net.evaluate(ws.n(), ws.rhs(), ws.pressure(), ws.control());
               if (loss) *loss = l);
 }

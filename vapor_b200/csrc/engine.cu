@@ -202,8 +202,8 @@ void Workspace::ensure_mixed() {
 // while the handle's value (set by a kernel before the node and by the body's
 // last kernel) is nonzero.
 template <class Body>
-static void add_while_loop(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditionalHandle handle,
-                           Body&& body) {
+static void add_conditional(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditionalHandle handle,
+                            cudaGraphConditionalNodeType type, Body&& body) {
     cudaStreamCaptureStatus status;
     cudaGraph_t graph;
     const cudaGraphNode_t* deps = nullptr;
@@ -213,7 +213,7 @@ static void add_while_loop(cudaStream_t s, cudaStream_t body_stream, cudaGraphCo
     cudaGraphNodeParams params = {};
     params.type = cudaGraphNodeTypeConditional;
     params.conditional.handle = handle;
-    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.type = type;
     params.conditional.size = 1;
     cudaGraphNode_t node;
     VB_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
@@ -224,6 +224,12 @@ static void add_while_loop(cudaStream_t s, cudaStream_t body_stream, cudaGraphCo
     body(body_stream);
     cudaGraph_t captured = nullptr;
     VB_CUDA(cudaStreamEndCapture(body_stream, &captured));
+}
+
+template <class Body>
+static void add_while_loop(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditionalHandle handle,
+                           Body&& body) {
+    add_conditional(s, body_stream, handle, cudaGraphCondTypeWhile, body);
 }
 
 static cudaGraphConditionalHandle new_condition(cudaStream_t s) {
@@ -264,11 +270,14 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     };
     // k guarded colour-pair sweeps on x (right-hand side rhs) on stream st.
     // Inner sweeps of the mixed solver use the divide-free relaxation.
-    auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean) {
+    // With `measure`, the last colour-1 launch also records the FP32 residual.
+    auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean,
+                      bool measure = false) {
         t.begin(VAPOR_PHASE_SOR);
         for (int j = 0; j < k; ++j) {
             launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
-            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
+            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
+                             measure && j + 1 == k);
         }
         t.end(VAPOR_PHASE_SOR, 2LL * k);
     };
@@ -282,33 +291,51 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     t.end(VAPOR_PHASE_RHS, 3);
 
     if (mixed) {
-        // FP32 red-black sweeps on the error equation, re-centred in FP64 at
-        // every residual check (the oracle's refinementSolve).
+        // FP32 red-black sweeps on the error equation A e = r32. Every check
+        // interval the FP32 residual of that equation decides whether to
+        // re-centre in FP64 (x64 += e, r32 = b - A x64, e = 0) and test the FP64
+        // residual against the target (the oracle's refinementSolve).
         if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);  // x0 = network prediction
         else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
-        auto recentre = [&](cudaStream_t st, int done_sweeps, bool accumulate) {
-            t.begin(VAPOR_PHASE_RESIDUAL);
-            launch_refine_residual(a, b_.p, p_.p, r32_.p, ctrl_, st);
-            launch_check(ctrl_, done_sweeps, accumulate, true, cond, st);
-            t.end(VAPOR_PHASE_RESIDUAL, 2);
+        t.begin(VAPOR_PHASE_RESIDUAL);
+        launch_refine_residual(a, b_.p, p_.p, r32_.p, ctrl_, s);
+        launch_check(ctrl_, 0, false, true, cond, s);
+        t.end(VAPOR_PHASE_RESIDUAL, 2);
+        const bool fused = sor_fuses_measure(n_);
+        auto recentre_group = [&](cudaStream_t st, LoopCond loop_cond) {
+            launch_refine_residual_gated(a, b_.p, p_.p, r32_.p, ctrl_, st);
+            launch_check_gated(ctrl_, loop_cond, st);
+            launch_zero_error_gated(a, p_.p, ctrl_, st);
         };
-        const int chunk = std::max(1, std::min(interval, o.max_iterations));
+        auto chunk_then_check = [&](cudaStream_t st, int k) {
+            sweeps(st, k, 0, p_.p, r32_.p, false, true);
+            t.begin(VAPOR_PHASE_RESIDUAL);
+            if (graph) {
+                // the re-centring runs under a conditional if-node that the
+                // decision kernel sets, so skipped re-centrings cost nothing
+                const cudaGraphConditionalHandle ifh = new_condition(st);
+                LoopCond if_cond;
+                if_cond.active = 1;
+                if_cond.handle = (unsigned long long)ifh;
+                launch_error_check(a, p_.p, r32_.p, ctrl_, k, fused, LoopCond{}, if_cond, st);
+                add_conditional(st, body_stream2_.s, ifh, cudaGraphCondTypeIf,
+                                [&](cudaStream_t is) { recentre_group(is, LoopCond{}); });
+                launch_loop_condition(ctrl_, cond, st);  // continue while !ctrl->done
+            } else {
+                launch_error_check(a, p_.p, r32_.p, ctrl_, k, fused, cond, LoopCond{}, st);
+                recentre_group(st, cond);
+            }
+            t.end(VAPOR_PHASE_RESIDUAL, 6);
+        };
         if (graph) {
-            recentre(s, 0, false);
-            add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) {
-                VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), bs));
-                sweeps(bs, chunk, 0, p_.p, r32_.p, false);
-                recentre(bs, chunk, true);
-            });
+            const int chunk = std::max(1, std::min(interval, o.max_iterations));
+            add_while_loop(s, body_stream_.s, handle, [&](cudaStream_t bs) { chunk_then_check(bs, chunk); });
         } else {
             int it = 0;
-            recentre(s, 0, false);
             while (!wait_done()) {
-                VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), s));
                 const int k = std::min(interval - it % interval, o.max_iterations - it);
-                sweeps(s, k, 0, p_.p, r32_.p, false);
+                chunk_then_check(s, k);
                 it += k;
-                recentre(s, k, true);
             }
         }
         t.begin(VAPOR_PHASE_GRADIENT);
@@ -405,6 +432,7 @@ Simulation::Simulation(int n, float box, const vapor_mac3d_params& p) : params(p
 Simulation::~Simulation() {
     cudaStreamSynchronize(ws_.stream());
     release_graphs();
+    if (warm_) warm_->use_own_stream();  // the network outlives this simulation's stream
 }
 
 void Simulation::reset() {
@@ -553,6 +581,7 @@ void Simulation::set_warm_start(unet::UNet* net) {
         fail(VAPOR_INVALID_ARGUMENT, "the warm-start network needs n divisible by 4 (n >= 8)");
     VB_CUDA(cudaStreamSynchronize(ws_.stream()));
     release_graphs();
+    if (warm_ && warm_ != net) warm_->use_own_stream();
     warm_ = net;
     if (warm_) {
         warm_->set_stream(ws_.stream());
@@ -602,6 +631,8 @@ void Simulation::advance(float dt) {
     key.dt = dt;
     key.box = ws_.box();
     key.params = params;
+    key.warm = warm_;
+    key.warm_buffers = warm_ ? warm_->generation() : 0ull;
     if (!slot.exec || std::memcmp(&slot.key, &key, sizeof(GraphKey)) != 0) {
         if (slot.exec) {
             cudaGraphExecDestroy(slot.exec);

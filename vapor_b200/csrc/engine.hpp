@@ -142,6 +142,7 @@ private:
     int* done_host_ = nullptr;          // pinned
     PhaseTimer timer_;
     Stream body_stream_;                // records conditional-loop bodies
+    Stream body_stream2_;               // records conditional bodies nested in a loop
     bool capturing_ = false;
     long long total_iterations_ = 0;
     unsigned int sticky_errors_ = 0u;
@@ -197,6 +198,8 @@ private:
         float dt;
         float box;
         vapor_mac3d_params params;
+        const void* warm;                 // warm-start network, if any
+        unsigned long long warm_buffers;  // its buffer generation (reallocation re-records)
     };
     struct CachedGraph {
         GraphKey key{};

@@ -34,8 +34,11 @@ struct ProjControl {
     int fixed;
     int continue_flag;              // mirror of the graph while-condition
     int x64_cur;                    // mixed precision: index of the current FP64 pressure
-    int reserved2;
+    int recentre;                   // mixed precision: 1 when this check re-centres in FP64
     double* x64[2];                 // mixed precision: FP64 pressure ping-pong buffers
+    double r0;                      // mixed precision: FP64 residual at the last re-centring
+    unsigned int res32_bits;        // mixed precision: FP32 error-equation residual, float bits
+    int since;                      // mixed precision: sweeps since the last re-centring
     vapor_projection_result result;
     // persistent across projections (cleared only by a workspace reset)
     unsigned int sticky_nonfinite;  // OR of `nonfinite` over finished projections
@@ -109,12 +112,37 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
 // ctrl->iterations + sweep_index reaches the iteration budget.
 // `exact` = false selects the mixed solver's divide-free relaxation
 // x += (b - off - diag x) * (omega / max(diag, floor)).
-void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true);
+// `measure` (colour 1 only) also records max |b' - off - diag x| of the updated
+// cells into ctrl->res32_bits when sor_fuses_measure(n); otherwise
+// launch_error_check measures the same value in a separate pass.
+void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, ProjControl* ctrl,
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true,
+                      bool measure = false);
+bool sor_fuses_measure(int n);
 // Mixed precision: x64[1-cur] = x64[cur] + e (FP64), r32 = float(b' - A x)
 // with the FP64 residual norm into ctrl->res_bits.
 void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
                             ProjControl* ctrl, cudaStream_t s);
+// Mixed precision check between re-centrings: the FP32 residual of the error
+// equation over the colour-1 cells, max |r32 - A e| (measured here unless the
+// last sweep already did, `measured`), then the decision (ctrl->recentre) to
+// re-centre in FP64: when that residual reaches the target, drops below
+// kRecentreDrop * r0, after kRecentreSweeps sweeps, or at the iteration budget.
+// Adds `sweeps` to the iteration count. Without a re-centring it sets the
+// loop condition to continue; `recentre_cond` (a graph if-condition) receives
+// the decision.
+constexpr float kRecentreDrop = 1e-2f;
+constexpr int kRecentreSweeps = 1024;
+void launch_error_check(const ProjectionArgs& a, const float* e, const float* r32, ProjControl* ctrl, int sweeps,
+                        bool measured, LoopCond cond, LoopCond recentre_cond, cudaStream_t s);
+// Gated forms (they do nothing unless ctrl->recentre): the re-centring pass,
+// its check, and e = 0 afterwards.
+void launch_refine_residual_gated(const ProjectionArgs& a, const float* b, const float* e, float* r32,
+                                  ProjControl* ctrl, cudaStream_t s);
+void launch_check_gated(ProjControl* ctrl, LoopCond cond, cudaStream_t s);
+// Sets the graph loop condition to !ctrl->done.
+void launch_loop_condition(const ProjControl* ctrl, LoopCond cond, cudaStream_t s);
+void launch_zero_error_gated(const ProjectionArgs& a, float* e, const ProjControl* ctrl, cudaStream_t s);
 // Mixed precision epilogue: FP64 pressure mean, final FP64 residual, float
 // pressure copy (x64 - mean) into p32 with ctrl->p_mean_f = 0.
 void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,

@@ -57,6 +57,10 @@ __global__ void k_begin_projection(ProjControl* ctrl, vapor_linear_solve_options
     ctrl->check_interval = o.residual_check_interval;
     ctrl->fixed = o.fixed_iterations;
     ctrl->continue_flag = 0;
+    ctrl->recentre = 1;
+    ctrl->r0 = 0.0;
+    ctrl->res32_bits = 0u;
+    ctrl->since = 0;
     vapor_projection_result r = {};
     ctrl->result = r;
 }
@@ -245,6 +249,110 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
     }
 }
 
+// The same colour sweep marching in z: each thread owns 4 consecutive slots
+// of one row (y) for zb consecutive planes and keeps the other colour's rows
+// of planes z-1, z, z+1 in registers, so a plane costs 5 vector loads (own,
+// rhs, other colour at z+1, y-1, y+1) instead of 7, and the index arithmetic
+// is 32-bit and amortised over the column. Missing neighbours read as zero,
+// which leaves the reference's sum unchanged (x + (-1 * 0) == x bitwise for
+// every x, including signed zeros), so results equal k_sor_rb's bit for bit.
+// Needs hw % 4 == 0 and 2 * n^2 * hw < 2^31.
+template <bool EXACT, bool RESID>
+__global__ void __launch_bounds__(kThreads) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
+                                                      RelaxTable wr, float* __restrict__ xs,
+                                                      const float* __restrict__ bs, ProjControl* ctrl,
+                                                      int guarded, int sweep_index, int subtract_mean, int zb) {
+    if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
+    const int n = g.n;
+    const int hw = (n + 1) >> 1;
+    const int groups = hw >> 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = t / groups;
+    float rmax = 0.f;
+    if (y < n) {
+        const int i0 = (t - y * groups) << 2;
+        const int plane = n * hw;
+        const int stride = n * plane;
+        float* __restrict__ own = xs + colour * stride + y * hw + i0;
+        const float* __restrict__ oth = xs + (1 - colour) * stride + y * hw + i0;
+        const float* __restrict__ rhs = bs + colour * stride + y * hw + i0;
+        const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
+        const int z0 = blockIdx.y * zb;
+        const int z1 = min(n, z0 + zb);
+        const bool has_ym = y > 0, has_yp = y + 1 < n;
+        const int nyz = int(has_ym) + int(has_yp);
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
+        float4 cm = z0 > 0 ? ld4(oth + (z0 - 1) * plane) : zero4;
+        float4 cc = ld4(oth + z0 * plane);
+        const float w3 = wr.w[3], w4 = wr.w[4], w5 = wr.w[5], w6 = wr.w[6];
+        for (int z = z0; z < z1; ++z) {
+            const int zoff = z * plane;
+            const float4 cp = z + 1 < n ? ld4(oth + zoff + plane) : zero4;
+            const float4 m4 = has_ym ? ld4(oth + zoff - hw) : zero4;
+            const float4 p4 = has_yp ? ld4(oth + zoff + hw) : zero4;
+            const float4 a4 = ld4(own + zoff);
+            const float4 b4 = __ldg(reinterpret_cast<const float4*>(rhs + zoff));
+            const int sh = (y + z + colour) & 1;
+            float xl[5];
+            if (sh == 0) {
+                xl[0] = i0 > 0 ? oth[zoff - 1] : 0.f;
+                xl[1] = cc.x; xl[2] = cc.y; xl[3] = cc.z; xl[4] = cc.w;
+            } else {
+                xl[0] = cc.x; xl[1] = cc.y; xl[2] = cc.z; xl[3] = cc.w;
+                xl[4] = i0 + 4 < hw ? oth[zoff + 4] : 0.f;
+            }
+            const float xo[4] = {a4.x, a4.y, a4.z, a4.w};
+            const float bv[4] = {b4.x, b4.y, b4.z, b4.w};
+            const float ym[4] = {m4.x, m4.y, m4.z, m4.w};
+            const float yp[4] = {p4.x, p4.y, p4.z, p4.w};
+            const float zm[4] = {cm.x, cm.y, cm.z, cm.w};
+            const float zp[4] = {cp.x, cp.y, cp.z, cp.w};
+            const int ny = nyz + int(z > 0) + int(z + 1 < n);
+            float res[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int xc = 2 * (i0 + k) + sh;
+                const bool left = xc > 0, right = xc + 1 < n;
+                const int d = int(left) + int(right) + ny;
+                const float diag = float(d);
+                float off = 0.f;
+                off += -1.f * (left ? xl[k] : 0.f);
+                off += -1.f * (right ? xl[k + 1] : 0.f);
+                off += -1.f * ym[k];
+                off += -1.f * yp[k];
+                off += -1.f * zm[k];
+                off += -1.f * zp[k];
+                const float bi = subtract_mean ? bv[k] - bm : bv[k];
+                float r;
+                if (EXACT) {
+                    const float relax = maxf_ref(diag, floor_diag);
+                    r = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
+                } else {
+                    const float w = d == 6 ? w6 : (d == 5 ? w5 : (d == 4 ? w4 : w3));
+                    r = xo[k] + (bi - off - diag * xo[k]) * w;
+                }
+                const bool valid = xc < n && d > 0;
+                res[k] = valid ? r : xo[k];
+                if (RESID && valid) {
+                    // residual of this cell after its update: the other
+                    // colour (all its neighbours) does not change in this sweep
+                    const float rr = bi - off - diag * r;
+                    rmax = fmaxf(rmax, fabsf(rr));
+                }
+            }
+            *reinterpret_cast<float4*>(own + zoff) = make_float4(res[0], res[1], res[2], res[3]);
+            cm = cc;
+            cc = cp;
+        }
+    }
+    if (RESID) {
+        __shared__ float s_max[32];
+        const float br = block_max(rmax, s_max);
+        if (threadIdx.x == 0 && br > 0.f) atomicMax(&ctrl->res32_bits, __float_as_uint(br));
+    }
+}
+
 // Mixed precision re-centring on the split layout: x_out = x_in + e and
 // r32 = float(b' - A x_out), both in FP64 with the neighbour order of the
 // reference residual. One thread per VEC consecutive slots of one row of one
@@ -252,8 +360,9 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
 template <int VEC>
 __global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __restrict__ bs,
                                                         const float* __restrict__ es, float* __restrict__ r32,
-                                                        ProjControl* ctrl) {
+                                                        ProjControl* ctrl, int gated) {
     __shared__ double s_max[32];
+    if (gated && !ctrl->recentre) return;
     const double* __restrict__ xin = ctrl->x64[ctrl->x64_cur];
     double* __restrict__ xout = ctrl->x64[1 - ctrl->x64_cur];
     const int n = g.n;
@@ -315,6 +424,99 @@ __global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __r
         atomic_max_nonneg(&ctrl->res_bits, br);
         if (any_bad) atomicOr(&ctrl->nonfinite, 4u);
     }
+}
+
+// FP32 residual of the mixed solver's error equation, max |r32 - A e| over
+// the colour-1 cells (the colour a sweep updates last), with A the Neumann
+// operator (neighbour-count diagonal) and the operations in the sweep's order:
+// (r32 - off) - count * e with off = sum of -1 * e_nb in x-, x+, y-, y+, z-,
+// z+ order. Same value as the fused measurement of k_sor_rbz<*, true>; used
+// when that kernel does not apply (hw % 4 != 0).
+template <int VEC>
+__global__ void __launch_bounds__(kThreads) k_error_residual(Grid g, const float* __restrict__ es,
+                                                             const float* __restrict__ r32, ProjControl* ctrl,
+                                                             int first_colour) {
+    __shared__ float s_max[32];
+    const int n = g.n;
+    const RBLayout L = rb_layout(n);
+    const int hw = L.hw, groups = hw / VEC;
+    const int colour = first_colour + blockIdx.z;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y;
+    const int y = t / groups;
+    float rmax = 0.f;
+    unsigned int bad = 0u;
+    if (y < n) {
+        const int i0 = (t - y * groups) * VEC;
+        const int s = (y + z + colour) & 1;
+        const size_t row = (size_t(z) * n + y) * hw;
+        const size_t own = size_t(colour) * L.stride + row, oth = size_t(1 - colour) * L.stride + row;
+        const size_t yo = size_t(hw), zo = size_t(n) * hw;
+        float xo[VEC], xl[VEC + 1], ym[VEC], yp[VEC], zm[VEC], zp[VEC];
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            xo[k] = es[own + i0 + k];
+            ym[k] = y > 0 ? es[oth + i0 + k - yo] : 0.f;
+            yp[k] = y + 1 < n ? es[oth + i0 + k + yo] : 0.f;
+            zm[k] = z > 0 ? es[oth + i0 + k - zo] : 0.f;
+            zp[k] = z + 1 < n ? es[oth + i0 + k + zo] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k <= VEC; ++k) {
+            const int slot = i0 - 1 + s + k;
+            xl[k] = (slot >= 0 && slot < hw) ? es[oth + slot] : 0.f;
+        }
+        const int ny = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            const int xc = 2 * (i0 + k) + s;
+            if (xc >= n) continue;
+            const float diag = float((xc > 0) + (xc + 1 < n) + ny);
+            float off = 0.f;
+            if (xc > 0) off += -1.f * xl[k];
+            if (xc + 1 < n) off += -1.f * xl[k + 1];
+            if (y > 0) off += -1.f * ym[k];
+            if (y + 1 < n) off += -1.f * yp[k];
+            if (z > 0) off += -1.f * zm[k];
+            if (z + 1 < n) off += -1.f * zp[k];
+            const float res = r32[own + i0 + k] - off - diag * xo[k];
+            if (!isfinite(res)) bad = 1u;
+            const float aa = fabsf(res);
+            rmax = rmax < aa ? aa : rmax;
+        }
+    }
+    const float br = block_max(rmax, s_max);
+    const int any_bad = __syncthreads_or(int(bad));
+    if (threadIdx.x == 0) {
+        atomicMax(&ctrl->res32_bits, __float_as_uint(br));
+        if (any_bad) atomicOr(&ctrl->nonfinite, 4u);
+    }
+}
+
+__global__ void k_error_decide(ProjControl* ctrl, int sweeps, int use_conditional,
+                               cudaGraphConditionalHandle handle, int use_if, cudaGraphConditionalHandle if_handle) {
+    ctrl->iterations = min(ctrl->iterations + sweeps, ctrl->max_iterations);
+    ctrl->since += sweeps;
+    const float rho = __uint_as_float(ctrl->res32_bits);
+    ctrl->res32_bits = 0u;
+    const int recentre = double(rho) <= ctrl->target || double(rho) <= double(kRecentreDrop) * ctrl->r0 ||
+                         ctrl->since >= kRecentreSweeps || ctrl->iterations >= ctrl->max_iterations ||
+                         (ctrl->nonfinite & 4u) != 0u;
+    ctrl->recentre = recentre;
+    if (use_if) cudaGraphSetConditional(if_handle, recentre ? 1u : 0u);
+    ctrl->result.linear_solve.iterations = ctrl->iterations;
+    if (!recentre) {
+        ctrl->done = 0;
+        ctrl->continue_flag = 1;
+        if (use_conditional) cudaGraphSetConditional(handle, 1u);
+    }
+}
+
+// e = 0 over both colours after a re-centring (e is the next correction).
+__global__ void k_zero_error_gated(float* __restrict__ e, size_t count, const ProjControl* __restrict__ ctrl) {
+    if (!ctrl->recentre) return;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x)
+        e[i] = 0.f;
 }
 
 __global__ void __launch_bounds__(kThreads) k_psum64(Grid g, const ProjControl* __restrict__ ctrl,
@@ -487,12 +689,15 @@ __global__ void __launch_bounds__(kThreads) k_residual(Grid g, const float* __re
 // converged, and whether the loop stops. Optionally sets the CUDA graph
 // while-condition so the loop can run on the device without the host.
 __global__ void k_check(ProjControl* ctrl, int iterations, int accumulate, int flip_x64, int use_conditional,
-                        cudaGraphConditionalHandle handle) {
+                        cudaGraphConditionalHandle handle, int gated) {
+    if (gated && !ctrl->recentre) return;
     if (accumulate) ctrl->iterations = min(ctrl->iterations + iterations, ctrl->max_iterations);
     else ctrl->iterations = iterations;
     if (flip_x64) ctrl->x64_cur = 1 - ctrl->x64_cur;
     const double res = __longlong_as_double((long long)ctrl->res_bits);
     ctrl->res_bits = 0ull;
+    ctrl->r0 = res;
+    ctrl->since = 0;
     const int converged = res <= ctrl->target;
     ctrl->result.linear_solve.iterations = ctrl->iterations;
     ctrl->result.linear_solve.final_residual = res;
@@ -707,15 +912,36 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
                                     (cudaGraphConditionalHandle)cond.handle);
 }
 
-void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, const ProjControl* ctrl,
-                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact) {
+bool sor_fuses_measure(int n) {
+    const RBLayout L = rb_layout(n);
+    return L.hw % 4 == 0 && 2 * L.stride < (size_t(1) << 31);
+}
+
+// Planes per thread of the z-marching sweep: at least 4 waves of blocks.
+static int sor_planes(int n, int blocks_x) {
+    const long target_blocks = 148L * 5 * 4;
+    const long per_plane = long(blocks_x);
+    int zb = int(std::max(1L, (per_plane * n) / target_blocks));
+    return std::min(zb, 8);
+}
+
+void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, ProjControl* ctrl,
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact, bool measure) {
     const int n = a.g.n;
     const RBLayout L = rb_layout(n);
     RelaxTable wr;
     for (int d = 0; d < 7; ++d) wr.w[d] = a.omega / std::max(float(d), a.diagonal_floor);
     const int g = guarded ? 1 : 0, m = subtract_mean ? 1 : 0;
     count_launch();
-    if (L.hw % 4 == 0) {
+    if (sor_fuses_measure(n)) {
+        const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
+        const int zb = sor_planes(n, bx);
+        const dim3 grid(bx, (n + zb - 1) / zb);
+        if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
+        else if (exact) k_sor_rbz<true, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
+        else if (measure) k_sor_rbz<false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
+        else k_sor_rbz<false, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
+    } else if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n);
         if (exact) k_sor_rb<4, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
         else k_sor_rb<4, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
@@ -732,18 +958,69 @@ void launch_unsplit_pressure(const Grid& g, const float* p, const ProjControl* c
     k_unsplit_pressure<<<reduction_blocks(cells), kThreads, 0, s>>>(g, p, ctrl, out);
 }
 
-void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
-                            ProjControl* ctrl, cudaStream_t s) {
+static void refine_launch(const ProjectionArgs& a, const float* b, const float* e, float* r32, ProjControl* ctrl,
+                          int gated, cudaStream_t s) {
     const int n = a.g.n;
     const RBLayout L = rb_layout(n);
     count_launch();
     if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n, 2);
-        k_refine_rb<4><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
+        k_refine_rb<4><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated);
     } else {
         const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n, 2);
-        k_refine_rb<1><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl);
+        k_refine_rb<1><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated);
     }
+}
+
+void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,
+                            ProjControl* ctrl, cudaStream_t s) {
+    refine_launch(a, b, e, r32, ctrl, 0, s);
+}
+
+void launch_refine_residual_gated(const ProjectionArgs& a, const float* b, const float* e, float* r32,
+                                  ProjControl* ctrl, cudaStream_t s) {
+    refine_launch(a, b, e, r32, ctrl, 1, s);
+}
+
+void launch_error_check(const ProjectionArgs& a, const float* e, const float* r32, ProjControl* ctrl, int sweeps,
+                        bool measured, LoopCond cond, LoopCond recentre_cond, cudaStream_t s) {
+    const int n = a.g.n;
+    const RBLayout L = rb_layout(n);
+    if (!measured) {
+        count_launch();
+        if (L.hw % 4 == 0) {
+            const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n, 1);
+            k_error_residual<4><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1);
+        } else {
+            const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n, 1);
+            k_error_residual<1><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1);
+        }
+    }
+    count_launch();
+    k_error_decide<<<1, 1, 0, s>>>(ctrl, sweeps, cond.active, (cudaGraphConditionalHandle)cond.handle,
+                                   recentre_cond.active, (cudaGraphConditionalHandle)recentre_cond.handle);
+}
+
+__global__ void k_loop_condition(const ProjControl* ctrl, cudaGraphConditionalHandle handle) {
+    cudaGraphSetConditional(handle, ctrl->done ? 0u : 1u);
+}
+
+void launch_loop_condition(const ProjControl* ctrl, LoopCond cond, cudaStream_t s) {
+    if (!cond.active) return;
+    count_launch();
+    k_loop_condition<<<1, 1, 0, s>>>(ctrl, (cudaGraphConditionalHandle)cond.handle);
+}
+
+void launch_check_gated(ProjControl* ctrl, LoopCond cond, cudaStream_t s) {
+    count_launch();
+    k_check<<<1, 1, 0, s>>>(ctrl, 0, 1, 1, cond.active, (cudaGraphConditionalHandle)cond.handle, 1);
+}
+
+void launch_zero_error_gated(const ProjectionArgs& a, float* e, const ProjControl* ctrl, cudaStream_t s) {
+    const RBLayout L = rb_layout(a.g.n);
+    const size_t count = 2 * L.stride;
+    count_launch();
+    k_zero_error_gated<<<kMaxReductionBlocks, kThreads, 0, s>>>(e, count, ctrl);
 }
 
 void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
@@ -784,7 +1061,7 @@ void launch_check(ProjControl* ctrl, int iterations, bool accumulate, bool flip_
                   cudaStream_t s) {
     count_launch();
     k_check<<<1, 1, 0, s>>>(ctrl, iterations, accumulate ? 1 : 0, flip_x64 ? 1 : 0, cond.active,
-                            (cudaGraphConditionalHandle)cond.handle);
+                            (cudaGraphConditionalHandle)cond.handle, 0);
 }
 
 void launch_pressure_mean(const ProjectionArgs& a, const float* x, double* partials, int partial_capacity,

@@ -22,7 +22,7 @@ namespace {
 __nv_bfloat16* bf(DevArray<uint16_t>& a) { return reinterpret_cast<__nv_bfloat16*>(a.p); }
 }  // namespace
 
-UNet::UNet(cudaStream_t stream) : s_(stream) {
+UNet::UNet(cudaStream_t stream) : s_(stream), own_(stream) {
     configure_conv_kernels();
     const long P = parameter_count();
     params_.allocate(P);
@@ -34,7 +34,7 @@ UNet::UNet(cudaStream_t stream) : s_(stream) {
     for (const auto& l : kLayers) maxw = std::max(maxw, 27L * l.cout * l.cin);
     wflip_.allocate(maxw);
     partial_.allocate(1184);
-    scalars_.allocate(4);
+    scalars_.allocate(8);
     scale_.allocate(1);
     error_.allocate(1);
     VB_CUDA(cudaMemsetAsync(error_.p, 0, sizeof(uint32_t), s_));
@@ -106,13 +106,13 @@ void UNet::ensure(int n) {
     d1b_.allocate(V1 * 16);
     out_.allocate(V1);
     n_ = n;
+    ++generation_;
     // training buffers are allocated on first use (train_step)
     g1_.release();
     g2_.release();
     g3_.release();
     g4_.release();
     target_.release();
-    diff_.release();
     gout_.release();
 }
 
@@ -161,8 +161,7 @@ void UNet::infer_into(int n, const float* b_split, const ProjControl* ctrl, floa
     ensure(n);
     launch_prep_input(n, b_split, ctrl, partial_.p, scale_.p, bf(in0_), s_);
     forward(n);
-    launch_mean(long(n) * n * n, out_.p, partial_.p, scalars_.p, s_);
-    launch_store_warm_start(n, out_.p, scale_.p, scalars_.p, x_split, x64_split, s_);
+    launch_store_warm_start(n, out_.p, b_split, ctrl, partial_.p, scalars_.p, x_split, x64_split, s_);
     VB_CUDA(cudaGetLastError());
 }
 
@@ -292,26 +291,22 @@ double UNet::train_step(int n, const float* b_split, const float* p_split, const
     const long V1 = long(n) * n * n;
     if (target_.n != size_t(V1)) {
         target_.allocate(V1);
-        diff_.allocate(V1);
         gout_.allocate(V1);
     }
     launch_prep_input(n, b_split, ctrl, partial_.p, scale_.p, bf(in0_), s_);
     launch_target(n, p_split, ctrl, scale_.p, target_.p, s_);
     forward(n);
-    launch_loss_grad(V1, out_.p, target_.p, diff_.p, partial_.p, scalars_.p, gout_.p, s_);
-    // loss = sum of partials / V (the partials of k_loss_grad)
-    std::vector<double> h(1184);
-    const int blocks = int(std::max<long>(1, std::min<long>((V1 + 255) / 256, 1184)));
-    VB_CUDA(cudaMemcpyAsync(h.data(), partial_.p, blocks * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    launch_loss_grad(V1, out_.p, target_.p, partial_.p, scalars_.p, gout_.p, s_);
+    double loss = 0.0;
+    VB_CUDA(cudaMemcpyAsync(&loss_host_, scalars_.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s_));
     grad_.zero(s_);
     backward(n);
     ++step_;
     launch_adam(parameter_count(), params_.p, m_.p, v_.p, grad_.p, bf(wbf_), lr, step_, s_);
     VB_CUDA(cudaStreamSynchronize(s_));
     if (error_flag()) fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out");
-    double loss = 0.0;
-    for (int i = 0; i < blocks; ++i) loss += h[i];
-    return loss / double(V1);
+    loss = loss_host_;
+    return loss;
 }
 
 double UNet::evaluate(int n, const float* b_split, const float* p_split, const ProjControl* ctrl) {
@@ -319,20 +314,16 @@ double UNet::evaluate(int n, const float* b_split, const float* p_split, const P
     const long V1 = long(n) * n * n;
     if (target_.n != size_t(V1)) {
         target_.allocate(V1);
-        diff_.allocate(V1);
         gout_.allocate(V1);
     }
     launch_prep_input(n, b_split, ctrl, partial_.p, scale_.p, bf(in0_), s_);
     launch_target(n, p_split, ctrl, scale_.p, target_.p, s_);
     forward(n);
-    launch_loss_grad(V1, out_.p, target_.p, diff_.p, partial_.p, scalars_.p, gout_.p, s_);
-    std::vector<double> h(1184);
-    const int blocks = int(std::max<long>(1, std::min<long>((V1 + 255) / 256, 1184)));
-    VB_CUDA(cudaMemcpyAsync(h.data(), partial_.p, blocks * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    launch_loss_grad(V1, out_.p, target_.p, partial_.p, scalars_.p, nullptr, s_);
+    VB_CUDA(cudaMemcpyAsync(&loss_host_, scalars_.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s_));
     VB_CUDA(cudaStreamSynchronize(s_));
-    double loss = 0.0;
-    for (int i = 0; i < blocks; ++i) loss += h[i];
-    return loss / double(V1);
+    if (error_flag()) fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out");
+    return loss_host_;
 }
 
 }  // namespace unet

@@ -60,12 +60,17 @@ void launch_upsample2(int d, int h, int w, int C, const __nv_bfloat16* in, __nv_
 void launch_head(long V, int C, const __nv_bfloat16* act, const float* w, const float* bias, float* out,
                  cudaStream_t s);
 void launch_mean(long V, const float* a, double* partial, double* mean, cudaStream_t s);
-void launch_store_warm_start(int n, const float* p, const float* scale, const double* mean, float* x_split,
-                             double* x64_split, cudaStream_t s);
+// x = alpha (p - mean p) into the solver's split iterate (FP32 or FP64), alpha
+// by the Galerkin condition against the mean-free right-hand side. Uses
+// partial[0..1183] and scalars[0..1].
+void launch_store_warm_start(int n, const float* p, const float* b_split, const ProjControl* ctrl,
+                             double* partial, double* scalars, float* x_split, double* x64_split, cudaStream_t s);
 void launch_target(int n, const float* p_split, const ProjControl* ctrl, const float* scale, float* target,
                    cudaStream_t s);
-void launch_loss_grad(long V, const float* p, const float* t, float* diff, double* partial, double* mean_e,
-                      float* grad, cudaStream_t s);
+// Scale-invariant loss 1 - cos^2(p - mean p, t - mean t) into scalars[2] and,
+// when grad is given, its gradient with respect to p. Uses scalars[0..4].
+void launch_loss_grad(long V, const float* p, const float* t, double* partial, double* scalars, float* grad,
+                      cudaStream_t s);
 void launch_head_backward(long V, int C, const __nv_bfloat16* act, const float* w, const float* g,
                           __nv_bfloat16* dact, float* dw, float* db, cudaStream_t s);
 void launch_relu_mask(long V, int C, const __nv_bfloat16* act, int act_stride, int act_offset, __nv_bfloat16* g,
@@ -101,11 +106,16 @@ class UNet {
 public:
     explicit UNet(cudaStream_t stream);
     ~UNet();
-    // The stream all later work is ordered on (the owning simulation's).
+    // The stream all later work is ordered on (the owning simulation's while
+    // a simulation uses the network, else the one given at construction).
     void set_stream(cudaStream_t s) { s_ = s; }
+    void use_own_stream() { s_ = own_; }
     cudaStream_t stream() const { return s_; }
     // Allocates the activation buffers for n (outside any stream capture).
     void prepare(int n) { ensure(n); }
+    // Incremented whenever the activation buffers are reallocated; a recorded
+    // CUDA graph that uses the network is valid only for one generation.
+    unsigned long long generation() const { return generation_; }
     UNet(const UNet&) = delete;
     UNet& operator=(const UNet&) = delete;
 
@@ -114,13 +124,15 @@ public:
     void init_parameters(unsigned seed);      // He-uniform weights, zero biases
 
     // Forward on an n^3 grid (n divisible by 4) from the solver's split RHS;
-    // writes the warm start x = scale * (p - mean p) into x_split (FP32) or
-    // x64_split (FP64). Returns nothing; errors raise.
+    // writes the warm start x = alpha * (p - mean p) into x_split (FP32) or
+    // x64_split (FP64), alpha = (q.b)/(q.Aq) for q = p - mean p. Errors raise.
     void infer_into(int n, const float* b_split, const ProjControl* ctrl, float* x_split, double* x64_split);
     // One training step on (b, p*) from a finished projection: forward,
     // loss, backward, Adam. Returns the loss (waits for the device).
     double train_step(int n, const float* b_split, const float* p_split, const ProjControl* ctrl, float lr);
-    // Forward only and the loss against p* (no update); waits.
+    // Forward only and the loss against p* (no update); waits. The loss is
+    // the relative squared error left after the best scaling of the
+    // prediction, 1 - cos^2 between the mean-free prediction and p*.
     double evaluate(int n, const float* b_split, const float* p_split, const ProjControl* ctrl);
     unsigned int error_flag();
     int adam_steps() const { return step_; }
@@ -137,8 +149,10 @@ private:
               int out_offset, bool relu, bool fp32_out = false);
 
     cudaStream_t s_;
+    cudaStream_t own_;
     int n_ = 0;
     int step_ = 0;
+    unsigned long long generation_ = 0;
     DevArray<float> params_, grad_, m_, v_;
     DevArray<uint16_t> wbf_;   // BF16 copy of the parameters
     DevArray<uint16_t> wflip_;  // flipped/transposed weights of one layer
@@ -146,7 +160,8 @@ private:
     DevArray<uint16_t> in0_, e1a_, dec1_, e2in_, e2a_, dec2_, e3in_, e3a_, e3b_, d2a_, d2b_, d1a_, d1b_;
     // gradients (BF16)
     DevArray<uint16_t> g1_, g2_, g3_, g4_;
-    DevArray<float> out_, target_, diff_, gout_;
+    DevArray<float> out_, target_, gout_;
+    double loss_host_ = 0.0;
     DevArray<double> partial_, scalars_;
     DevArray<float> scale_;
     DevArray<uint32_t> error_;

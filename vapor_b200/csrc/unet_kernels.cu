@@ -225,27 +225,80 @@ __global__ void k_head(long V, int C, const __nv_bfloat16* __restrict__ act, con
     }
 }
 
-// Warm start into the solver's split iterate: x = scale * (p - mean p).
-__global__ void k_store_warm_start(int n, const float* __restrict__ p, const float* __restrict__ scale,
+// Warm start scale by the Galerkin condition on span{q}, q = p - mean p:
+// alpha = (q . b) / (q . A q) minimises the A-norm error of alpha q against the
+// exact pressure (A: the Neumann 7-point operator of the residual, b: the
+// mean-free right-hand side). The network then only has to predict the shape
+// of the pressure, and the guess is never worse than zero in the A-norm.
+__global__ void k_galerkin_sums(int n, const float* __restrict__ p, const double* __restrict__ mean,
+                                const float* __restrict__ b_split, const ProjControl* __restrict__ ctrl,
+                                double* __restrict__ partial) {
+    __shared__ double s_sum[32];
+    const RBLayout L = rb_layout(n);
+    const long V = long(n) * n * n;
+    const double m = *mean;
+    const float bm = ctrl->rhs_mean_f;
+    double num = 0.0, den = 0.0;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(v, n, n, x, y, z);
+        const double q = double(p[v]) - m;
+        double aq = 0.0;
+        int nb = 0;
+        auto add = [&](long u) {
+            aq -= double(p[u]) - m;
+            ++nb;
+        };
+        if (x > 0) add(v - 1);
+        if (x + 1 < n) add(v + 1);
+        if (y > 0) add(v - n);
+        if (y + 1 < n) add(v + n);
+        if (z > 0) add(v - long(n) * n);
+        if (z + 1 < n) add(v + long(n) * n);
+        aq += double(nb) * q;
+        num += q * double(b_split[rb_index(L, x, y, z)] - bm);
+        den += q * aq;
+    }
+    const double sn = block_sum(num, s_sum);
+    const double sd = block_sum(den, s_sum);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = sn;
+        partial[2 * blockIdx.x + 1] = sd;
+    }
+}
+__global__ void k_galerkin_finish(const double* __restrict__ partial, int blocks, double* __restrict__ alpha) {
+    __shared__ double s_sum[32];
+    double num = 0.0, den = 0.0;
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x) {
+        num += partial[2 * i];
+        den += partial[2 * i + 1];
+    }
+    const double sn = block_sum(num, s_sum);
+    const double sd = block_sum(den, s_sum);
+    if (threadIdx.x == 0) *alpha = (sd > 0.0 && isfinite(sn / sd)) ? sn / sd : 0.0;
+}
+
+// Warm start into the solver's split iterate: x = alpha * (p - mean p).
+__global__ void k_store_warm_start(int n, const float* __restrict__ p, const double* __restrict__ alpha,
                                    const double* __restrict__ mean, float* __restrict__ x_split) {
     const RBLayout L = rb_layout(n);
     const long V = long(n) * n * n;
-    const float s = *scale, m = float(*mean);
+    const double a = *alpha, m = *mean;
     for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode(v, n, n, x, y, z);
-        x_split[rb_index(L, x, y, z)] = s * (p[v] - m);
+        x_split[rb_index(L, x, y, z)] = float(a * (double(p[v]) - m));
     }
 }
-__global__ void k_store_warm_start64(int n, const float* __restrict__ p, const float* __restrict__ scale,
+__global__ void k_store_warm_start64(int n, const float* __restrict__ p, const double* __restrict__ alpha,
                                      const double* __restrict__ mean, double* __restrict__ x_split) {
     const RBLayout L = rb_layout(n);
     const long V = long(n) * n * n;
-    const double s = double(*scale), m = *mean;
+    const double a = *alpha, m = *mean;
     for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode(v, n, n, x, y, z);
-        x_split[rb_index(L, x, y, z)] = s * (double(p[v]) - m);
+        x_split[rb_index(L, x, y, z)] = a * (double(p[v]) - m);
     }
 }
 
@@ -280,29 +333,58 @@ __global__ void k_target(int n, const float* __restrict__ p_split, const ProjCon
     }
 }
 
-// Loss L = mean(((p - mean p) - t)^2) and dL/dp = 2/V * (e - mean e) with
-// e = p - t (t has zero mean). Writes per-block partial losses.
-__global__ void k_loss_grad(long V, const float* __restrict__ p, const float* __restrict__ t,
-                            const double* __restrict__ mean_e, float* __restrict__ grad,
-                            double* __restrict__ partial) {
+// Scale-invariant loss: with q = p - mean p and r = t - mean t,
+//   L = min_c |c q - r|^2 / |r|^2 = 1 - (q.r)^2 / (|q|^2 |r|^2),
+// the relative squared error left after the best scaling of the prediction
+// (the warm start applies its own scale). Per-block sums of q.r, q.q, r.r.
+__global__ void k_loss_sums(long V, const float* __restrict__ p, const float* __restrict__ t,
+                            const double* __restrict__ means, double* __restrict__ partial) {
     __shared__ double s_sum[32];
-    const double me = *mean_e;
-    double acc = 0.0;
+    const double mp = means[0], mt = means[1];
+    double qr = 0.0, qq = 0.0, rr = 0.0;
     for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
-        const double e = double(p[v]) - double(t[v]) - me;
-        acc += e * e;
-        grad[v] = float(2.0 * e / double(V));
+        const double q = double(p[v]) - mp, r = double(t[v]) - mt;
+        qr += q * r;
+        qq += q * q;
+        rr += r * r;
     }
-    const double s = block_sum(acc, s_sum);
-    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    const double a = block_sum(qr, s_sum);
+    const double b = block_sum(qq, s_sum);
+    const double c = block_sum(rr, s_sum);
+    if (threadIdx.x == 0) {
+        partial[3 * blockIdx.x] = a;
+        partial[3 * blockIdx.x + 1] = b;
+        partial[3 * blockIdx.x + 2] = c;
+    }
 }
-__global__ void k_diff(long V, const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out) {
+// scalars: [0] mean p, [1] mean t, [2] loss, [3] coefficient of r, [4] of q.
+__global__ void k_loss_finish(const double* __restrict__ partial, int blocks, double* __restrict__ scalars) {
+    __shared__ double s_sum[32];
+    double qr = 0.0, qq = 0.0, rr = 0.0;
+    for (int i = threadIdx.x; i < blocks; i += blockDim.x) {
+        qr += partial[3 * i];
+        qq += partial[3 * i + 1];
+        rr += partial[3 * i + 2];
+    }
+    const double a = block_sum(qr, s_sum);
+    const double b = block_sum(qq, s_sum);
+    const double c = block_sum(rr, s_sum);
+    if (threadIdx.x == 0) {
+        const bool ok = b > 0.0 && c > 0.0;
+        scalars[2] = ok ? 1.0 - a * a / (b * c) : 1.0;
+        // dL/dq = -2 (q.r)/(|q|^2 |r|^2) r + 2 (q.r)^2/(|q|^4 |r|^2) q; it has
+        // zero mean, so it is also dL/dp.
+        scalars[3] = ok ? -2.0 * a / (b * c) : 0.0;
+        scalars[4] = ok ? 2.0 * a * a / (b * b * c) : 0.0;
+    }
+}
+__global__ void k_loss_grad(long V, const float* __restrict__ p, const float* __restrict__ t,
+                            const double* __restrict__ scalars, float* __restrict__ grad) {
+    const double mp = scalars[0], mt = scalars[1], cr = scalars[3], cq = scalars[4];
     for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x)
-        out[v] = a[v] - b[v];
+        grad[v] = float(cr * (double(t[v]) - mt) + cq * (double(p[v]) - mp));
 }
 
-// Head backward: d_act[v,c] = g[v] * w[c] (BF16, masked by act > 0 for the
-// ReLU before the head), dw[c] += sum g*act, db += sum g.
 __global__ void k_head_backward(long V, int C, const __nv_bfloat16* __restrict__ act, const float* __restrict__ w,
                                 const float* __restrict__ g, __nv_bfloat16* __restrict__ dact,
                                 float* __restrict__ dw, float* __restrict__ db) {
@@ -553,12 +635,18 @@ void launch_mean(long V, const float* a, double* partial, double* mean, cudaStre
     k_mean_finish<<<1, 1024, 0, s>>>(partial, blocks, double(V), mean);
 }
 
-void launch_store_warm_start(int n, const float* p, const float* scale, const double* mean, float* x_split,
-                             double* x64_split, cudaStream_t s) {
+void launch_store_warm_start(int n, const float* p, const float* b_split, const ProjControl* ctrl,
+                             double* partial, double* scalars, float* x_split, double* x64_split, cudaStream_t s) {
     const long V = long(n) * n * n;
+    launch_mean(V, p, partial, scalars, s);
+    const int blocks = std::min(blocks_for(V), 592);
     count_launch();
-    if (x64_split) k_store_warm_start64<<<blocks_for(V), 256, 0, s>>>(n, p, scale, mean, x64_split);
-    else k_store_warm_start<<<blocks_for(V), 256, 0, s>>>(n, p, scale, mean, x_split);
+    k_galerkin_sums<<<blocks, 256, 0, s>>>(n, p, scalars, b_split, ctrl, partial);
+    count_launch();
+    k_galerkin_finish<<<1, 1024, 0, s>>>(partial, blocks, scalars + 1);
+    count_launch();
+    if (x64_split) k_store_warm_start64<<<blocks_for(V), 256, 0, s>>>(n, p, scalars + 1, scalars, x64_split);
+    else k_store_warm_start<<<blocks_for(V), 256, 0, s>>>(n, p, scalars + 1, scalars, x_split);
 }
 
 void launch_target(int n, const float* p_split, const ProjControl* ctrl, const float* scale, float* target,
@@ -567,14 +655,19 @@ void launch_target(int n, const float* p_split, const ProjControl* ctrl, const f
     k_target<<<blocks_for(long(n) * n * n), 256, 0, s>>>(n, p_split, ctrl, scale, target);
 }
 
-void launch_loss_grad(long V, const float* p, const float* t, float* diff, double* partial, double* mean_e,
-                      float* grad, cudaStream_t s) {
-    const int blocks = std::min(blocks_for(V), 1184);
+void launch_loss_grad(long V, const float* p, const float* t, double* partial, double* scalars, float* grad,
+                      cudaStream_t s) {
+    launch_mean(V, p, partial, scalars, s);
+    launch_mean(V, t, partial, scalars + 1, s);
+    const int blocks = std::min(blocks_for(V), 392);
     count_launch();
-    k_diff<<<blocks_for(V), 256, 0, s>>>(V, p, t, diff);
-    launch_mean(V, diff, partial, mean_e, s);
+    k_loss_sums<<<blocks, 256, 0, s>>>(V, p, t, scalars, partial);
     count_launch();
-    k_loss_grad<<<blocks, 256, 0, s>>>(V, p, t, mean_e, grad, partial);
+    k_loss_finish<<<1, 1024, 0, s>>>(partial, blocks, scalars);
+    if (grad) {
+        count_launch();
+        k_loss_grad<<<blocks_for(V), 256, 0, s>>>(V, p, t, scalars, grad);
+    }
 }
 
 void launch_head_backward(long V, int C, const __nv_bfloat16* act, const float* w, const float* g,
