@@ -77,7 +77,13 @@ typedef enum vapor_face_axis { VAPOR_FACE_X = 0, VAPOR_FACE_Y = 1, VAPOR_FACE_Z 
  * kinds are extensions that always finish with the same residual test. */
 typedef enum vapor_solver_kind {
     VAPOR_SOLVER_RED_BLACK_SOR = 0,
-    VAPOR_SOLVER_MIXED_REFINEMENT = 1 /* FP32 SOR inner sweeps, FP64 residual and correction */
+    VAPOR_SOLVER_MIXED_REFINEMENT = 1, /* FP32 SOR inner sweeps, FP64 residual and correction */
+    /* Flexible PCG: FP32 vectors, FP64 dot products, FP64 residual and
+     * re-centring. Preconditioner: 2 red-black Gauss-Seidel sweeps, the
+     * learned coarse-grid correction when a network is attached
+     * (vapor_mac3d_set_preconditioner / vapor_stage_set_preconditioner), then
+     * 2 sweeps in reverse colour order. Iterations count CG steps. */
+    VAPOR_SOLVER_FPCG = 2
 } vapor_solver_kind;
 
 /* LinearSolveOptions / LinearSolveResult (src/common/LinearSolveOptions.hpp:4-24). */
@@ -171,7 +177,9 @@ typedef enum vapor_phase {
     VAPOR_PHASE_SOR = 3,       /* red-black colour sweeps */
     VAPOR_PHASE_RESIDUAL = 4,  /* FP64 residual checks and re-centring */
     VAPOR_PHASE_GRADIENT = 5,  /* pressure gauge, final residual, gradient, divergence after */
-    VAPOR_PHASE_COUNT = 6
+    VAPOR_PHASE_KRYLOV = 6,    /* FPCG: A p, dot products, vector updates */
+    VAPOR_PHASE_COARSE = 7,    /* FPCG: restriction, network, Galerkin scale, prolongation */
+    VAPOR_PHASE_COUNT = 8
 } vapor_phase;
 
 typedef struct vapor_phase_timings {
@@ -360,6 +368,21 @@ vapor_status vapor_mac3d_train_warm_start(vapor_mac3d *sim, vapor_unet *net, flo
                                           double *loss);
 /* The same loss without an update. */
 vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d *sim, vapor_unet *net, double *loss);
+/* Coarse-grid correction of the VAPOR_SOLVER_FPCG preconditioner (NULL: the
+ * smoothing-only preconditioner). The network runs on the grid coarsened 4x
+ * per axis (right-hand side: 4^3 block sums of the smoothed residual), its
+ * output is scaled by the Galerkin condition of the coarse operator 16 L and
+ * prolonged piecewise constant. Needs n divisible by 16 (n >= 32). The
+ * network must outlive the simulation or be detached first, and serves one
+ * simulation or stage at a time (its activation buffers are shared state). */
+vapor_status vapor_mac3d_set_preconditioner(vapor_mac3d *sim, vapor_unet *net);
+vapor_status vapor_stage_set_preconditioner(vapor_stage *stage, vapor_unet *net);
+/* One Adam step of `net` on the stage's last projection (its right-hand side
+ * and converged pressure, on the stage's own n^3 grid); the loss as for
+ * vapor_mac3d_train_warm_start. Used to train the coarse-grid network on
+ * solves at the coarse resolution. */
+vapor_status vapor_stage_train_network(vapor_stage *stage, vapor_unet *net, float learning_rate,
+                                       double *loss);
 
 #ifdef __cplusplus
 }

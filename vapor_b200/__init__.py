@@ -119,6 +119,9 @@ def _declare(lib):
     f("vapor_mac3d_set_warm_start", _vp, _vp)
     f("vapor_mac3d_train_warm_start", _vp, _vp, C.c_float, C.POINTER(C.c_double))
     f("vapor_mac3d_evaluate_warm_start", _vp, _vp, C.POINTER(C.c_double))
+    f("vapor_mac3d_set_preconditioner", _vp, _vp)
+    f("vapor_stage_set_preconditioner", _vp, _vp)
+    f("vapor_stage_train_network", _vp, _vp, C.c_float, C.POINTER(C.c_double))
     return lib
 
 
@@ -315,6 +318,11 @@ class MacSimulation3D:
         check(library().vapor_mac3d_evaluate_warm_start(self._h, net.handle, C.byref(loss)))
         return loss.value
 
+    def set_preconditioner(self, net):
+        """Learned coarse-grid correction of the FPCG solver (None: smoothing only)."""
+        check(library().vapor_mac3d_set_preconditioner(self._h, net.handle if net is not None else None))
+        self._coarse = net
+
 
 class StageBackend:
     """Staged Projection3D / Advection3D plugins over host (numpy) spans."""
@@ -337,6 +345,17 @@ class StageBackend:
 
     def set_solver_kind(self, kind):
         check(library().vapor_stage_set_solver_kind(self._h, int(kind)))
+
+    def set_preconditioner(self, net):
+        """Coarse-grid network of the FPCG solver (None: smoothing only)."""
+        check(library().vapor_stage_set_preconditioner(self._h, net.handle if net is not None else None))
+        self._coarse = net
+
+    def train_network(self, net, learning_rate):
+        """One Adam step of `net` on this stage's last projection; returns the loss."""
+        loss = C.c_double()
+        check(library().vapor_stage_train_network(self._h, net.handle, float(learning_rate), C.byref(loss)))
+        return loss.value
 
     def project(self, u, v, w, options, diagonal_floor=0.0, want_pressure=False):
         """Projection3D::project in place on (u, v, w); returns (result, pressure)."""

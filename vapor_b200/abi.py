@@ -27,6 +27,7 @@ FACE_X, FACE_Y, FACE_Z = 0, 1, 2
 
 SOLVER_RED_BLACK_SOR = 0
 SOLVER_MIXED_REFINEMENT = 1
+SOLVER_FPCG = 2
 
 
 class LinearSolveOptions(C.Structure):
@@ -126,11 +127,11 @@ class MacParams(C.Structure):
         return self
 
 
-PHASES = ("forcing", "advect", "rhs", "sor", "residual", "gradient")
+PHASES = ("forcing", "advect", "rhs", "sor", "residual", "gradient", "krylov", "coarse")
 
 
 class PhaseTimings(C.Structure):
-    _fields_ = [("milliseconds", C.c_double * 6), ("launches", C.c_int64 * 6), ("intervals", C.c_int64 * 6)]
+    _fields_ = [("milliseconds", C.c_double * 8), ("launches", C.c_int64 * 8), ("intervals", C.c_int64 * 8)]
 
     def as_dict(self):
         return {name: {"ms": self.milliseconds[i], "launches": self.launches[i], "intervals": self.intervals[i]}

@@ -274,7 +274,8 @@ VB_API vapor_status vapor_stage_advect_scalar_device(vapor_stage* stage, float d
     STAGE_GUARD(stage->stage.advect(0, dt, cfl_limit, method, field, fu, fv, fw, field, true));
 }
 VB_API vapor_status vapor_stage_set_solver_kind(vapor_stage* stage, int32_t kind) {
-    STAGE_GUARD(require(kind == VAPOR_SOLVER_RED_BLACK_SOR || kind == VAPOR_SOLVER_MIXED_REFINEMENT,
+    STAGE_GUARD(require(kind == VAPOR_SOLVER_RED_BLACK_SOR || kind == VAPOR_SOLVER_MIXED_REFINEMENT ||
+                            kind == VAPOR_SOLVER_FPCG,
                         "Unknown solver kind");
                 stage->stage.solver_kind = kind);
 }
@@ -348,6 +349,14 @@ VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float*
 VB_API vapor_status vapor_mac3d_set_warm_start(vapor_mac3d* sim, vapor_unet* net) {
     SIM_GUARD(sim->sim.set_warm_start(net ? &net->net : nullptr));
 }
+VB_API vapor_status vapor_mac3d_set_preconditioner(vapor_mac3d* sim, vapor_unet* net) {
+    SIM_GUARD(sim->sim.set_preconditioner(net ? &net->net : nullptr));
+}
+VB_API vapor_status vapor_stage_set_preconditioner(vapor_stage* stage, vapor_unet* net) {
+    STAGE_GUARD(if (net && (stage->stage.n() % 16 != 0 || stage->stage.n() < 32))
+                    vb::fail(VAPOR_INVALID_ARGUMENT, "the coarse-grid network needs n divisible by 16 (n >= 32)");
+                stage->stage.coarse = net ? &net->net : nullptr);
+}
 VB_API vapor_status vapor_mac3d_train_warm_start(vapor_mac3d* sim, vapor_unet* net, float learning_rate,
                                                  double* loss) {
     SIM_GUARD(require(net != nullptr, "null network handle");
@@ -355,6 +364,21 @@ VB_API vapor_status vapor_mac3d_train_warm_start(vapor_mac3d* sim, vapor_unet* n
               vb::Workspace& ws = sim->sim.workspace(); StreamBinding bind(sim->sim, net->net, ws.stream());
               const double l = net->net.train_step(ws.n(), ws.rhs(), ws.pressure(), ws.control(), learning_rate);
               if (loss) *loss = l);
+}
+VB_API vapor_status vapor_stage_train_network(vapor_stage* stage, vapor_unet* net, float learning_rate,
+                                              double* loss) {
+    STAGE_GUARD(require(net != nullptr, "null network handle");
+                require(std::isfinite(learning_rate) && learning_rate > 0.f, "invalid learning rate");
+                vb::Workspace& ws = stage->stage.workspace(); net->net.set_stream(ws.stream());
+                double l = 0.0;
+                try {
+                    l = net->net.train_step(ws.n(), ws.rhs(), ws.pressure(), ws.control(), learning_rate);
+                } catch (...) {
+                    net->net.use_own_stream();
+                    throw;
+                }
+                net->net.use_own_stream();
+                if (loss) *loss = l);
 }
 VB_API vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d* sim, vapor_unet* net, double* loss) {
     SIM_GUARD(require(net != nullptr, "null network handle"); vb::Workspace& ws = sim->sim.workspace();

@@ -164,6 +164,7 @@ Workspace::Workspace(int n, float box, cudaStream_t stream)
 Workspace::~Workspace() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (ctrl_) cudaFree(ctrl_);
+    if (cg_) cudaFree(cg_);
     if (diag_) cudaFree(diag_);
     if (ctrl_host_) cudaFreeHost(ctrl_host_);
     if (diag_host_) cudaFreeHost(diag_host_);
@@ -194,7 +195,10 @@ void Workspace::ensure_mixed() {
     const size_t cells = rb_count(n_);
     for (auto& x : x64_)
         if (x.n != cells) x.allocate(cells);
-    if (r32_.n != cells) r32_.allocate(cells);
+    if (r32_.n != cells) {
+        r32_.allocate(cells);
+        r32_.zero(stream_);  // padding slots stay zero (they enter the CG dot products)
+    }
 }
 
 // Adds a while-loop node at the current capture position of stream `s` whose
@@ -242,16 +246,128 @@ static cudaGraphConditionalHandle new_condition(cudaStream_t s) {
     return h;
 }
 
+void Workspace::ensure_fpcg(bool coarse) {
+    const size_t count = rb_count(n_);
+    for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_})
+        if (v->n != count) {
+            v->allocate(count);
+            v->zero(stream_);
+        }
+    if (cg_partials_.n < size_t(cg_partial_capacity())) cg_partials_.allocate(cg_partial_capacity());
+    if (!cg_) VB_CUDA(cudaMalloc(&cg_, sizeof(CgControl)));
+    if (coarse) {
+        if (n_ % 16 != 0 || n_ < 32)
+            fail(VAPOR_INVALID_ARGUMENT, "the coarse-grid network needs n divisible by 16 (n >= 32)");
+        const size_t nc = size_t(n_ / 4);
+        if (cg_rc_.n != nc * nc * nc) cg_rc_.allocate(nc * nc * nc);
+    }
+}
+
+// Flexible PCG on the error equation with FP64 re-centring (x64 += e,
+// r = float(b - A x64), e = 0) whenever the FP32 recurrence residual reaches
+// the target or drops by kRecentreDrop; stops when the FP64 residual meets
+// the target. Preconditioner: kFpcgSmoothing red-black Gauss-Seidel sweeps,
+// the coarse-grid correction when `coarse` is given, then the same sweeps in
+// reverse colour order. Iterations count CG steps.
+void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UNet* coarse, LoopCond cond,
+                             cudaGraphConditionalHandle handle) {
+    cudaStream_t s = stream_;
+    PhaseTimer& t = timer_;
+    const bool graph = capturing_;
+    const size_t count = rb_count(n_);
+    float* e = p_.p;
+    float* r = r32_.p;
+    const ProjectionArgs smooth{a.g, a.dt, 1.0f, 0.0f, a.options};
+    if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);
+    else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
+    t.begin(VAPOR_PHASE_RESIDUAL);
+    launch_refine_residual(a, b_.p, e, r, ctrl_, s);
+    launch_check(ctrl_, 0, false, true, cond, s);
+    t.end(VAPOR_PHASE_RESIDUAL, 2);
+    auto precondition = [&](cudaStream_t st) {
+        t.begin(VAPOR_PHASE_SOR);
+        VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
+        for (int j = 0; j < kFpcgSmoothing; ++j) {
+            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+        }
+        t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
+        if (coarse) {
+            t.begin(VAPOR_PHASE_COARSE);
+            launch_restrict_residual(n_, r, cg_z_.p, cg_rc_.p, st);
+            coarse->set_stream(st);
+            const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
+            coarse->set_stream(s);
+            launch_coarse_correction(n_, cg_z_.p, zc, cg_rc_.p, cg_partials_.p, cg_, st);
+            t.end(VAPOR_PHASE_COARSE, 0);
+        }
+        t.begin(VAPOR_PHASE_SOR);
+        for (int j = 0; j < kFpcgSmoothing; ++j) {
+            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+        }
+        t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
+    };
+    auto recentre_group = [&](cudaStream_t st) {
+        launch_refine_residual_gated(a, b_.p, e, r, ctrl_, st);
+        launch_check_gated(ctrl_, LoopCond{}, st);
+        launch_zero_error_gated(a, e, ctrl_, st);
+    };
+    auto iteration = [&](cudaStream_t st) {
+        t.begin(VAPOR_PHASE_KRYLOV);
+        launch_apply_A(n_, cg_p_.p, cg_q_.p, st);
+        launch_cg_alpha(count, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
+        t.end(VAPOR_PHASE_KRYLOV, 3);
+        t.begin(VAPOR_PHASE_RESIDUAL);
+        if (graph) {
+            const cudaGraphConditionalHandle ifh = new_condition(st);
+            LoopCond if_cond;
+            if_cond.active = 1;
+            if_cond.handle = (unsigned long long)ifh;
+            launch_cg_update(count, e, r, cg_p_.p, cg_q_.p, cg_, ctrl_, if_cond, st);
+            add_conditional(st, body_stream2_.s, ifh, cudaGraphCondTypeIf,
+                            [&](cudaStream_t is) { recentre_group(is); });
+        } else {
+            launch_cg_update(count, e, r, cg_p_.p, cg_q_.p, cg_, ctrl_, LoopCond{}, st);
+            recentre_group(st);
+        }
+        t.end(VAPOR_PHASE_RESIDUAL, 5);
+        precondition(st);
+        t.begin(VAPOR_PHASE_KRYLOV);
+        launch_cg_beta(count, cg_z_.p, r, cg_q_.p, cg_partials_.p, cg_, st);
+        launch_cg_direction(count, cg_p_.p, cg_z_.p, cg_, st);
+        t.end(VAPOR_PHASE_KRYLOV, 3);
+        launch_loop_condition(ctrl_, cond, st);
+    };
+    precondition(s);
+    launch_cg_rho(count, cg_z_.p, r, cg_partials_.p, cg_, s);
+    VB_CUDA(cudaMemcpyAsync(cg_p_.p, cg_z_.p, cg_z_.bytes(), cudaMemcpyDeviceToDevice, s));
+    if (graph) {
+        add_while_loop(s, body_stream_.s, handle, iteration);
+    } else {
+        auto wait_done = [&]() {
+            VB_CUDA(cudaMemcpyAsync(done_host_, &ctrl_->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+            VB_CUDA(cudaStreamSynchronize(s));
+            t.fold(false);
+            return *done_host_ != 0;
+        };
+        while (!wait_done()) iteration(s);
+    }
+}
+
 void Workspace::project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo,
                         float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
-                        const vapor_linear_solve_options& o, int solver_kind, unet::UNet* warm) {
+                        const vapor_linear_solve_options& o, int solver_kind, unet::UNet* warm,
+                        unet::UNet* coarse) {
     const ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
     cudaStream_t s = stream_;
     PhaseTimer& t = timer_;
-    const bool mixed = solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT;
+    const bool fpcg = solver_kind == VAPOR_SOLVER_FPCG;
+    const bool mixed = solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT || fpcg;
     const bool graph = capturing_;
     const int interval = o.residual_check_interval;
     if (mixed) ensure_mixed();
+    if (fpcg) ensure_fpcg(coarse != nullptr);
     // A device-side while loop is recorded only when the solve has one; a
     // conditional handle that no node uses makes graph instantiation fail.
     const bool loop = graph && (mixed || !o.fixed_iterations || o.max_iterations > interval);
@@ -290,7 +406,13 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), s));
     t.end(VAPOR_PHASE_RHS, 3);
 
-    if (mixed) {
+    if (fpcg) {
+        project_fpcg(a, warm, coarse, cond, handle);
+        t.begin(VAPOR_PHASE_GRADIENT);
+        launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
+        launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        t.end(VAPOR_PHASE_GRADIENT, 5);
+    } else if (mixed) {
         // FP32 red-black sweeps on the error equation A e = r32. Every check
         // interval the FP32 residual of that equation decides whether to
         // re-centre in FP64 (x64 += e, r32 = b - A x64, e = 0) and test the FP64
@@ -432,7 +554,8 @@ Simulation::Simulation(int n, float box, const vapor_mac3d_params& p) : params(p
 Simulation::~Simulation() {
     cudaStreamSynchronize(ws_.stream());
     release_graphs();
-    if (warm_) warm_->use_own_stream();  // the network outlives this simulation's stream
+    if (warm_) warm_->use_own_stream();  // the networks outlive this simulation's stream
+    if (coarse_) coarse_->use_own_stream();
 }
 
 void Simulation::reset() {
@@ -531,7 +654,8 @@ void Simulation::validate_step(float dt) const {
         !std::isfinite(p.stir_strength) || !std::isfinite(p.cfl_mc) || p.cfl_mc <= 0.f)
         fail(VAPOR_INVALID_ARGUMENT, "Invalid resident GPU step parameters");
     if (p.use_solve_options && !valid_options(p.solve)) fail(VAPOR_INVALID_ARGUMENT, "Invalid linear solve options");
-    if (p.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && p.solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
+    if (p.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && p.solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT &&
+        p.solver_kind != VAPOR_SOLVER_FPCG)
         fail(VAPOR_INVALID_ARGUMENT, "Unknown solver kind");
     if (p.emitter_count < 1 || p.emitter_count > 2) fail(VAPOR_INVALID_ARGUMENT, "emitter_count must be 1 or 2");
     if (p.emitter_profile < 0 || p.emitter_profile > 1) fail(VAPOR_INVALID_ARGUMENT, "emitter_profile must be 0 or 1");
@@ -558,16 +682,16 @@ void Simulation::record_step(float dt) {
         advect_velocity(half, S_, S_, T_);  // T = advected (tilde)
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
                     vel_[U_][0].p, vel_[U_][1].p, vel_[U_][2].p, half, p.sor_omega, 6.f, o,
-                    p.solver_kind, warm_);  // S = projected, U = hat
+                    p.solver_kind, warm_, coarse_);  // S = projected, U = hat
         advect_velocity(half, U_, S_, T_);
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
-                    nullptr, nullptr, nullptr, half, p.sor_omega, 6.f, o, p.solver_kind, warm_);
+                    nullptr, nullptr, nullptr, half, p.sor_omega, 6.f, o, p.solver_kind, warm_, coarse_);
     } else {
         // MacGridFluidSolver3D::stepNoReflect (MacGridFluidSolver3D.cpp:230-245).
         advect_velocity(dt, S_, S_, T_);
         ws_.project(vel_[T_][0].p, vel_[T_][1].p, vel_[T_][2].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p,
                     nullptr, nullptr, nullptr, dt, p.sor_omega, 6.f, solve_options(p.project_iterations),
-                    p.solver_kind, warm_);
+                    p.solver_kind, warm_, coarse_);
     }
     // Smoke transport through the projected velocity, then dissipation
     // (MacGridFluidSolver3D.cpp:183-190) fused as a post-scale.
@@ -586,6 +710,19 @@ void Simulation::set_warm_start(unet::UNet* net) {
     if (warm_) {
         warm_->set_stream(ws_.stream());
         warm_->prepare(ws_.n());
+    }
+}
+
+void Simulation::set_preconditioner(unet::UNet* net) {
+    if (net && (ws_.n() % 16 != 0 || ws_.n() < 32))
+        fail(VAPOR_INVALID_ARGUMENT, "the coarse-grid network needs n divisible by 16 (n >= 32)");
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+    release_graphs();
+    if (coarse_ && coarse_ != net) coarse_->use_own_stream();
+    coarse_ = net;
+    if (coarse_) {
+        coarse_->set_stream(ws_.stream());
+        coarse_->prepare(ws_.n() / 4);
     }
 }
 
@@ -613,10 +750,15 @@ void Simulation::advance(float dt) {
             release_graphs();
             noise_.allocate(need);
         }
-        if (params.solver_kind == VAPOR_SOLVER_MIXED_REFINEMENT) ws_.ensure_mixed();
+        if (params.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR) ws_.ensure_mixed();
         if (warm_) {
             warm_->set_stream(ws_.stream());
             warm_->prepare(ws_.n());
+        }
+        if (params.solver_kind == VAPOR_SOLVER_FPCG) ws_.ensure_fpcg(coarse_ != nullptr);
+        if (coarse_) {
+            coarse_->set_stream(ws_.stream());
+            coarse_->prepare(ws_.n() / 4);
         }
     }
     cudaStream_t s = ws_.stream();
@@ -633,6 +775,8 @@ void Simulation::advance(float dt) {
     key.params = params;
     key.warm = warm_;
     key.warm_buffers = warm_ ? warm_->generation() : 0ull;
+    key.coarse = coarse_;
+    key.coarse_buffers = coarse_ ? coarse_->generation() : 0ull;
     if (!slot.exec || std::memcmp(&slot.key, &key, sizeof(GraphKey)) != 0) {
         if (slot.exec) {
             cudaGraphExecDestroy(slot.exec);
@@ -739,10 +883,22 @@ void Stage::project(float* u, float* v, float* w, const vapor_projection_options
     const cudaMemcpyKind out_kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     for (int c = 0; c < 3; ++c) VB_CUDA(cudaMemcpyAsync(in_[c].p, user[c], bytes, in_kind, s));
     ws_.clear_errors();
-    if (solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
+    if (solver_kind != VAPOR_SOLVER_RED_BLACK_SOR && solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT &&
+        solver_kind != VAPOR_SOLVER_FPCG)
         fail(VAPOR_INVALID_ARGUMENT, "Unknown solver kind");
-    ws_.project(in_[0].p, in_[1].p, in_[2].p, out_[0].p, out_[1].p, out_[2].p, nullptr, nullptr, nullptr, o.dt,
-                o.relaxation, floor_diag, o.linear_solve, solver_kind);
+    unet::UNet* net = solver_kind == VAPOR_SOLVER_FPCG ? coarse : nullptr;
+    if (net) {
+        if (g.n % 16 != 0 || g.n < 32)
+            fail(VAPOR_INVALID_ARGUMENT, "the coarse-grid network needs n divisible by 16 (n >= 32)");
+        net->set_stream(s);
+    }
+    try {
+        ws_.project(in_[0].p, in_[1].p, in_[2].p, out_[0].p, out_[1].p, out_[2].p, nullptr, nullptr, nullptr, o.dt,
+                    o.relaxation, floor_diag, o.linear_solve, solver_kind, nullptr, net);
+    } catch (...) {
+        if (net) net->use_own_stream();
+        throw;
+    }
     const vapor_projection_result r = ws_.last_result();  // waits; raises on non-finite input
     for (int c = 0; c < 3; ++c) VB_CUDA(cudaMemcpyAsync(user[c], out_[c].p, bytes, out_kind, s));
     if (pressure_out) {
@@ -756,6 +912,7 @@ void Stage::project(float* u, float* v, float* w, const vapor_projection_options
             VB_CUDA(cudaMemcpyAsync(pressure_out, natural, cells * sizeof(float), cudaMemcpyDeviceToHost, s));
     }
     VB_CUDA(cudaStreamSynchronize(s));
+    if (net) net->use_own_stream();
     if (result) *result = r;
 }
 

@@ -81,6 +81,10 @@ private:
     vapor_phase_timings acc_{};
 };
 
+// Red-black Gauss-Seidel sweeps before (and, in reverse colour order, after)
+// the coarse correction in the FPCG preconditioner.
+constexpr int kFpcgSmoothing = 2;
+
 // Validation shared by every entry point (MacGridDomain3D.cpp:7-22).
 void validate_grid(int n, float box);
 
@@ -105,7 +109,7 @@ public:
     void project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo, float* uh,
                  float* vh, float* wh, float dt, float omega, float diagonal_floor,
                  const vapor_linear_solve_options& options, int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR,
-                 unet::UNet* warm_start = nullptr);
+                 unet::UNet* warm_start = nullptr, unet::UNet* coarse = nullptr);
     float* rhs() { return b_.p; }
     void advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
                 const float* w, float* out, float post_scale);
@@ -122,18 +126,26 @@ public:
     long long total_iterations();
     PhaseTimer& timer() { return timer_; }
     void ensure_mixed();
+    void ensure_fpcg(bool coarse);
     // While true, project() records CUDA-graph nodes (the solve loops become
     // conditional while nodes) instead of driving the loop from the host.
     void set_capturing(bool on) { capturing_ = on; }
 
 private:
+    void project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UNet* coarse, LoopCond cond,
+                      cudaGraphConditionalHandle handle);
+
     int n_;
     float box_;
     cudaStream_t stream_;
     DevArray<float> b_, p_, fwd_;
     DevArray<double> partials_;
     DevArray<double> x64_[2];           // mixed-precision pressure (ping-pong)
-    DevArray<float> r32_;               // mixed-precision inner right-hand side
+    DevArray<float> r32_;               // mixed-precision inner right-hand side (FPCG: the residual)
+    DevArray<float> cg_p_, cg_q_, cg_z_;  // FPCG direction, A p, preconditioned residual
+    DevArray<float> cg_rc_;             // FPCG coarse right-hand side ((n/4)^3, natural layout)
+    DevArray<double> cg_partials_;
+    CgControl* cg_ = nullptr;           // device
     int partial_capacity_ = 0;
     ProjControl* ctrl_ = nullptr;       // device
     ProjControl* ctrl_host_ = nullptr;  // pinned mirror
@@ -184,6 +196,10 @@ public:
     // reference's x = 0). The network is bound to this simulation's stream.
     void set_warm_start(unet::UNet* net);
     unet::UNet* warm_start() const { return warm_; }
+    // Learned coarse-grid correction of the FPCG solver (VAPOR_SOLVER_FPCG;
+    // null: smoothing-only preconditioner). Needs n divisible by 16.
+    void set_preconditioner(unet::UNet* net);
+    unet::UNet* preconditioner() const { return coarse_; }
     Workspace& workspace() { return ws_; }
 
 private:
@@ -200,6 +216,8 @@ private:
         vapor_mac3d_params params;
         const void* warm;                 // warm-start network, if any
         unsigned long long warm_buffers;  // its buffer generation (reallocation re-records)
+        const void* coarse;               // coarse-grid network of the FPCG solver, if any
+        unsigned long long coarse_buffers;
     };
     struct CachedGraph {
         GraphKey key{};
@@ -208,6 +226,7 @@ private:
     CachedGraph graphs_[2];
     bool use_graphs_ = true;
     unet::UNet* warm_ = nullptr;
+    unet::UNet* coarse_ = nullptr;
 
     Stream stream_;
     Workspace ws_;
@@ -229,12 +248,14 @@ public:
 
     void reset();
     int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR;
+    unet::UNet* coarse = nullptr;  // FPCG coarse-grid network (bound to this stage's stream per call)
     void project(float* u, float* v, float* w, const vapor_projection_options& options, float diagonal_floor,
                  vapor_projection_result* result, float* pressure_out, bool device_pointers);
     void advect(int loc, float dt, float cfl, int method, const float* src, const float* fu, const float* fv,
                 const float* fw, float* out, bool device_pointers);
     cudaStream_t stream() const { return ws_.stream(); }
     int n() const { return ws_.n(); }
+    Workspace& workspace() { return ws_; }
 
 private:
     Stream stream_;

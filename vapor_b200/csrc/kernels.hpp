@@ -46,6 +46,16 @@ struct ProjControl {
     long long total_iterations;     // SOR iterations over finished projections
 };
 
+// Scalars of the flexible PCG solve (device).
+struct CgControl {
+    double rho;      // z.r of the current search direction
+    double alpha;    // step length rho / (p.Ap)
+    double beta;     // flexible (Polak-Ribiere) direction update
+    double pq;       // p.Ap
+    double gamma;    // scale of the coarse-grid correction (Galerkin)
+    double zc_mean;  // mean of the coarse correction, removed before use
+};
+
 // Simulation-wide reduction outputs (diagnostics).
 struct DiagControl {
     unsigned int max_velocity_bits;
@@ -174,6 +184,32 @@ void launch_gradient(const ProjectionArgs& a, const float* x, const float* u_in,
 void launch_unsplit_pressure(const Grid& g, const float* p, const ProjControl* ctrl, float* out, cudaStream_t s);
 // Assemble ctrl->result from the accumulators.
 void launch_finish_projection(ProjControl* ctrl, cudaStream_t s);
+
+// ---- flexible PCG (kernels_fpcg.cu) ----
+// Vectors are FP32 in the split layout (count = rb_count(n) slots, padding
+// zero). Partials need cg_partial_capacity() doubles.
+int cg_partial_capacity();
+// q = A p.
+void launch_apply_A(int n, const float* p, float* q, cudaStream_t s);
+// cg->rho = z.r (FP64).
+void launch_cg_rho(size_t count, const float* z, const float* r, double* partials, CgControl* cg, cudaStream_t s);
+// cg->alpha = rho / p.q.
+void launch_cg_alpha(size_t count, const float* p, const float* q, double* partials, CgControl* cg,
+                     cudaStream_t s);
+// e += alpha p; r -= alpha q; then count the iteration and decide the FP64
+// re-centring (ctrl->recentre, and the graph if-condition when active).
+void launch_cg_update(size_t count, float* e, float* r, const float* p, const float* q, const CgControl* cg,
+                      ProjControl* ctrl, LoopCond recentre_cond, cudaStream_t s);
+// beta = -alpha z.q / rho; rho = z.r.
+void launch_cg_beta(size_t count, const float* z, const float* r, const float* q, double* partials, CgControl* cg,
+                    cudaStream_t s);
+// p = z + beta p.
+void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s);
+// rc = 4^3 block sums of r - A z on the (n/4)^3 grid (natural layout); n % 4 == 0.
+void launch_restrict_residual(int n, const float* r, const float* z, float* rc, cudaStream_t s);
+// z += gamma (P zc - mean zc), gamma by the Galerkin condition on the coarse grid.
+void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
+                              cudaStream_t s);
 
 // ---- diagnostics ----
 void launch_diagnostics(const Grid& g, const float* u, const float* v, const float* w, double* partials,

@@ -165,6 +165,13 @@ void UNet::infer_into(int n, const float* b_split, const ProjControl* ctrl, floa
     VB_CUDA(cudaGetLastError());
 }
 
+const float* UNet::precondition(int n, const float* rhs) {
+    ensure(n);
+    launch_prep_natural(long(n) * n * n, rhs, partial_.p, scalars_.p, scale_.p, bf(in0_), s_);
+    forward(n);
+    return out_.p;
+}
+
 void UNet::forward_features(int n, const __nv_bfloat16* input16, float* out) {
     ensure(n);
     const long V1 = long(n) * n * n;

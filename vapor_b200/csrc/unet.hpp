@@ -53,6 +53,10 @@ void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
 void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,
                        __nv_bfloat16* out, cudaStream_t s);
+// Features from a natural-layout FP32 field: channel 0 = (a - mean) / rms.
+// Uses partial[0..1183], scalars[0].
+void launch_prep_natural(long V, const float* a, double* partial, double* scalars, float* scale,
+                         __nv_bfloat16* out, cudaStream_t s);
 void launch_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* in, int in_stride, __nv_bfloat16* out,
                      cudaStream_t s);
 void launch_upsample2(int d, int h, int w, int C, const __nv_bfloat16* in, __nv_bfloat16* out, int out_stride,
@@ -139,6 +143,11 @@ public:
     // Raw forward on device channels-last input [n^3][16] -> FP32 output.
     void forward_features(int n, const __nv_bfloat16* input16, float* out);
     void backward_from_output(int n, const float* grad_out);  // after forward_features
+    // Coarse-grid correction of the flexible PCG solve: the network applied
+    // to a natural-layout FP32 right-hand side on an n^3 grid; returns the
+    // FP32 output (natural layout, valid until the next call). Its scale is
+    // arbitrary: the caller scales it by the Galerkin condition.
+    const float* precondition(int n, const float* rhs);
     float* gradient() { return grad_.p; }
 
 private:

@@ -155,6 +155,32 @@ __global__ void k_prep_input(int n, const float* __restrict__ b_split, const Pro
     }
 }
 
+// Input features from a natural-layout FP32 field a (a coarse residual):
+// channel 0 = (a - mean a) / scale, channels 1..15 = 0.
+__global__ void k_prep_natural(long V, const float* __restrict__ a, const double* __restrict__ mean,
+                               const float* __restrict__ scale, __nv_bfloat16* __restrict__ out) {
+    const float inv = 1.f / fmaxf(*scale, 1e-30f);
+    const float m = float(*mean);
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        __nv_bfloat16* o = out + v * 16;
+        o[0] = __float2bfloat16_rn((a[v] - m) * inv);
+#pragma unroll
+        for (int c = 1; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+    }
+}
+__global__ void k_rms_natural(long V, const float* __restrict__ a, const double* __restrict__ mean,
+                              double* __restrict__ partial) {
+    __shared__ double s_sum[32];
+    const double m = *mean;
+    double acc = 0.0;
+    for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
+        const double d = double(a[v]) - m;
+        acc += d * d;
+    }
+    const double s = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 // Root-mean-square of the mean-free RHS (FP64), the normalization scale.
 __global__ void k_rms(int n, const float* __restrict__ b_split, const ProjControl* __restrict__ ctrl,
                       double* __restrict__ partial) {
@@ -607,6 +633,18 @@ void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, dou
     k_rms_finish<<<1, 1024, 0, s>>>(partial, blocks, double(V), scale);
     count_launch();
     k_prep_input<<<blocks_for(V), 256, 0, s>>>(n, b_split, ctrl, scale, out);
+}
+
+void launch_prep_natural(long V, const float* a, double* partial, double* scalars, float* scale,
+                         __nv_bfloat16* out, cudaStream_t s) {
+    launch_mean(V, a, partial, scalars, s);
+    const int blocks = std::min(blocks_for(V), 1184);
+    count_launch();
+    k_rms_natural<<<blocks, 256, 0, s>>>(V, a, scalars, partial);
+    count_launch();
+    k_rms_finish<<<1, 1024, 0, s>>>(partial, blocks, double(V), scale);
+    count_launch();
+    k_prep_natural<<<blocks_for(V), 256, 0, s>>>(V, a, scalars, scale, out);
 }
 
 void launch_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* in, int in_stride, __nv_bfloat16* out,

@@ -10,6 +10,15 @@ tolerance, so the plain solver remains both the fallback and the judge.
 
   python -m vapor_b200.learned train --out weights.npy [--n 128 --rollouts 8 --steps 100]
   python -m vapor_b200.learned compare --weights weights.npy [--n 256 --steps 4]
+  python -m vapor_b200.learned train-coarse --out coarse.npy [--n 64 --rollouts 8 --steps 60]
+  python -m vapor_b200.learned compare-fpcg --weights coarse.npy [--n 256 --steps 3]
+
+The same network also serves as the coarse-grid correction of the flexible
+PCG solver (VAPOR_SOLVER_FPCG): applied on the grid coarsened 4x per axis to
+the restricted residual, scaled by the Galerkin condition, prolonged and
+smoothed. For that role it is trained at the coarse resolution (64^3 for a
+256^3 solve) on plume projections and on projections of seeded random
+velocity fields with a k^-5/3 spectrum.
 """
 import argparse
 import ctypes as C
@@ -20,10 +29,12 @@ import time
 
 import numpy as np
 
-from . import MacSimulation3D, check, default_params, library
-from .plume import DT, scene_params, swirl_fields, training_scene
+from . import MacSimulation3D, StageBackend, check, default_params, library
+from .abi import SOLVER_FPCG, SOLVER_MIXED_REFINEMENT, LinearSolveOptions, ProjectionOptions
+from .plume import DT, omega_for, scene_params, spectral_fields, swirl_fields, training_scene
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warm_start_unet.npy")
+COARSE_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "coarse_unet.npy")
 
 
 class WarmStartNet:
@@ -142,6 +153,87 @@ def compare(net, n=128, warmup=10, steps=4, seed=12345, scene=None, rel=1e-6):
     return out
 
 
+def train_coarse(net, n=64, rollouts=8, steps=60, random_pairs=1, lr=1e-3, lr_final=1e-4, seed=0, skip=2,
+                 log=None):
+    """Trains the coarse-grid network at resolution n: each plume step's last
+    projection, plus `random_pairs` projections of seeded spectral velocity
+    fields per step (a stage with the mixed solver to relative 1e-6)."""
+    total = rollouts * max(0, steps - skip) * (1 + random_pairs)
+    stage = StageBackend(n, 1.0)
+    stage.set_solver_kind(SOLVER_MIXED_REFINEMENT)
+    opts = ProjectionOptions(DT, omega_for(n), LinearSolveOptions.defaults(
+        max_iterations=20000, relative_tolerance=1e-6, absolute_tolerance=0.0))
+    history, k = [], 0
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed + 99991)
+    for r in range(rollouts):
+        sim = make_scene(n, seed * 7919 + r)
+        for s in range(steps):
+            sim.advance(DT)
+            if s < skip:
+                continue
+            history.append(sim.train_warm_start(net, _lr(k, total, lr, lr_final)))
+            k += 1
+            for _ in range(random_pairs):
+                slope = float(rng.uniform(-3.0, -1.0))
+                u, v, w = spectral_fields(n, int(rng.integers(1 << 31)), slope=slope,
+                                          gradient_fraction=float(rng.uniform(0.2, 1.0)))
+                stage.project(u, v, w, opts, 6.0)
+                history.append(stage.train_network(net, _lr(k, total, lr, lr_final)))
+                k += 1
+            if log and (s % 10 == 0 or s == steps - 1):
+                log(json.dumps({"rollout": r, "step": s, "loss": float(np.mean(history[-(1 + random_pairs):])),
+                                "pairs": len(history), "elapsed_s": round(time.perf_counter() - t0, 1)}))
+        sim.close()
+    stage.close()
+    return history
+
+
+def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6):
+    """Per-step sweeps/iterations and device time on the benchmark plume for
+    the plain mixed-precision red-black SOR, FPCG with the smoothing-only
+    preconditioner, and FPCG with the learned coarse-grid correction."""
+    import torch
+    out = {}
+    for name, kind, use in (("sor", SOLVER_MIXED_REFINEMENT, False), ("fpcg", SOLVER_FPCG, False),
+                            ("fpcg_learned", SOLVER_FPCG, True)):
+        p = scene_params(default_params(), n, rel=rel, max_iterations=20000)
+        p.solver_kind = kind
+        sim = MacSimulation3D(n, 1.0, p)
+        sim.upload(*swirl_fields(n, seed))
+        if use:
+            sim.set_preconditioner(net)
+        for _ in range(warmup):
+            sim.advance(DT)
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        it0 = sim.total_iterations()
+        e0.record(stream)
+        for _ in range(steps):
+            sim.advance(DT)
+        e1.record(stream)
+        e1.synchronize()
+        r = sim.last_projection().linear_solve
+        its = (sim.total_iterations() - it0) / steps
+        out[name] = {"iterations_per_step": its, "ms_per_step": e0.elapsed_time(e1) / steps,
+                     "final_relative_residual": r.final_residual / max(r.initial_residual, 1e-300),
+                     "converged": bool(r.converged)}
+        if kind == SOLVER_FPCG:
+            # each CG step applies the preconditioner once (4 colour-pair sweeps),
+            # plus one application per projection before the loop (2 per step)
+            out[name]["sweeps_per_step"] = 4 * (its + 2)
+        else:
+            out[name]["sweeps_per_step"] = its
+        sim.close()
+    base = out["sor"]
+    for name in ("fpcg", "fpcg_learned"):
+        out[name]["sweep_ratio_vs_sor"] = base["sweeps_per_step"] / max(1e-9, out[name]["sweeps_per_step"])
+        out[name]["speedup_vs_sor"] = base["ms_per_step"] / max(1e-9, out[name]["ms_per_step"])
+    out["learned_gain_vs_fpcg"] = out["fpcg"]["ms_per_step"] / max(1e-9, out["fpcg_learned"]["ms_per_step"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -155,6 +247,21 @@ def main():
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--lr-final", type=float, default=1e-4)
     t.add_argument("--seed", type=int, default=0)
+    tc = sub.add_parser("train-coarse")
+    tc.add_argument("--out", default=COARSE_WEIGHTS)
+    tc.add_argument("--init", default=None)
+    tc.add_argument("--n", type=int, default=64)
+    tc.add_argument("--rollouts", type=int, default=8)
+    tc.add_argument("--steps", type=int, default=60)
+    tc.add_argument("--random-pairs", type=int, default=1)
+    tc.add_argument("--lr", type=float, default=1e-3)
+    tc.add_argument("--lr-final", type=float, default=1e-4)
+    tc.add_argument("--seed", type=int, default=0)
+    cf = sub.add_parser("compare-fpcg")
+    cf.add_argument("--weights", default=COARSE_WEIGHTS)
+    cf.add_argument("--n", type=int, default=256)
+    cf.add_argument("--warmup", type=int, default=4)
+    cf.add_argument("--steps", type=int, default=3)
     c = sub.add_parser("compare")
     c.add_argument("--weights", default=DEFAULT_WEIGHTS)
     c.add_argument("--n", type=int, default=128)
@@ -168,6 +275,16 @@ def main():
         net.save(args.out)
         tail = hist[-50:] if hist else [float("nan")]
         print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(tail))}))
+    elif args.cmd == "train-coarse":
+        net = WarmStartNet.load(args.init) if args.init else WarmStartNet(seed=args.seed)
+        hist = train_coarse(net, n=args.n, rollouts=args.rollouts, steps=args.steps, random_pairs=args.random_pairs,
+                            lr=args.lr, lr_final=args.lr_final, seed=args.seed, log=print)
+        net.save(args.out)
+        tail = hist[-50:] if hist else [float("nan")]
+        print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(tail))}))
+    elif args.cmd == "compare-fpcg":
+        net = WarmStartNet.load(args.weights) if os.path.exists(args.weights) else WarmStartNet(seed=0)
+        print(json.dumps(compare_fpcg(net, n=args.n, warmup=args.warmup, steps=args.steps)))
     else:
         net = WarmStartNet.load(args.weights)
         print(json.dumps(compare(net, n=args.n, warmup=args.warmup, steps=args.steps)))

@@ -94,3 +94,34 @@ def swirl_fields(n, seed, amplitude=0.5, vortices=8, sigma=0.08):
     v[:, 0, :] = v[:, -1, :] = 0
     w[0] = w[-1] = 0
     return [np.zeros((n, n, n), np.float32), u, v, w]
+
+
+def spectral_fields(n, seed, slope=-5.0 / 3.0, amplitude=1.0, gradient_fraction=0.5):
+    """Seeded random velocity with energy spectrum ~ k^slope: a solenoidal
+    part plus a gradient part (weight `gradient_fraction`), on the MAC faces,
+    walls zeroed. Returns (u, v, w) in the MAC layout (z, y, x)."""
+    rng = np.random.default_rng(seed)
+    m = n + 1
+    k = np.fft.fftfreq(m) * m
+    kz, ky, kx = np.meshgrid(k, k, k, indexing="ij")
+    kk = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    kk[0, 0, 0] = 1.0
+    amp = kk ** ((slope - 2.0) / 2.0)
+    amp[0, 0, 0] = 0.0
+    comps = []
+    for _ in range(3):
+        noise = rng.standard_normal((m, m, m)) + 1j * rng.standard_normal((m, m, m))
+        comps.append(noise * amp)
+    # Helmholtz split in Fourier space: gradient part = k (k . a) / |k|^2
+    dot = (kx * comps[0] + ky * comps[1] + kz * comps[2]) / kk ** 2
+    grad = [kx * dot, ky * dot, kz * dot]
+    sol = [c - g for c, g in zip(comps, grad)]
+    fields = [np.real(np.fft.ifftn((1 - gradient_fraction) * s_ + gradient_fraction * g)) for s_, g in zip(sol, grad)]
+    scale = amplitude / max(1e-30, max(float(np.abs(f).max()) for f in fields))
+    u = (fields[0][:n, :n, :] * scale).astype(np.float32)
+    v = (fields[1][:n, :, :n] * scale).astype(np.float32)
+    w = (fields[2][:, :n, :n] * scale).astype(np.float32)
+    u[:, :, 0] = u[:, :, -1] = 0
+    v[:, 0, :] = v[:, -1, :] = 0
+    w[0] = w[-1] = 0
+    return u, v, w
