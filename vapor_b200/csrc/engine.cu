@@ -260,6 +260,7 @@ void Workspace::ensure_fpcg(bool coarse) {
             fail(VAPOR_INVALID_ARGUMENT, "the coarse-grid network needs n divisible by 16 (n >= 32)");
         const size_t nc = size_t(n_ / 4);
         if (cg_rc_.n != nc * nc * nc) cg_rc_.allocate(nc * nc * nc);
+        if (cg_rows_.n != size_t(n_) * n_ * nc) cg_rows_.allocate(size_t(n_) * n_ * nc);
     }
 }
 
@@ -294,7 +295,7 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
-            launch_restrict_residual(n_, r, cg_z_.p, cg_rc_.p, st);
+            launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
             coarse->set_stream(st);
             const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
             coarse->set_stream(s);

@@ -144,6 +144,7 @@ private:
     DevArray<float> r32_;               // mixed-precision inner right-hand side (FPCG: the residual)
     DevArray<float> cg_p_, cg_q_, cg_z_;  // FPCG direction, A p, preconditioned residual
     DevArray<float> cg_rc_;             // FPCG coarse right-hand side ((n/4)^3, natural layout)
+    DevArray<float> cg_rows_;           // FPCG restriction scratch (n^2 * n/4 row sums)
     DevArray<double> cg_partials_;
     CgControl* cg_ = nullptr;           // device
     int partial_capacity_ = 0;

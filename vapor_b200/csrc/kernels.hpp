@@ -206,7 +206,8 @@ void launch_cg_beta(size_t count, const float* z, const float* r, const float* q
 // p = z + beta p.
 void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s);
 // rc = 4^3 block sums of r - A z on the (n/4)^3 grid (natural layout); n % 4 == 0.
-void launch_restrict_residual(int n, const float* r, const float* z, float* rc, cudaStream_t s);
+// `rows` holds n^3 / 4 floats of scratch.
+void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s);
 // z += gamma (P zc - mean zc), gamma by the Galerkin condition on the coarse grid.
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
                               cudaStream_t s);

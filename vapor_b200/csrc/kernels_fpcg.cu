@@ -170,12 +170,40 @@ __global__ void k_cg_decide(ProjControl* ctrl, int use_if, cudaGraphConditionalH
     if (use_if) cudaGraphSetConditional(if_handle, recentre ? 1u : 0u);
 }
 
-// Coarse right-hand side: rc[C] = sum over the 4^3 fine cells of C of
-// r - A z (FP32, fixed order), natural layout of the (n/4)^3 grid.
-__global__ void __launch_bounds__(kThreads) k_restrict_residual(int n, const float* __restrict__ r,
-                                                                const float* __restrict__ zs,
-                                                                float* __restrict__ rc) {
+// Coarse right-hand side rc[C] = sum over the 4^3 fine cells of C of
+// r - A z, in two deterministic passes. Pass 1: one thread per run of 4
+// fine cells along x (row y, plane z) sums their residuals (FP32, x order)
+// into rows[(z * n + y) * nc + cx].
+__global__ void __launch_bounds__(kThreads) k_restrict_rows(int n, const float* __restrict__ r,
+                                                            const float* __restrict__ zs, float* __restrict__ rows) {
     const RBLayout L = rb_layout(n);
+    const int nc = n >> 2;
+    const long total = long(n) * n * nc;
+    for (long t = long(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const int cx = int(t % nc);
+        const long yz = t / nc;
+        const int y = int(yz % n), z = int(yz / n);
+        float acc = 0.f;
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+            const int x = 4 * cx + dx;
+            const size_t me = rb_index(L, x, y, z);
+            float ax = float(neighbours(n, x, y, z)) * zs[me];
+            if (x > 0) ax -= zs[rb_index(L, x - 1, y, z)];
+            if (x + 1 < n) ax -= zs[rb_index(L, x + 1, y, z)];
+            if (y > 0) ax -= zs[rb_index(L, x, y - 1, z)];
+            if (y + 1 < n) ax -= zs[rb_index(L, x, y + 1, z)];
+            if (z > 0) ax -= zs[rb_index(L, x, y, z - 1)];
+            if (z + 1 < n) ax -= zs[rb_index(L, x, y, z + 1)];
+            acc += r[me] - ax;
+        }
+        rows[t] = acc;
+    }
+}
+
+// Pass 2: rc[C] = sum of the 4 x 4 (y, z) row sums of C, fixed order.
+__global__ void __launch_bounds__(kThreads) k_restrict_blocks(int n, const float* __restrict__ rows,
+                                                              float* __restrict__ rc) {
     const int nc = n >> 2;
     const long cells = long(nc) * nc * nc;
     for (long c = long(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += long(gridDim.x) * blockDim.x) {
@@ -183,18 +211,7 @@ __global__ void __launch_bounds__(kThreads) k_restrict_residual(int n, const flo
         float acc = 0.f;
         for (int dz = 0; dz < 4; ++dz)
             for (int dy = 0; dy < 4; ++dy)
-                for (int dx = 0; dx < 4; ++dx) {
-                    const int x = 4 * cx + dx, y = 4 * cy + dy, z = 4 * cz + dz;
-                    const size_t me = rb_index(L, x, y, z);
-                    float ax = float(neighbours(n, x, y, z)) * zs[me];
-                    if (x > 0) ax -= zs[rb_index(L, x - 1, y, z)];
-                    if (x + 1 < n) ax -= zs[rb_index(L, x + 1, y, z)];
-                    if (y > 0) ax -= zs[rb_index(L, x, y - 1, z)];
-                    if (y + 1 < n) ax -= zs[rb_index(L, x, y + 1, z)];
-                    if (z > 0) ax -= zs[rb_index(L, x, y, z - 1)];
-                    if (z + 1 < n) ax -= zs[rb_index(L, x, y, z + 1)];
-                    acc += r[me] - ax;
-                }
+                acc += rows[(long(4 * cz + dz) * n + (4 * cy + dy)) * nc + cx];
         rc[c] = acc;
     }
 }
@@ -260,18 +277,24 @@ __global__ void k_coarse_finish(const double* __restrict__ partials, int blocks,
     }
 }
 
-// z += gamma (zc[C(cell)] - mean) over every fine cell (split layout).
+// z += gamma (zc[C(cell)] - mean) over every fine cell, walking the split
+// layout in storage order (coalesced); padding slots are left alone.
 __global__ void __launch_bounds__(kThreads) k_prolong_add(int n, float* __restrict__ zs, const float* __restrict__ zc,
                                                           const CgControl* __restrict__ cg) {
     const RBLayout L = rb_layout(n);
     const int nc = n >> 2;
     const float g = float(cg->gamma), m = float(cg->zc_mean);
-    const size_t cells = size_t(n) * n * n;
-    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
-        const int x = int(c % n), y = int((c / n) % n), z = int(c / (size_t(n) * n));
+    const size_t count = 2 * L.stride;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x) {
+        const int colour = int(i / L.stride);
+        const size_t rem = i - size_t(colour) * L.stride;
+        const int slot = int(rem % L.hw);
+        const size_t row = rem / L.hw;
+        const int y = int(row % n), z = int(row / n);
+        const int x = 2 * slot + ((y + z + colour) & 1);
+        if (x >= n) continue;
         const size_t coarse = (size_t(z >> 2) * nc + (y >> 2)) * nc + (x >> 2);
-        const size_t me = rb_index(L, x, y, z);
-        zs[me] = zs[me] + g * (zc[coarse] - m);
+        zs[i] = zs[i] + g * (zc[coarse] - m);
     }
 }
 
@@ -334,10 +357,12 @@ void launch_cg_direction(size_t count, float* p, const float* z, const CgControl
     k_p_update<<<blocks_for(count), kThreads, 0, s>>>(count, p, z, cg);
 }
 
-void launch_restrict_residual(int n, const float* r, const float* z, float* rc, cudaStream_t s) {
+void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s) {
     const int nc = n / 4;
     count_launch();
-    k_restrict_residual<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, r, z, rc);
+    k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
+    count_launch();
+    k_restrict_blocks<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, rows, rc);
 }
 
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
@@ -350,7 +375,7 @@ void launch_coarse_correction(int n, float* z, const float* zc, const float* rc,
     count_launch();
     k_coarse_finish<<<1, 1024, 0, s>>>(partials, blocks, double(cells), cg);
     count_launch();
-    k_prolong_add<<<blocks_for(size_t(n) * n * n), kThreads, 0, s>>>(n, z, zc, cg);
+    k_prolong_add<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, cg);
 }
 
 }  // namespace vb

@@ -4,7 +4,7 @@
 //
 // The 3x3x3 convolutions - forward, and backward with respect to the input
 // (a convolution with the spatially flipped, channel-transposed weights) - run
-// on the tensor cores through k_conv3_tc (tc_conv.cuh). Weight gradients,
+// on the tensor cores through k_conv3_tc (PTX helpers in tc_conv.cuh). Weight gradients,
 // pooling, upsampling, the 1x1 output head, the loss and Adam are memory-bound
 // or small and run on CUDA cores.
 #include <cuda_bf16.h>
@@ -33,105 +33,153 @@ struct TmemColumns {
     static constexpr int value = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
 };
 
-// Implicit-GEMM 3x3x3 convolution on tcgen05 (see tc_conv.cuh for the layout).
+// Implicit-GEMM 3x3x3 convolution on tcgen05 with a halo tile in shared
+// memory. A CTA computes M = 128 voxels: 8 consecutive x by 16 consecutive y
+// in one z plane (row m = 8 * yi + xi, TMEM lane m). For each 16-channel
+// chunk of the input it stages
+//   A: the halo (x0-1 .. x0+8, y0-1 .. y0+16, z-1 .. z+1) as three copies
+//      shifted by dx = -1, 0, +1, each row of 8 x-voxels one 256-byte pair of
+//      core matrices (canonical K-major, no swizzle: element (r, k) at
+//      (k/8)*128 + r*16 + (k%8)*2), rows ordered (dx, dz, y);
+//   B: the chunk's weights of all 27 taps, [tap][N/8][2][8][16 B];
+// then one thread issues the 27 MMAs (M=128, N, K=16) back to back: the A
+// operand of tap (dz, dy, dx) starts at row (dx, dz, dy) of the halo and
+// steps 256 bytes per 8 rows (SBO), so no data moves per tap. Chunks are
+// double-buffered when two stages fit in shared memory. Out-of-range
+// neighbours are zero-filled (zero padding). Every wait is bounded; a timeout
+// sets the error flag and skips the epilogue.
 template <int N>
-__global__ void __launch_bounds__(128) k_conv3_tc(ConvArgs a) {
-    constexpr int kStage = 128 * 32 + N * 32;  // A then B, bytes
-    extern __shared__ __align__(1024) uint8_t smem[];
+struct ConvTile {
+    static constexpr int kHaloRows = 3 * 3 * 18;          // (dx, dz, y) rows of 8 voxels
+    static constexpr int kA = kHaloRows * 256;             // bytes
+    static constexpr int kB = 27 * N * 32;                 // bytes
+    static constexpr int kStage = kA + kB;
+    static constexpr int kStages = (2 * kStage <= 200 * 1024) ? 2 : 1;
+    static constexpr int kSmem = kStages * kStage + 1024;  // + alignment slack
+    static constexpr uint32_t kCols = TmemColumns<N>::value;
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
+    using T = ConvTile<N>;
+    extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const long V = long(a.D) * a.H * a.W;
-    const long v = long(blockIdx.x) * 128 + tid;
-    const bool vin = v < V;
-    int x = 0, y = 0, z = 0;
-    if (vin) decode(v, a.H, a.W, x, y, z);
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16, z = blockIdx.z;
 
-    constexpr uint32_t kCols = TmemColumns<N>::value;
-    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), kCols);
-    const uint32_t bar0 = tc::smem_addr(&bars[0]), bar1 = tc::smem_addr(&bars[1]);
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
+    const uint32_t bar_addr[2] = {tc::smem_addr(&bars[0]), tc::smem_addr(&bars[1])};
     if (tid == 0) {
-        tc::mbar_init(bar0, 1);
-        tc::mbar_init(bar1, 1);
+        tc::mbar_init(bar_addr[0], 1);
+        tc::mbar_init(bar_addr[1], 1);
         tc::fence_mbarrier_init();
     }
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = tmem_slot;
-
-    const int chunks = a.cin / 16;
-    const int steps = 27 * chunks;
     constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
     const uint32_t sbase = tc::smem_addr(smem);
-    const uint32_t arow = uint32_t((tid >> 3) * 256 + (tid & 7) * 16);
+    const int chunks = a.cin / 16;
     bool ok = true;
-    for (int s = 0; s < steps; ++s) {
-        const int st = s & 1;
-        const uint32_t bar = st ? bar1 : bar0;
-        if (s >= 2) {
-            const bool mine = tc::mbar_wait(bar, uint32_t((s - 2) >> 1) & 1u, kWaitLimit);
+    int issued[2] = {0, 0};  // commits per stage (phase tracking)
+
+    for (int cc = 0; cc < chunks; ++cc) {
+        const int st = T::kStages == 2 ? (cc & 1) : 0;
+        const uint32_t abase = sbase + uint32_t(st * T::kStage);
+        const uint32_t bbase = abase + T::kA;
+        // the stage's previous MMAs must be done before it is overwritten
+        if (issued[st] > 0) {
+            const bool mine = tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
             if (!__syncthreads_and(mine)) {
                 ok = false;
                 break;
             }
         }
-        const int tap = s / chunks, cc = s - tap * chunks;
-        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        const int xs = x + dx, ys = y + dy, zs = z + dz;
-        const bool valid = vin && xs >= 0 && xs < a.W && ys >= 0 && ys < a.H && zs >= 0 && zs < a.D;
-        const __nv_bfloat16* src =
-            valid ? a.in + ((long(zs) * a.H + ys) * a.W + xs) * a.in_stride + cc * 16 : a.in;
-        const uint32_t abase = sbase + uint32_t(st * kStage);
-        const uint32_t bbase = abase + 128 * 32;
-        tc::cp_async16(abase + arow, src, valid);
-        tc::cp_async16(abase + arow + 128, src + 8, valid);
-        for (int i = tid; i < 2 * N; i += 128) {
-            const int co = i >> 1, kc = i & 1;
-            const __nv_bfloat16* wsrc = a.w + (long(tap) * N + co) * a.cin + cc * 16 + kc * 8;
-            tc::cp_async16(bbase + uint32_t((co >> 3) * 256 + kc * 128 + (co & 7) * 16), wsrc, true);
+        for (int i = tid; i < T::kHaloRows * 16; i += blockDim.x) {
+            const int half = i & 1, r = (i >> 1) & 7, row = i >> 4;  // row = (dx * 3 + dz) * 18 + ry
+            const int ry = row % 18, dz = (row / 18) % 3, dx = row / 54;
+            const int x = x0 + r + dx - 1, y = y0 + ry - 1, zz = z + dz - 1;
+            const bool valid = x >= 0 && x < a.W && y >= 0 && y < a.H && zz >= 0 && zz < a.D;
+            const __nv_bfloat16* src =
+                valid ? a.in + ((long(zz) * a.H + y) * a.W + x) * a.in_stride + cc * 16 + half * 8 : a.in;
+            tc::cp_async16(abase + uint32_t(row * 256 + half * 128 + r * 16), src, valid);
+        }
+        for (int i = tid; i < 27 * N * 2; i += blockDim.x) {
+            const int half = i & 1, co = (i >> 1) % N, t = (i >> 1) / N;
+            const __nv_bfloat16* wsrc = a.w + (long(t) * N + co) * a.cin + cc * 16 + half * 8;
+            tc::cp_async16(bbase + uint32_t(t * N * 32 + (co >> 3) * 256 + half * 128 + (co & 7) * 16), wsrc, true);
         }
         tc::cp_async_wait_all();
         tc::fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-            tc::mma_bf16(tmem, tc::smem_desc(abase, 128, 256), tc::smem_desc(bbase, 128, 256), idesc, s > 0);
-            tc::mma_commit(bar);
+#pragma unroll 1
+            for (int t = 0; t < 27; ++t) {
+                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                const uint32_t a_addr = abase + uint32_t(((dx * 3 + dz) * 18 + dy) * 256);
+                const uint32_t b_addr = bbase + uint32_t(t * N * 32);
+                tc::mma_bf16(tmem, tc::smem_desc(a_addr, 128, 256), tc::smem_desc(b_addr, 128, 256), idesc,
+                             cc > 0 || t > 0);
+            }
+            tc::mma_commit(bar_addr[st]);
         }
+        ++issued[st];
     }
-    if (ok && steps > 0) {
-        const int last = steps - 1;
-        const bool mine = tc::mbar_wait((last & 1) ? bar1 : bar0, uint32_t(last >> 1) & 1u, kWaitLimit);
+    if (ok) {
+        // the last commit covers every earlier MMA of this thread
+        const int last = chunks - 1;
+        const int st = T::kStages == 2 ? (last & 1) : 0;
+        const bool mine = tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
         ok = __syncthreads_and(mine);
     }
     tc::tc_fence_after();
     if (ok) {
-        const uint32_t lane_base = uint32_t(warp * 32) << 16;
+        if (warp < 4) {
+            const int m = warp * 32 + lane;
+            const int x = x0 + (m & 7), y = y0 + (m >> 3);
+            const bool vin = x < a.W && y < a.H;
+            const long v = (long(z) * a.H + y) * a.W + x;
+            const uint32_t lane_base = uint32_t(warp * 32) << 16;
 #pragma unroll
-        for (int c0 = 0; c0 < N; c0 += 16) {
-            float acc[16];
-            tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
-            if (vin) {
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float acc[16];
+                tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
+                if (vin) {
+                    float val[16];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    float val = acc[i] + (a.bias ? a.bias[c0 + i] : 0.f);
-                    if (a.relu) val = fmaxf(val, 0.f);
-                    const long o = v * a.out_stride + a.out_offset + c0 + i;
-                    if (a.out_fp32) static_cast<float*>(a.out)[o] = val;
-                    else static_cast<__nv_bfloat16*>(a.out)[o] = __float2bfloat16_rn(val);
+                    for (int i = 0; i < 16; ++i) {
+                        val[i] = acc[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                        if (a.relu) val[i] = fmaxf(val[i], 0.f);
+                    }
+                    const long o = v * a.out_stride + a.out_offset + c0;
+                    if (a.out_fp32) {
+                        float* dst = static_cast<float*>(a.out) + o;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) dst[i] = val[i];
+                    } else {
+                        __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(val[i]);
+                        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o);
+                        dst[0] = reinterpret_cast<const uint4*>(h)[0];
+                        dst[1] = reinterpret_cast<const uint4*>(h)[1];
+                    }
                 }
             }
         }
     } else {
-        // Drain: wait (bounded) for anything still in flight before freeing TMEM.
         if (tid == 0) atomicOr(a.error, 1u);
-        tc::mbar_wait(bar0, 0u, kWaitLimit);
-        tc::mbar_wait(bar1, 0u, kWaitLimit);
+        // drain: wait (bounded) for every commit still in flight
+        for (int st = 0; st < T::kStages; ++st)
+            if (issued[st] > 0) tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+    if (warp == 0) tc::tmem_dealloc(tmem, T::kCols);
 }
 
 // ---- CUDA-core kernels -------------------------------------------------------
@@ -572,26 +620,21 @@ __global__ void k_to_bf16(long count, const float* __restrict__ a, __nv_bfloat16
 
 int blocks_for(long count) { return int(std::max<long>(1, std::min<long>((count + 255) / 256, 148L * 16))); }
 
-// Dynamic shared memory per block: enough that at most 512 / columns blocks
-// share an SM, so tensor-memory allocation never waits on another block.
-template <int N>
-int conv_smem_bytes() {
-    constexpr int stage = 128 * 32 + N * 32;
-    constexpr int per_sm = 512 / TmemColumns<N>::value;
-    const int cap = (227 * 1024) / (per_sm + 1) + 1024;
-    return std::max(2 * stage, std::min(cap, 227 * 1024 - 1024));
-}
-
+// Shared memory of the halo and weight stages: at most two blocks fit on an
+// SM (N = 16), so tensor-memory allocation (at most 2 x 64 columns) never
+// waits on another block.
 template <int N>
 void configure_n() {
-    VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem_bytes<N>()));
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, ConvTile<N>::kSmem));
 }
 
 template <int N>
 void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
-    const long V = long(a.D) * a.H * a.W;
+    if (a.cin % 16 != 0 || a.in_stride % 8 != 0 || a.out_stride % 8 != 0 || a.out_offset % 8 != 0)
+        fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
+    const dim3 grid(unsigned((a.W + 7) / 8), unsigned((a.H + 15) / 16), unsigned(a.D));
     count_launch();
-    k_conv3_tc<N><<<unsigned((V + 127) / 128), 128, conv_smem_bytes<N>(), s>>>(a);
+    k_conv3_tc<N><<<grid, 256, ConvTile<N>::kSmem, s>>>(a);
 }
 
 }  // namespace

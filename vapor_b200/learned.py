@@ -189,7 +189,8 @@ def train_coarse(net, n=64, rollouts=8, steps=60, random_pairs=1, lr=1e-3, lr_fi
     return history
 
 
-def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6):
+def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6, phases=False,
+                 arms=("sor", "fpcg", "fpcg_learned")):
     """Per-step sweeps/iterations and device time on the benchmark plume for
     the plain mixed-precision red-black SOR, FPCG with the smoothing-only
     preconditioner, and FPCG with the learned coarse-grid correction."""
@@ -197,6 +198,8 @@ def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6):
     out = {}
     for name, kind, use in (("sor", SOLVER_MIXED_REFINEMENT, False), ("fpcg", SOLVER_FPCG, False),
                             ("fpcg_learned", SOLVER_FPCG, True)):
+        if name not in arms:
+            continue
         p = scene_params(default_params(), n, rel=rel, max_iterations=20000)
         p.solver_kind = kind
         sim = MacSimulation3D(n, 1.0, p)
@@ -219,6 +222,14 @@ def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6):
         out[name] = {"iterations_per_step": its, "ms_per_step": e0.elapsed_time(e1) / steps,
                      "final_relative_residual": r.final_residual / max(r.initial_residual, 1e-300),
                      "converged": bool(r.converged)}
+        if phases:
+            sim.set_timing(True)
+            sim.advance(DT)
+            sim.synchronize()
+            t = sim.timings()
+            out[name]["phases_ms"] = {k: round(v["ms"], 3) for k, v in t.items() if v["ms"] > 0}
+            out[name]["phase_launches"] = {k: v["launches"] for k, v in t.items() if v["launches"] > 0}
+            sim.set_timing(False)
         if kind == SOLVER_FPCG:
             # each CG step applies the preconditioner once (4 colour-pair sweeps),
             # plus one application per projection before the loop (2 per step)
@@ -226,11 +237,13 @@ def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6):
         else:
             out[name]["sweeps_per_step"] = its
         sim.close()
-    base = out["sor"]
-    for name in ("fpcg", "fpcg_learned"):
-        out[name]["sweep_ratio_vs_sor"] = base["sweeps_per_step"] / max(1e-9, out[name]["sweeps_per_step"])
-        out[name]["speedup_vs_sor"] = base["ms_per_step"] / max(1e-9, out[name]["ms_per_step"])
-    out["learned_gain_vs_fpcg"] = out["fpcg"]["ms_per_step"] / max(1e-9, out["fpcg_learned"]["ms_per_step"])
+    if "sor" in out:
+        for name in ("fpcg", "fpcg_learned"):
+            if name in out:
+                out[name]["sweep_ratio_vs_sor"] = out["sor"]["sweeps_per_step"] / max(1e-9, out[name]["sweeps_per_step"])
+                out[name]["speedup_vs_sor"] = out["sor"]["ms_per_step"] / max(1e-9, out[name]["ms_per_step"])
+    if "fpcg" in out and "fpcg_learned" in out:
+        out["learned_gain_vs_fpcg"] = out["fpcg"]["ms_per_step"] / max(1e-9, out["fpcg_learned"]["ms_per_step"])
     return out
 
 
@@ -262,6 +275,8 @@ def main():
     cf.add_argument("--n", type=int, default=256)
     cf.add_argument("--warmup", type=int, default=4)
     cf.add_argument("--steps", type=int, default=3)
+    cf.add_argument("--phases", action="store_true", help="add a per-phase breakdown of one eager step")
+    cf.add_argument("--arms", default="sor,fpcg,fpcg_learned")
     c = sub.add_parser("compare")
     c.add_argument("--weights", default=DEFAULT_WEIGHTS)
     c.add_argument("--n", type=int, default=128)
@@ -284,7 +299,8 @@ def main():
         print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(tail))}))
     elif args.cmd == "compare-fpcg":
         net = WarmStartNet.load(args.weights) if os.path.exists(args.weights) else WarmStartNet(seed=0)
-        print(json.dumps(compare_fpcg(net, n=args.n, warmup=args.warmup, steps=args.steps)))
+        print(json.dumps(compare_fpcg(net, n=args.n, warmup=args.warmup, steps=args.steps, phases=args.phases,
+                                      arms=tuple(args.arms.split(",")))))
     else:
         net = WarmStartNet.load(args.weights)
         print(json.dumps(compare(net, n=args.n, warmup=args.warmup, steps=args.steps)))
