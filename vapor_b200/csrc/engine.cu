@@ -316,9 +316,8 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     };
     auto iteration = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_KRYLOV);
-        launch_apply_A(n_, cg_p_.p, cg_q_.p, st);
-        launch_cg_alpha(count, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
-        t.end(VAPOR_PHASE_KRYLOV, 3);
+        launch_apply_A_alpha(n_, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
+        t.end(VAPOR_PHASE_KRYLOV, 2);
         t.begin(VAPOR_PHASE_RESIDUAL);
         if (graph) {
             const cudaGraphConditionalHandle ifh = new_condition(st);

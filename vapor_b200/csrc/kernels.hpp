@@ -196,6 +196,8 @@ void launch_cg_rho(size_t count, const float* z, const float* r, double* partial
 // cg->alpha = rho / p.q.
 void launch_cg_alpha(size_t count, const float* p, const float* q, double* partials, CgControl* cg,
                      cudaStream_t s);
+// q = A p and cg->alpha = rho / p.q in one pass over p (two launches).
+void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s);
 // e += alpha p; r -= alpha q; then count the iteration and decide the FP64
 // re-centring (ctrl->recentre, and the graph if-condition when active).
 void launch_cg_update(size_t count, float* e, float* r, const float* p, const float* q, const CgControl* cg,

@@ -61,6 +61,146 @@ __global__ void __launch_bounds__(kThreads) k_apply_A(int n, const float* __rest
     }
 }
 
+// Row-pair access (n % 8 == 0): thread t owns slots 4j..4j+3 of both colours
+// in row (y, z), i.e. the 8 cells x = 8j .. 8j+7; cell x = 8j + m has colour
+// (x + y + z) & 1 and slot 4j + (m >> 1). Loads are float4 per colour and
+// row, index arithmetic is 32-bit, and no thread divides 64-bit values.
+struct RowPair {
+    float v[2][4];  // [colour][slot - 4j]
+};
+__device__ __forceinline__ RowPair load_pair(const float* __restrict__ a, int stride, int off) {
+    RowPair p;
+    const float4 c0 = *reinterpret_cast<const float4*>(a + off);
+    const float4 c1 = *reinterpret_cast<const float4*>(a + stride + off);
+    p.v[0][0] = c0.x; p.v[0][1] = c0.y; p.v[0][2] = c0.z; p.v[0][3] = c0.w;
+    p.v[1][0] = c1.x; p.v[1][1] = c1.y; p.v[1][2] = c1.z; p.v[1][3] = c1.w;
+    return p;
+}
+__device__ __forceinline__ RowPair zero_pair() {
+    RowPair p;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p.v[c][k] = 0.f;
+    return p;
+}
+
+// (A a) at the 8 cells of a row pair, in the residual's operation order:
+// count * a, minus x-, x+, y-, y+, z-, z+ (missing neighbours skipped).
+__device__ __forceinline__ void apply_pair(const float* __restrict__ a, int n, int hw, int j, int y, int z,
+                                           float out[8]) {
+    const int plane = n * hw, stride = n * plane;
+    const int off = z * plane + y * hw + 4 * j;
+    const RowPair me = load_pair(a, stride, off);
+    const RowPair ym = y > 0 ? load_pair(a, stride, off - hw) : zero_pair();
+    const RowPair yp = y + 1 < n ? load_pair(a, stride, off + hw) : zero_pair();
+    const RowPair zm = z > 0 ? load_pair(a, stride, off - plane) : zero_pair();
+    const RowPair zp = z + 1 < n ? load_pair(a, stride, off + plane) : zero_pair();
+    const int x0 = 8 * j;
+    // x-neighbours outside the run: cell x0 - 1 (slot 4j - 1) and x0 + 8 (slot 4j + 4)
+    const float left = x0 > 0 ? a[((x0 - 1 + y + z) & 1) * stride + off - 1] : 0.f;
+    const float right = x0 + 8 < n ? a[((x0 + 8 + y + z) & 1) * stride + off + 4] : 0.f;
+    const int nyz = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int x = x0 + m;
+        const int c = (x + y + z) & 1, k = m >> 1;
+        const float v = me.v[c][k];
+        float ax = float((x > 0) + (x + 1 < n) + nyz) * v;
+        if (x > 0) ax -= m > 0 ? me.v[1 - c][(m - 1) >> 1] : left;
+        if (x + 1 < n) ax -= m < 7 ? me.v[1 - c][(m + 1) >> 1] : right;
+        if (y > 0) ax -= ym.v[1 - c][k];
+        if (y + 1 < n) ax -= yp.v[1 - c][k];
+        if (z > 0) ax -= zm.v[1 - c][k];
+        if (z + 1 < n) ax -= zp.v[1 - c][k];
+        out[m] = ax;
+    }
+}
+
+// q = A p with FP64 block partials of p.q (n % 8 == 0; grid-stride over row pairs).
+__global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __restrict__ ps, float* __restrict__ qs,
+                                                          double* __restrict__ partials) {
+    __shared__ double s_sum[32];
+    const int hw = n >> 1, groups = hw >> 2;
+    const int plane = n * hw, stride = n * plane;
+    const int total = groups * n * n;
+    double acc = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
+        float q[8];
+        apply_pair(ps, n, hw, j, y, z, q);
+        const int off = z * plane + y * hw + 4 * j;
+        float o[2][4];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int c = (8 * j + m + y + z) & 1;
+            o[c][m >> 1] = q[m];
+        }
+        const float4 p0 = *reinterpret_cast<const float4*>(ps + off);
+        const float4 p1 = *reinterpret_cast<const float4*>(ps + stride + off);
+        *reinterpret_cast<float4*>(qs + off) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
+        *reinterpret_cast<float4*>(qs + stride + off) = make_float4(o[1][0], o[1][1], o[1][2], o[1][3]);
+        acc += double(p0.x) * o[0][0] + double(p0.y) * o[0][1] + double(p0.z) * o[0][2] + double(p0.w) * o[0][3];
+        acc += double(p1.x) * o[1][0] + double(p1.y) * o[1][1] + double(p1.z) * o[1][2] + double(p1.w) * o[1][3];
+    }
+    const double b = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = b;
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// Restriction pass 1 on row pairs (n % 16 == 0): the residuals r - A z of the
+// 8 cells, summed per coarse block in x order, into rows[(z n + y) nc + cx].
+__global__ void __launch_bounds__(kThreads) k_restrict_pairs(int n, const float* __restrict__ r,
+                                                             const float* __restrict__ zs, float* __restrict__ rows) {
+    const int hw = n >> 1, groups = hw >> 2, nc = n >> 2;
+    const int plane = n * hw, stride = n * plane;
+    const int total = groups * n * n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
+        float az[8];
+        apply_pair(zs, n, hw, j, y, z, az);
+        const RowPair rr = load_pair(r, stride, z * plane + y * hw + 4 * j);
+        float sum[2] = {0.f, 0.f};
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int c = (8 * j + m + y + z) & 1;
+            sum[m >> 2] += rr.v[c][m >> 1] - az[m];
+        }
+        const int base = (z * n + y) * nc + 2 * j;
+        rows[base] = sum[0];
+        rows[base + 1] = sum[1];
+    }
+}
+
+// z += gamma (zc[C] - mean) on row pairs (n % 16 == 0).
+__global__ void __launch_bounds__(kThreads) k_prolong_pairs(int n, float* __restrict__ zs,
+                                                            const float* __restrict__ zc,
+                                                            const CgControl* __restrict__ cg) {
+    const int hw = n >> 1, groups = hw >> 2, nc = n >> 2;
+    const int plane = n * hw, stride = n * plane;
+    const int total = groups * n * n;
+    const float g = float(cg->gamma), mean = float(cg->zc_mean);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
+        const int cbase = ((z >> 2) * nc + (y >> 2)) * nc + 2 * j;
+        const float a = g * (zc[cbase] - mean), b = g * (zc[cbase + 1] - mean);
+        const int off = z * plane + y * hw + 4 * j;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            float4* p = reinterpret_cast<float4*>(zs + c * stride + off);
+            float4 v = *p;
+            // slots 4j, 4j+1 hold x in [8j, 8j+3] (coarse 2j); 4j+2, 4j+3 hold [8j+4, 8j+7]
+            v.x = v.x + a;
+            v.y = v.y + a;
+            v.z = v.z + b;
+            v.w = v.w + b;
+            *p = v;
+        }
+    }
+}
+
 // Per-block FP64 partials of sum a.b (and of c.d when c is given).
 __global__ void __launch_bounds__(kThreads) k_dot2(size_t count, const float* __restrict__ a,
                                                    const float* __restrict__ b, const float* __restrict__ c,
@@ -335,6 +475,19 @@ void launch_cg_alpha(size_t count, const float* p, const float* q, double* parti
     k_alpha_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
 }
 
+void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s) {
+    if (n % 8 != 0) {
+        launch_apply_A(n, p, q, s);
+        launch_cg_alpha(rb_count(n), p, q, partials, cg, s);
+        return;
+    }
+    const int blocks = blocks_for(size_t(n / 8) * n * n);
+    count_launch();
+    k_apply_A_dot<<<blocks, kThreads, 0, s>>>(n, p, q, partials);
+    count_launch();
+    k_alpha_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
+}
+
 void launch_cg_update(size_t count, float* e, float* r, const float* p, const float* q, const CgControl* cg,
                       ProjControl* ctrl, LoopCond recentre_cond, cudaStream_t s) {
     count_launch();
@@ -360,7 +513,8 @@ void launch_cg_direction(size_t count, float* p, const float* z, const CgControl
 void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s) {
     const int nc = n / 4;
     count_launch();
-    k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
+    if (n % 16 == 0) k_restrict_pairs<<<blocks_for(size_t(n / 8) * n * n), kThreads, 0, s>>>(n, r, z, rows);
+    else k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
     count_launch();
     k_restrict_blocks<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, rows, rc);
 }
@@ -375,7 +529,8 @@ void launch_coarse_correction(int n, float* z, const float* zc, const float* rc,
     count_launch();
     k_coarse_finish<<<1, 1024, 0, s>>>(partials, blocks, double(cells), cg);
     count_launch();
-    k_prolong_add<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, cg);
+    if (n % 16 == 0) k_prolong_pairs<<<blocks_for(size_t(n / 8) * n * n), kThreads, 0, s>>>(n, z, zc, cg);
+    else k_prolong_add<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, cg);
 }
 
 }  // namespace vb

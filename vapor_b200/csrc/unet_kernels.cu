@@ -37,26 +37,29 @@ struct TmemColumns {
 // memory. A CTA computes M = 128 voxels: 8 consecutive x by 16 consecutive y
 // in one z plane (row m = 8 * yi + xi, TMEM lane m). For each 16-channel
 // chunk of the input it stages
-//   A: the halo (x0-1 .. x0+8, y0-1 .. y0+16, z-1 .. z+1) as three copies
-//      shifted by dx = -1, 0, +1, each row of 8 x-voxels one 256-byte pair of
-//      core matrices (canonical K-major, no swizzle: element (r, k) at
-//      (k/8)*128 + r*16 + (k%8)*2), rows ordered (dx, dz, y);
+//   A: the halo x0-1 .. x0+8, y0-1 .. y0+16, z-1 .. z+1 once, as 54 rows
+//      (dz, y) of 320 bytes: the 10 voxels' channels 0-7 (16 bytes each),
+//      then their channels 8-15;
 //   B: the chunk's weights of all 27 taps, [tap][N/8][2][8][16 B];
-// then one thread issues the 27 MMAs (M=128, N, K=16) back to back: the A
-// operand of tap (dz, dy, dx) starts at row (dx, dz, dy) of the halo and
-// steps 256 bytes per 8 rows (SBO), so no data moves per tap. Chunks are
-// double-buffered when two stages fit in shared memory. Out-of-range
-// neighbours are zero-filled (zero padding). Every wait is bounded; a timeout
-// sets the error flag and skips the epilogue.
+// then one thread issues the 27 MMAs (M=128, N, K=16) back to back. The A
+// operand of tap (dz, dy, dx) is a view of the halo in the canonical K-major
+// layout without swizzle: its 8-row core matrices are the 8 voxels from
+// x0-1+dx (16-byte rows), the second K half sits 160 bytes further (LBO) and
+// the next 8 rows (next y) 320 bytes further (SBO); so no data moves per tap.
+// Chunks are double-buffered when there are several and two stages fit.
+// Out-of-range neighbours are zero-filled (zero padding). Every wait is
+// bounded; a timeout sets the error flag and skips the epilogue.
 template <int N>
 struct ConvTile {
-    static constexpr int kHaloRows = 3 * 3 * 18;          // (dx, dz, y) rows of 8 voxels
-    static constexpr int kA = kHaloRows * 256;             // bytes
+    static constexpr int kRows = 3 * 18;                   // (dz, y) halo rows
+    static constexpr int kRowBytes = 320;                  // 10 voxels x 2 K halves x 16 B
+    static constexpr int kA = kRows * kRowBytes;           // bytes
     static constexpr int kB = 27 * N * 32;                 // bytes
     static constexpr int kStage = kA + kB;
-    static constexpr int kStages = (2 * kStage <= 200 * 1024) ? 2 : 1;
-    static constexpr int kSmem = kStages * kStage + 1024;  // + alignment slack
+    static constexpr bool kTwoStages = 2 * kStage <= 200 * 1024;
+    static constexpr int kSmemMax = (kTwoStages ? 2 : 1) * kStage + 1024;  // + alignment slack
     static constexpr uint32_t kCols = TmemColumns<N>::value;
+    static int smem(int chunks) { return ((kTwoStages && chunks > 1) ? 2 : 1) * kStage + 1024; }
 };
 
 template <int N>
@@ -65,9 +68,12 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ float s_bias[N];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16, z = blockIdx.z;
+    const int chunks = a.cin / 16;
+    const int stages = (T::kTwoStages && chunks > 1) ? 2 : 1;
 
     if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
     const uint32_t bar_addr[2] = {tc::smem_addr(&bars[0]), tc::smem_addr(&bars[1])};
@@ -76,18 +82,18 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
         tc::mbar_init(bar_addr[1], 1);
         tc::fence_mbarrier_init();
     }
+    for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = tmem_slot;
     constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
     const uint32_t sbase = tc::smem_addr(smem);
-    const int chunks = a.cin / 16;
     bool ok = true;
     int issued[2] = {0, 0};  // commits per stage (phase tracking)
 
     for (int cc = 0; cc < chunks; ++cc) {
-        const int st = T::kStages == 2 ? (cc & 1) : 0;
+        const int st = stages == 2 ? (cc & 1) : 0;
         const uint32_t abase = sbase + uint32_t(st * T::kStage);
         const uint32_t bbase = abase + T::kA;
         // the stage's previous MMAs must be done before it is overwritten
@@ -98,14 +104,14 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
                 break;
             }
         }
-        for (int i = tid; i < T::kHaloRows * 16; i += blockDim.x) {
-            const int half = i & 1, r = (i >> 1) & 7, row = i >> 4;  // row = (dx * 3 + dz) * 18 + ry
-            const int ry = row % 18, dz = (row / 18) % 3, dx = row / 54;
-            const int x = x0 + r + dx - 1, y = y0 + ry - 1, zz = z + dz - 1;
+        for (int i = tid; i < T::kRows * 20; i += blockDim.x) {
+            const int half = i & 1, v = (i >> 1) % 10, row = (i >> 1) / 10;  // row = dz * 18 + ry
+            const int ry = row % 18, dz = row / 18;
+            const int x = x0 - 1 + v, y = y0 + ry - 1, zz = z + dz - 1;
             const bool valid = x >= 0 && x < a.W && y >= 0 && y < a.H && zz >= 0 && zz < a.D;
             const __nv_bfloat16* src =
                 valid ? a.in + ((long(zz) * a.H + y) * a.W + x) * a.in_stride + cc * 16 + half * 8 : a.in;
-            tc::cp_async16(abase + uint32_t(row * 256 + half * 128 + r * 16), src, valid);
+            tc::cp_async16(abase + uint32_t(row * T::kRowBytes + half * 160 + v * 16), src, valid);
         }
         for (int i = tid; i < 27 * N * 2; i += blockDim.x) {
             const int half = i & 1, co = (i >> 1) % N, t = (i >> 1) / N;
@@ -120,10 +126,10 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
 #pragma unroll 1
             for (int t = 0; t < 27; ++t) {
                 const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-                const uint32_t a_addr = abase + uint32_t(((dx * 3 + dz) * 18 + dy) * 256);
+                const uint32_t a_addr = abase + uint32_t((dz * 18 + dy) * T::kRowBytes + dx * 16);
                 const uint32_t b_addr = bbase + uint32_t(t * N * 32);
-                tc::mma_bf16(tmem, tc::smem_desc(a_addr, 128, 256), tc::smem_desc(b_addr, 128, 256), idesc,
-                             cc > 0 || t > 0);
+                tc::mma_bf16(tmem, tc::smem_desc(a_addr, 160, T::kRowBytes), tc::smem_desc(b_addr, 128, 256),
+                             idesc, cc > 0 || t > 0);
             }
             tc::mma_commit(bar_addr[st]);
         }
@@ -131,8 +137,7 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     }
     if (ok) {
         // the last commit covers every earlier MMA of this thread
-        const int last = chunks - 1;
-        const int st = T::kStages == 2 ? (last & 1) : 0;
+        const int st = stages == 2 ? ((chunks - 1) & 1) : 0;
         const bool mine = tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
         ok = __syncthreads_and(mine);
     }
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
                     float val[16];
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
-                        val[i] = acc[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                        val[i] = acc[i] + s_bias[c0 + i];
                         if (a.relu) val[i] = fmaxf(val[i], 0.f);
                     }
                     const long o = v * a.out_stride + a.out_offset + c0;
@@ -174,7 +179,7 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     } else {
         if (tid == 0) atomicOr(a.error, 1u);
         // drain: wait (bounded) for every commit still in flight
-        for (int st = 0; st < T::kStages; ++st)
+        for (int st = 0; st < stages; ++st)
             if (issued[st] > 0) tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
     }
     tc::tc_fence_before();
@@ -620,12 +625,13 @@ __global__ void k_to_bf16(long count, const float* __restrict__ a, __nv_bfloat16
 
 int blocks_for(long count) { return int(std::max<long>(1, std::min<long>((count + 255) / 256, 148L * 16))); }
 
-// Shared memory of the halo and weight stages: at most two blocks fit on an
-// SM (N = 16), so tensor-memory allocation (at most 2 x 64 columns) never
-// waits on another block.
+// Shared memory of the halo and weight stages bounds the blocks per SM (at
+// most 7, for N = 16 with one stage), so the tensor memory the blocks of one
+// launch allocate (at most 7 x 32, 3 x 64 or 2 x 128 columns) fits in 512.
 template <int N>
 void configure_n() {
-    VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, ConvTile<N>::kSmem));
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 ConvTile<N>::kSmemMax));
 }
 
 template <int N>
@@ -634,7 +640,7 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
         fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
     const dim3 grid(unsigned((a.W + 7) / 8), unsigned((a.H + 15) / 16), unsigned(a.D));
     count_launch();
-    k_conv3_tc<N><<<grid, 256, ConvTile<N>::kSmem, s>>>(a);
+    k_conv3_tc<N><<<grid, 256, ConvTile<N>::smem(a.cin / 16), s>>>(a);
 }
 
 }  // namespace

@@ -247,6 +247,28 @@ def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6, phases=Fals
     return out
 
 
+def bench_net(n=64, reps=20, seed=0):
+    """Times the raw network forward on an n^3 grid (16 BF16 input channels,
+    FP32 output; each call synchronizes). Returns ms per call and TFLOP/s of
+    the ten 3x3x3 convolutions."""
+    import torch
+    net = WarmStartNet(seed=seed)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.zeros((n ** 3, 16), dtype=torch.bfloat16, device="cuda")
+    x[:, 0] = torch.randn(n ** 3, generator=g, device="cuda").to(torch.bfloat16)
+    out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+    lib = library()
+    for _ in range(3):
+        check(lib.vapor_unet_forward_features(net.handle, n, x.data_ptr(), out.data_ptr()))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        check(lib.vapor_unet_forward_features(net.handle, n, x.data_ptr(), out.data_ptr()))
+    ms = (time.perf_counter() - t0) * 1e3 / reps
+    macs = 27 * n ** 3 * (16 * 16 * 2 + 48 * 16 + 16 * 16 + (16 * 32 + 32 * 32 + 96 * 32 + 32 * 32) / 8.0 +
+                          (32 * 64 + 64 * 64) / 64.0)
+    return {"n": n, "ms_per_forward": ms, "conv_tflops": 2 * macs / (ms * 1e-3) / 1e12}
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -277,6 +299,9 @@ def main():
     cf.add_argument("--steps", type=int, default=3)
     cf.add_argument("--phases", action="store_true", help="add a per-phase breakdown of one eager step")
     cf.add_argument("--arms", default="sor,fpcg,fpcg_learned")
+    bn = sub.add_parser("bench-net")
+    bn.add_argument("--n", type=int, default=64)
+    bn.add_argument("--reps", type=int, default=20)
     c = sub.add_parser("compare")
     c.add_argument("--weights", default=DEFAULT_WEIGHTS)
     c.add_argument("--n", type=int, default=128)
@@ -297,6 +322,8 @@ def main():
         net.save(args.out)
         tail = hist[-50:] if hist else [float("nan")]
         print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(tail))}))
+    elif args.cmd == "bench-net":
+        print(json.dumps(bench_net(n=args.n, reps=args.reps)))
     elif args.cmd == "compare-fpcg":
         net = WarmStartNet.load(args.weights) if os.path.exists(args.weights) else WarmStartNet(seed=0)
         print(json.dumps(compare_fpcg(net, n=args.n, warmup=args.warmup, steps=args.steps, phases=args.phases,
