@@ -6,9 +6,15 @@ Workload (synthetic, seeded): the Reflection + MacCormack plume of the
 min(1, 3 exp(-3.5 (d/r)^2)) of radius .08 at (x, y, z) = (.3, .5, .15) and
 (.7, .5, .15) (z up), buoyancy 1.5, smoke decay .995 per step, no kick or stir,
 initial velocity a seeded swirl of 8 Gaussian vortices (amplitude .5). Every
-projection solves to relative residual (= relative divergence) 1e-6 in FP64
-with the mixed-precision red-black SOR (FP32 sweeps, FP64 residual and
-pressure). Metric: steps/s (higher is better).
+projection solves to relative residual (= relative divergence) 1e-6, verified
+in FP64. Two arms run on the same scene:
+  learned (the headline value): flexible PCG whose preconditioner is red-black
+    Gauss-Seidel smoothing around the learned U-Net coarse-grid correction
+    (weights vapor_b200/weights/coarse_unet.npy);
+  plain: the reference's red-black SOR (FP32 sweeps with FP64 residual and
+    re-centring, since FP32 SOR alone stalls above 1e-6).
+Metric: steps/s (higher is better), with the plain arm, the sweep ratio and
+the kernels' roofline fractions beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -50,6 +56,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--weights", default=os.path.join(ROOT, "vapor_b200", "weights", "coarse_unet.npy"),
+                    help="coarse-grid U-Net parameters of the learned arm")
     return ap.parse_args()
 
 
@@ -186,6 +194,70 @@ def run_reference(args):
 REFERENCE_SWEEPS_PER_STEP = 6000
 
 
+def network_flops(nc):
+    """FLOPs of one U-Net forward on an nc^3 grid: the ten 3x3x3 convolutions
+    (27 taps x cin x cout multiply-adds per voxel of their level)."""
+    macs = 27 * nc ** 3 * (16 * 16 * 2 + 48 * 16 + 16 * 16 + (16 * 32 + 32 * 32 + 96 * 32 + 32 * 32) / 8.0 +
+                           (32 * 64 + 64 * 64) / 64.0)
+    return 2.0 * macs
+
+
+def run_arm(vb, torch, args, n, fields, kind, net, dist, clocks=None):
+    """Warm-up, then K timed steps (CUDA-graph replays) of one solver arm."""
+    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega_for(n, args.omega),
+                          interval=args.interval)
+    params.solver_kind = kind
+    sim = vb.MacSimulation3D(n, 1.0, params)
+    sim.upload(*fields)
+    if net is not None:
+        sim.set_preconditioner(net)
+    for _ in range(args.warmup):
+        sim.advance(DT)
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it0 = sim.total_iterations()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    wall0 = time.perf_counter()
+    start.record(stream)
+    for _ in range(args.steps):
+        sim.advance(DT)
+    end.record(stream)
+    end.synchronize()
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop() if clocks else None
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    r = sim.last_projection().linear_solve
+    return sim, stream, {"ms": ms, "iterations": (sim.total_iterations() - it0) / args.steps,
+                         "final_relative_residual": r.final_residual / max(r.initial_residual, 1e-300),
+                         "converged": bool(r.converged), "wall_s": wall, "clocks": clock_info}
+
+
+def eager_phases(vb, sim, steps):
+    """The same step on the eager path with per-phase CUDA events on the
+    simulation's stream; also counts this library's kernel launches."""
+    sim.set_timing(True)
+    launches0 = vb.kernel_launch_count()
+    it0 = sim.total_iterations()
+    for _ in range(steps):
+        sim.advance(DT)
+    sim.synchronize()
+    launches = (vb.kernel_launch_count() - launches0) / steps
+    phases = sim.timings()
+    its = (sim.total_iterations() - it0) / steps
+    sim.set_timing(False)
+    return phases, launches, its
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -197,6 +269,8 @@ def main():
 
     import torch
     import vapor_b200 as vb
+    from vapor_b200.abi import SOLVER_FPCG, SOLVER_MIXED_REFINEMENT
+    from vapor_b200.learned import COARSE_WEIGHTS, WarmStartNet
 
     dist = None
     if world > 1:
@@ -208,54 +282,20 @@ def main():
     torch.cuda.set_device(local)
 
     n = args.n
-    omega = omega_for(n, args.omega)
-    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega, interval=args.interval)
     fields = swirl_fields(n, args.seed + rank)
-    sim = vb.MacSimulation3D(n, 1.0, params)
-    sim.upload(*fields)
-    for _ in range(args.warmup):
-        sim.advance(DT)
-    sim.synchronize()
-    stream = torch.cuda.ExternalStream(sim.stream())
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    it0 = sim.total_iterations()
-    clocks = ClockSampler(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    # Timed region: every step is one CUDA-graph launch (solve loops are
-    # device-side while-nodes); the state is far larger than L2.
-    clocks.start()
-    wall0 = time.perf_counter()
-    start.record(stream)
-    for _ in range(args.steps):
-        sim.advance(DT)
-    end.record(stream)
-    end.synchronize()
-    wall = time.perf_counter() - wall0
-    clock_info = clocks.stop()
-    torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    sweeps = sim.total_iterations() - it0
-    result = sim.last_projection()
-    rel = result.linear_solve.final_residual / max(result.linear_solve.initial_residual, 1e-300)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    if not os.path.exists(args.weights):
+        raise SystemExit(f"learned coarse-grid weights not found: {args.weights}")
+    net = WarmStartNet.load(args.weights)
 
-    # Roofline region: the same steps on the eager path with per-phase CUDA
-    # events on the simulation's stream; counts this library's kernel launches.
-    sim.set_timing(True)
-    launches0 = vb.kernel_launch_count()
+    # Plain arm: the reference's red-black SOR (mixed precision to reach 1e-6).
+    plain_sim, _, plain = run_arm(vb, torch, args, n, fields, SOLVER_MIXED_REFINEMENT, None, dist)
+    plain_phases, _, _ = eager_phases(vb, plain_sim, 1)
+    plain_sim.close()
+    # Learned arm (headline): flexible PCG with the U-Net coarse-grid correction.
+    clocks = ClockSampler(local)
+    sim, stream, learned = run_arm(vb, torch, args, n, fields, SOLVER_FPCG, net, dist, clocks)
     roof_steps = max(1, min(args.steps, 2))
-    for _ in range(roof_steps):
-        sim.advance(DT)
-    sim.synchronize()
-    launches_per_step = (vb.kernel_launch_count() - launches0) / roof_steps
-    phases = sim.timings()
-    sim.set_timing(False)
+    phases, launches_per_step, eager_its = eager_phases(vb, sim, roof_steps)
     launches = int(round(launches_per_step * args.steps))
 
     # End to end through the public API: pinned host state in, step, state out.
@@ -283,36 +323,69 @@ def main():
 
     peak, peak_kind = measured_peaks()
     cells = n ** 3
-    sor = phases["sor"]
-    sor_launch_ms = sor["ms"] / max(1, sor["launches"])
-    # One red-black iteration reads p and b and writes p once: 12 B/cell; a
-    # colour launch is half an iteration.
-    sor_bytes = 6.0 * cells
-    achieved = sor_bytes / (sor_launch_ms * 1e-3) / 1e9
+
+    def sor_roofline(ph):
+        sor = ph["sor"]
+        launch_ms = sor["ms"] / max(1, sor["launches"])
+        # one colour launch reads its colour's p and b, the other colour's p,
+        # and writes its p: 6 B/cell compulsory (12 B/cell per iteration)
+        nbytes = 6.0 * cells
+        achieved = nbytes / (launch_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": "k_sor_rbz (red-black colour sweep)", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "bytes_per_launch": nbytes, "avg_launch_us": launch_ms * 1e3}
+
+    # Network (tensor cores): FLOPs of the coarse U-Net per application over
+    # the coarse phase's time per application (restriction, normalization,
+    # Galerkin scale and prolongation included, so this is a lower bound).
+    applications = eager_its + 2.0
+    coarse_ms = phases["coarse"]["ms"] / roof_steps / max(1.0, applications)
+    net_flops = network_flops(n // 4)
+    tflops = net_flops / (coarse_ms * 1e-3) / 1e12 if coarse_ms > 0 else 0.0
+    tpeak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops_sustained", 1400.0)) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1400.0
+
     line = {
-        "metric": METRIC, "value": world * args.steps / (ms * 1e-3), "unit": "steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"mac3d_reflection_maccormack_{n}", "n": n, "dt": DT, "solver": "plain GPU "
-                   "red-black SOR, FP32 sweeps + FP64 residual/pressure refinement", "omega": omega,
-                   "relative_tolerance": args.rel, "sweeps_per_step": sweeps / args.steps,
-                   "final_relative_residual": rel, "converged": bool(result.linear_solve.converged),
-                   "l2": "state (4 x 67 MB fields) and solver buffers exceed the 126 MB L2",
+        "metric": METRIC, "value": world * args.steps / (learned["ms"] * 1e-3), "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"mac3d_reflection_maccormack_{n}", "n": n, "dt": DT,
+                   "solver": "flexible PCG, FP32 vectors + FP64 dots/residual/re-centring; preconditioner 2+2 "
+                             "red-black Gauss-Seidel sweeps around the learned U-Net coarse-grid correction "
+                             f"on {n // 4}^3 (BF16 tcgen05 convolutions)",
+                   "weights": os.path.relpath(args.weights, ROOT), "relative_tolerance": args.rel,
+                   "cg_iterations_per_step": learned["iterations"],
+                   "sweeps_per_step": 4 * (learned["iterations"] + 2),
+                   "final_relative_residual": learned["final_relative_residual"],
+                   "converged": learned["converged"],
+                   "l2": "state (4 x 67 MB fields) and solver vectors exceed the 126 MB L2",
                    "parallelism": f"replicas{world}"},
+        "plain": {"solver": "red-black SOR (the reference's method), FP32 sweeps + FP64 residual/re-centring",
+                  "value": world * args.steps / (plain["ms"] * 1e-3), "unit": "steps/s",
+                  "ms_per_step": plain["ms"] / args.steps, "sweeps_per_step": plain["iterations"],
+                  "omega": omega_for(n, args.omega), "final_relative_residual": plain["final_relative_residual"],
+                  "converged": plain["converged"], "roofline": sor_roofline(plain_phases),
+                  "phases_ms_per_step": {k: v["ms"] for k, v in plain_phases.items() if v["ms"] > 0}},
+        "speedup_vs_plain": plain["ms"] / learned["ms"],
+        "sweep_ratio_vs_plain": plain["iterations"] / max(1e-9, 4 * (learned["iterations"] + 2)),
         "gpu_launches": launches,
         "gpu_launches_note": "kernels per step counted on the eager replay of the same step, times steps",
-        "roofline": {"bound": "hbm", "kernel": "k_sor_color", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "bytes_per_launch": sor_bytes, "avg_launch_us": sor_launch_ms * 1e3},
-        "phases_ms_per_step": {k: v["ms"] / roof_steps for k, v in phases.items()},
+        "roofline": sor_roofline(phases),
+        "roofline_tensor": {"bound": "tensor", "kernel": "coarse U-Net forward (k_conv3_tc, 10 convolutions)",
+                            "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
+                            "peak_kind": "measured sustained", "flops_per_application": net_flops,
+                            "ms_per_application": coarse_ms,
+                            "note": "time includes restriction, normalization, Galerkin scale and prolongation"},
+        "phases_ms_per_step": {k: v["ms"] / roof_steps for k, v in phases.items() if v["ms"] > 0},
         "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},
-        "clocks": clock_info, "wall_s": wall,
+        "clocks": learned["clocks"], "wall_s": learned["wall_s"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = reference_cpu_sample(n, sweeps / args.steps, args.seed)
+        line["cpu_baseline"] = reference_cpu_sample(n, plain["iterations"], args.seed)
     if rank == 0:
         print(json.dumps(line))
+    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
