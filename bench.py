@@ -38,6 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from vapor_b200.plume import DT, omega_for, scene_params, swirl_fields  # noqa: E402
+from vapor_b200.replicas import aggregate_steps_per_second, max_over_ranks, rank_info, scene_seed  # noqa: E402
 
 METRIC = "256^3 steps/s: learned-warm-start vs plain GPU solve at rel div 1e-6; HBM %"
 
@@ -231,11 +232,7 @@ def run_arm(vb, torch, args, n, fields, kind, net, dist, clocks=None):
     wall = time.perf_counter() - wall0
     clock_info = clocks.stop() if clocks else None
     torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), dist, "cuda")
     r = sim.last_projection().linear_solve
     return sim, stream, {"ms": ms, "iterations": (sim.total_iterations() - it0) / args.steps,
                          "final_relative_residual": r.final_residual / max(r.initial_residual, 1e-300),
@@ -260,9 +257,7 @@ def eager_phases(vb, sim, steps):
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_info()
     if args.impl == "reference":
         run_reference(args)
         return
@@ -270,7 +265,7 @@ def main():
     import torch
     import vapor_b200 as vb
     from vapor_b200.abi import SOLVER_FPCG, SOLVER_MIXED_REFINEMENT
-    from vapor_b200.learned import COARSE_WEIGHTS, WarmStartNet
+    from vapor_b200.learned import WarmStartNet
 
     dist = None
     if world > 1:
@@ -282,7 +277,7 @@ def main():
     torch.cuda.set_device(local)
 
     n = args.n
-    fields = swirl_fields(n, args.seed + rank)
+    fields = swirl_fields(n, scene_seed(args.seed, rank))
     if not os.path.exists(args.weights):
         raise SystemExit(f"learned coarse-grid weights not found: {args.weights}")
     net = WarmStartNet.load(args.weights)
@@ -315,11 +310,7 @@ def main():
         sim.download(out)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, "cuda")
 
     peak, peak_kind = measured_peaks()
     cells = n ** 3
@@ -346,7 +337,8 @@ def main():
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1400.0
 
     line = {
-        "metric": METRIC, "value": world * args.steps / (learned["ms"] * 1e-3), "unit": "steps/s", "n_gpus": world,
+        "metric": METRIC, "value": aggregate_steps_per_second(world, args.steps, learned["ms"]), "unit": "steps/s",
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": learned["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"mac3d_reflection_maccormack_{n}", "n": n, "dt": DT,
@@ -361,7 +353,7 @@ def main():
                    "l2": "state (4 x 67 MB fields) and solver vectors exceed the 126 MB L2",
                    "parallelism": f"replicas{world}"},
         "plain": {"solver": "red-black SOR (the reference's method), FP32 sweeps + FP64 residual/re-centring",
-                  "value": world * args.steps / (plain["ms"] * 1e-3), "unit": "steps/s",
+                  "value": aggregate_steps_per_second(world, args.steps, plain["ms"]), "unit": "steps/s",
                   "ms_per_step": plain["ms"] / args.steps, "sweeps_per_step": plain["iterations"],
                   "omega": omega_for(n, args.omega), "final_relative_residual": plain["final_relative_residual"],
                   "converged": plain["converged"], "roofline": sor_roofline(plain_phases),
