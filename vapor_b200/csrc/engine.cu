@@ -253,7 +253,7 @@ void Workspace::ensure_fpcg(bool coarse) {
             v->allocate(count);
             v->zero(stream_);
         }
-    if (cg_partials_.n < size_t(cg_partial_capacity())) cg_partials_.allocate(cg_partial_capacity());
+    if (cg_partials_.n < size_t(cg_partial_capacity(n_))) cg_partials_.allocate(cg_partial_capacity(n_));
     if (!cg_) VB_CUDA(cudaMalloc(&cg_, sizeof(CgControl)));
     if (coarse) {
         if (n_ % 16 != 0 || n_ < 32)

@@ -187,8 +187,8 @@ void launch_finish_projection(ProjControl* ctrl, cudaStream_t s);
 
 // ---- flexible PCG (kernels_fpcg.cu) ----
 // Vectors are FP32 in the split layout (count = rb_count(n) slots, padding
-// zero). Partials need cg_partial_capacity() doubles.
-int cg_partial_capacity();
+// zero). Partials need cg_partial_capacity(n) doubles.
+int cg_partial_capacity(int n);
 // q = A p.
 void launch_apply_A(int n, const float* p, float* q, cudaStream_t s);
 // cg->rho = z.r (FP64).

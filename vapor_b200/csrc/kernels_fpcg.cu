@@ -117,16 +117,17 @@ __device__ __forceinline__ void apply_pair(const float* __restrict__ a, int n, i
     }
 }
 
-// q = A p with FP64 block partials of p.q (n % 8 == 0; grid-stride over row pairs).
+// q = A p with FP64 block partials of p.q (n % 8 == 0). Grid (row-pair
+// groups of one plane / 256, n planes): no index division beyond one per thread.
 __global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __restrict__ ps, float* __restrict__ qs,
                                                           double* __restrict__ partials) {
     __shared__ double s_sum[32];
     const int hw = n >> 1, groups = hw >> 2;
     const int plane = n * hw, stride = n * plane;
-    const int total = groups * n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y, y = t / groups, j = t - y * groups;
     double acc = 0.0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
+    if (y < n) {
         float q[8];
         apply_pair(ps, n, hw, j, y, z, q);
         const int off = z * plane + y * hw + 4 * j;
@@ -145,59 +146,59 @@ __global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __
     }
     const double b = block_sum(acc, s_sum);
     if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = b;
-        partials[2 * blockIdx.x + 1] = 0.0;
+        const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+        partials[2 * blk] = b;
+        partials[2 * blk + 1] = 0.0;
     }
 }
 
 // Restriction pass 1 on row pairs (n % 16 == 0): the residuals r - A z of the
 // 8 cells, summed per coarse block in x order, into rows[(z n + y) nc + cx].
+// Grid as k_apply_A_dot.
 __global__ void __launch_bounds__(kThreads) k_restrict_pairs(int n, const float* __restrict__ r,
                                                              const float* __restrict__ zs, float* __restrict__ rows) {
     const int hw = n >> 1, groups = hw >> 2, nc = n >> 2;
     const int plane = n * hw, stride = n * plane;
-    const int total = groups * n * n;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
-        float az[8];
-        apply_pair(zs, n, hw, j, y, z, az);
-        const RowPair rr = load_pair(r, stride, z * plane + y * hw + 4 * j);
-        float sum[2] = {0.f, 0.f};
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y, y = t / groups, j = t - y * groups;
+    if (y >= n) return;
+    float az[8];
+    apply_pair(zs, n, hw, j, y, z, az);
+    const RowPair rr = load_pair(r, stride, z * plane + y * hw + 4 * j);
+    float sum[2] = {0.f, 0.f};
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int c = (8 * j + m + y + z) & 1;
-            sum[m >> 2] += rr.v[c][m >> 1] - az[m];
-        }
-        const int base = (z * n + y) * nc + 2 * j;
-        rows[base] = sum[0];
-        rows[base + 1] = sum[1];
+    for (int m = 0; m < 8; ++m) {
+        const int c = (8 * j + m + y + z) & 1;
+        sum[m >> 2] += rr.v[c][m >> 1] - az[m];
     }
+    const int base = (z * n + y) * nc + 2 * j;
+    rows[base] = sum[0];
+    rows[base + 1] = sum[1];
 }
 
-// z += gamma (zc[C] - mean) on row pairs (n % 16 == 0).
+// z += gamma (zc[C] - mean) on row pairs (n % 16 == 0); grid as k_apply_A_dot.
 __global__ void __launch_bounds__(kThreads) k_prolong_pairs(int n, float* __restrict__ zs,
                                                             const float* __restrict__ zc,
                                                             const CgControl* __restrict__ cg) {
     const int hw = n >> 1, groups = hw >> 2, nc = n >> 2;
     const int plane = n * hw, stride = n * plane;
-    const int total = groups * n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y, y = t / groups, j = t - y * groups;
+    if (y >= n) return;
     const float g = float(cg->gamma), mean = float(cg->zc_mean);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int j = t % groups, yz = t / groups, y = yz % n, z = yz / n;
-        const int cbase = ((z >> 2) * nc + (y >> 2)) * nc + 2 * j;
-        const float a = g * (zc[cbase] - mean), b = g * (zc[cbase + 1] - mean);
-        const int off = z * plane + y * hw + 4 * j;
+    const int cbase = ((z >> 2) * nc + (y >> 2)) * nc + 2 * j;
+    const float a = g * (zc[cbase] - mean), b = g * (zc[cbase + 1] - mean);
+    const int off = z * plane + y * hw + 4 * j;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            float4* p = reinterpret_cast<float4*>(zs + c * stride + off);
-            float4 v = *p;
-            // slots 4j, 4j+1 hold x in [8j, 8j+3] (coarse 2j); 4j+2, 4j+3 hold [8j+4, 8j+7]
-            v.x = v.x + a;
-            v.y = v.y + a;
-            v.z = v.z + b;
-            v.w = v.w + b;
-            *p = v;
-        }
+    for (int c = 0; c < 2; ++c) {
+        float4* p = reinterpret_cast<float4*>(zs + c * stride + off);
+        float4 v = *p;
+        // slots 4j, 4j+1 hold x in [8j, 8j+3] (coarse 2j); 4j+2, 4j+3 hold [8j+4, 8j+7]
+        v.x = v.x + a;
+        v.y = v.y + a;
+        v.z = v.z + b;
+        v.w = v.w + b;
+        *p = v;
     }
 }
 
@@ -444,7 +445,15 @@ int blocks_for(size_t count) {
 
 }  // namespace
 
-int cg_partial_capacity() { return 4 * kDotBlocks; }
+static dim3 pair_grid(int n) {
+    const int groups = n / 8;
+    return dim3(unsigned((groups * n + kThreads - 1) / kThreads), unsigned(n));
+}
+
+int cg_partial_capacity(int n) {
+    const dim3 g = pair_grid(n);
+    return std::max(4 * kDotBlocks, int(2 * g.x * g.y));
+}
 
 void launch_apply_A(int n, const float* p, float* q, cudaStream_t s) {
     const RBLayout L = rb_layout(n);
@@ -481,11 +490,11 @@ void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgC
         launch_cg_alpha(rb_count(n), p, q, partials, cg, s);
         return;
     }
-    const int blocks = blocks_for(size_t(n / 8) * n * n);
+    const dim3 grid = pair_grid(n);
     count_launch();
-    k_apply_A_dot<<<blocks, kThreads, 0, s>>>(n, p, q, partials);
+    k_apply_A_dot<<<grid, kThreads, 0, s>>>(n, p, q, partials);
     count_launch();
-    k_alpha_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
+    k_alpha_finish<<<1, 1024, 0, s>>>(partials, int(grid.x * grid.y), cg);
 }
 
 void launch_cg_update(size_t count, float* e, float* r, const float* p, const float* q, const CgControl* cg,
@@ -513,7 +522,7 @@ void launch_cg_direction(size_t count, float* p, const float* z, const CgControl
 void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s) {
     const int nc = n / 4;
     count_launch();
-    if (n % 16 == 0) k_restrict_pairs<<<blocks_for(size_t(n / 8) * n * n), kThreads, 0, s>>>(n, r, z, rows);
+    if (n % 16 == 0) k_restrict_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, r, z, rows);
     else k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
     count_launch();
     k_restrict_blocks<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, rows, rc);
@@ -529,7 +538,7 @@ void launch_coarse_correction(int n, float* z, const float* zc, const float* rc,
     count_launch();
     k_coarse_finish<<<1, 1024, 0, s>>>(partials, blocks, double(cells), cg);
     count_launch();
-    if (n % 16 == 0) k_prolong_pairs<<<blocks_for(size_t(n / 8) * n * n), kThreads, 0, s>>>(n, z, zc, cg);
+    if (n % 16 == 0) k_prolong_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, z, zc, cg);
     else k_prolong_add<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, cg);
 }
 

@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
 // every x, including signed zeros), so results equal k_sor_rb's bit for bit.
 // Needs hw % 4 == 0 and 2 * n^2 * hw < 2^31.
 template <bool EXACT, bool RESID>
-__global__ void __launch_bounds__(kThreads) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
+__global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
                                                       RelaxTable wr, float* __restrict__ xs,
                                                       const float* __restrict__ bs, ProjControl* ctrl,
                                                       int guarded, int sweep_index, int subtract_mean, int zb) {

@@ -187,6 +187,150 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     if (warp == 0) tc::tmem_dealloc(tmem, T::kCols);
 }
 
+// The same convolution marching in z: a CTA computes zt consecutive planes of
+// its 8 x 16 tile. All of the layer's weights stay in shared memory
+// ([chunk][tap][N/8][2][8][16 B]) and the input halo is a ring of 4 planes
+// (each [chunk][18 rows][320 B] as above), so every input plane is loaded
+// once per CTA instead of three times per output plane, and plane z + 2
+// loads while plane z's 27 x chunks MMAs and epilogue run. Used when the
+// weights and the ring fit in shared memory (ConvMarch<N>::fits).
+template <int N>
+struct ConvMarch {
+    static constexpr int kPlane = 18 * 320;  // one chunk of one halo plane
+    static int smem(int cin) { return 27 * N * cin * 2 + 4 * (cin / 16) * kPlane + 1024; }
+    static bool fits(int cin) { return smem(cin) <= 200 * 1024; }
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt) {
+    using T = ConvTile<N>;
+    using Z = ConvMarch<N>;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float s_bias[N];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16;
+    const int z0 = blockIdx.z * zt, z1 = min(a.D, z0 + zt);
+    const int chunks = a.cin / 16;
+    const uint32_t sbase = tc::smem_addr(smem);
+    const uint32_t wbase = sbase;
+    const uint32_t rbase = sbase + uint32_t(27 * N * a.cin * 2);
+    const uint32_t bar_addr = tc::smem_addr(&bar);
+
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
+    if (tid == 0) {
+        tc::mbar_init(bar_addr, 1);
+        tc::fence_mbarrier_init();
+    }
+    for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
+    // all weights: (chunk, tap, co, half) segments of 16 bytes
+    for (int i = tid; i < chunks * 27 * N * 2; i += blockDim.x) {
+        const int half = i & 1, co = (i >> 1) % N, ct = (i >> 1) / N;  // ct = chunk * 27 + tap
+        const int t = ct % 27, cc = ct / 27;
+        const __nv_bfloat16* wsrc = a.w + (long(t) * N + co) * a.cin + cc * 16 + half * 8;
+        tc::cp_async16(wbase + uint32_t(ct * N * 32 + (co >> 3) * 256 + half * 128 + (co & 7) * 16), wsrc, true);
+    }
+    // halo plane zz (all chunks) into ring slot zz & 3; rows outside the grid read as zero
+    auto load_plane = [&](int zz) {
+        const uint32_t slot = rbase + uint32_t((zz & 3) * chunks * Z::kPlane);
+        for (int i = tid; i < chunks * 18 * 20; i += blockDim.x) {
+            const int half = i & 1, v = (i >> 1) % 10, rc = (i >> 1) / 10;  // rc = chunk * 18 + ry
+            const int ry = rc % 18, cc = rc / 18;
+            const int x = x0 - 1 + v, y = y0 + ry - 1;
+            const bool valid = x >= 0 && x < a.W && y >= 0 && y < a.H && zz >= 0 && zz < a.D;
+            const __nv_bfloat16* src =
+                valid ? a.in + ((long(zz) * a.H + y) * a.W + x) * a.in_stride + cc * 16 + half * 8 : a.in;
+            tc::cp_async16(slot + uint32_t(rc * 320 + half * 160 + v * 16), src, valid);
+        }
+    };
+    load_plane(z0 - 1);
+    load_plane(z0);
+    load_plane(z0 + 1);
+    tc::cp_async_wait_all();
+    tc::fence_proxy_async();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
+    bool ok = true;
+    int phase = 0;
+    for (int z = z0; z < z1; ++z) {
+        if (z + 2 <= z1) load_plane(z + 2);  // overlaps this plane's MMAs and epilogue
+        if (tid == 0) {
+            tc::tc_fence_after();
+#pragma unroll 1
+            for (int cc = 0; cc < chunks; ++cc)
+#pragma unroll 1
+                for (int t = 0; t < 27; ++t) {
+                    const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                    const uint32_t a_addr = rbase + uint32_t((((z + dz - 1) & 3) * chunks + cc) * Z::kPlane +
+                                                             dy * 320 + dx * 16);
+                    const uint32_t b_addr = wbase + uint32_t((cc * 27 + t) * N * 32);
+                    tc::mma_bf16(tmem, tc::smem_desc(a_addr, 160, 320), tc::smem_desc(b_addr, 128, 256), idesc,
+                                 cc > 0 || t > 0);
+                }
+            tc::mma_commit(bar_addr);
+        }
+        const bool mine = tc::mbar_wait(bar_addr, uint32_t(phase) & 1u, kWaitLimit);
+        ++phase;
+        if (!__syncthreads_and(mine)) {
+            ok = false;
+            break;
+        }
+        tc::tc_fence_after();
+        if (warp < 4) {
+            const int m = warp * 32 + lane;
+            const int x = x0 + (m & 7), y = y0 + (m >> 3);
+            const bool vin = x < a.W && y < a.H;
+            const long v = (long(z) * a.H + y) * a.W + x;
+            const uint32_t lane_base = uint32_t(warp * 32) << 16;
+#pragma unroll
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float acc[16];
+                tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
+                if (vin) {
+                    float val[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        val[i] = acc[i] + s_bias[c0 + i];
+                        if (a.relu) val[i] = fmaxf(val[i], 0.f);
+                    }
+                    const long o = v * a.out_stride + a.out_offset + c0;
+                    if (a.out_fp32) {
+                        float* dst = static_cast<float*>(a.out) + o;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) dst[i] = val[i];
+                    } else {
+                        __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(val[i]);
+                        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o);
+                        dst[0] = reinterpret_cast<const uint4*>(h)[0];
+                        dst[1] = reinterpret_cast<const uint4*>(h)[1];
+                    }
+                }
+            }
+        }
+        // the next plane's MMAs overwrite TMEM and read the plane loaded above
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async();
+        tc::tc_fence_before();
+        __syncthreads();
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(a.error, 1u);
+        // drain the commit whose wait timed out (phase - 1), bounded
+        tc::mbar_wait(bar_addr, uint32_t(phase - 1) & 1u, kWaitLimit);
+        tc::cp_async_wait_all();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, T::kCols);
+}
+
 // ---- CUDA-core kernels -------------------------------------------------------
 
 // Input features: channel 0 = b / scale (from the solver's red-black split RHS,
@@ -215,10 +359,13 @@ __global__ void k_prep_natural(long V, const float* __restrict__ a, const double
     const float inv = 1.f / fmaxf(*scale, 1e-30f);
     const float m = float(*mean);
     for (long v = long(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += long(gridDim.x) * blockDim.x) {
-        __nv_bfloat16* o = out + v * 16;
-        o[0] = __float2bfloat16_rn((a[v] - m) * inv);
+        __align__(16) __nv_bfloat16 h[8];
+        h[0] = __float2bfloat16_rn((a[v] - m) * inv);
 #pragma unroll
-        for (int c = 1; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+        for (int c = 1; c < 8; ++c) h[c] = __float2bfloat16_rn(0.f);
+        uint4* o = reinterpret_cast<uint4*>(out + v * 16);
+        o[0] = *reinterpret_cast<const uint4*>(h);
+        o[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 __global__ void k_rms_natural(long V, const float* __restrict__ a, const double* __restrict__ mean,
@@ -281,16 +428,20 @@ __global__ void k_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* __re
 
 // Nearest 2x upsampling of a coarse tensor into channels [0, C) of a fine
 // buffer with channel stride out_stride.
+// Nearest 2x upsampling into the first C channels of a concatenation buffer,
+// 8 channels (16 bytes) per thread (C, out_stride multiples of 8).
 __global__ void k_upsample2(int d, int h, int w, int C, const __nv_bfloat16* __restrict__ in,
                             __nv_bfloat16* __restrict__ out, int out_stride) {
     const int D = 2 * d, H = 2 * h, W = 2 * w;
-    const long total = long(D) * H * W * C;
+    const int C8 = C / 8;
+    const long total = long(D) * H * W * C8;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
-        const int c = int(i % C);
-        const long v = i / C;
+        const int c = int(i % C8) * 8;
+        const long v = i / C8;
         int x, y, z;
         decode(v, H, W, x, y, z);
-        out[v * out_stride + c] = in[((long(z / 2) * h + y / 2) * w + x / 2) * C + c];
+        *reinterpret_cast<uint4*>(out + v * out_stride + c) =
+            *reinterpret_cast<const uint4*>(in + ((long(z / 2) * h + y / 2) * w + x / 2) * C + c);
     }
 }
 
@@ -632,15 +783,26 @@ template <int N>
 void configure_n() {
     VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  ConvTile<N>::kSmemMax));
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_zm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 }
 
 template <int N>
 void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
     if (a.cin % 16 != 0 || a.in_stride % 8 != 0 || a.out_stride % 8 != 0 || a.out_offset % 8 != 0)
         fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
-    const dim3 grid(unsigned((a.W + 7) / 8), unsigned((a.H + 15) / 16), unsigned(a.D));
+    const unsigned gx = unsigned((a.W + 7) / 8), gy = unsigned((a.H + 15) / 16);
     count_launch();
-    k_conv3_tc<N><<<grid, 256, ConvTile<N>::smem(a.cin / 16), s>>>(a);
+    if (ConvMarch<N>::fits(a.cin)) {
+        // planes per CTA: the largest power of two up to 8 that keeps at least
+        // two CTAs per SM
+        int zt = 8;
+        while (zt > 1 && long(gx) * gy * ((a.D + zt - 1) / zt) < 2L * 148) zt >>= 1;
+        const dim3 grid(gx, gy, unsigned((a.D + zt - 1) / zt));
+        k_conv3_zm<N><<<grid, 256, ConvMarch<N>::smem(a.cin), s>>>(a, zt);
+    } else {
+        const dim3 grid(gx, gy, unsigned(a.D));
+        k_conv3_tc<N><<<grid, 256, ConvTile<N>::smem(a.cin / 16), s>>>(a);
+    }
 }
 
 }  // namespace
@@ -705,7 +867,8 @@ void launch_avgpool2(int D, int H, int W, int C, const __nv_bfloat16* in, int in
 void launch_upsample2(int d, int h, int w, int C, const __nv_bfloat16* in, __nv_bfloat16* out, int out_stride,
                       cudaStream_t s) {
     count_launch();
-    k_upsample2<<<blocks_for(8L * d * h * w * C), 256, 0, s>>>(d, h, w, C, in, out, out_stride);
+    if (C % 8 != 0 || out_stride % 8 != 0) fail(VAPOR_INVALID_ARGUMENT, "upsampling needs channels in multiples of 8");
+    k_upsample2<<<blocks_for(long(d) * h * w * C), 256, 0, s>>>(d, h, w, C, in, out, out_stride);
 }
 
 void launch_head(long V, int C, const __nv_bfloat16* act, const float* w, const float* bias, float* out,
