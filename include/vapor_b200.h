@@ -302,6 +302,15 @@ vapor_status vapor_stage_advect_scalar_device(vapor_stage *stage, float dt, floa
 /* Pressure solver used by vapor_stage_project (vapor_solver_kind); the default
  * is VAPOR_SOLVER_RED_BLACK_SOR, the reference's SOR. */
 vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
+/* Solid obstacles for vapor_stage_project (extension, no reference
+ * counterpart; Vapor's solvers have walls only). `mask` is n^3 host bytes,
+ * x fastest, nonzero = solid; NULL removes the obstacles. Faces touching a
+ * solid cell are closed (velocity 0 before and after the projection), solid
+ * cells are not unknowns (pressure 0, excluded from the residual), the
+ * diagonal of a fluid cell counts its fluid neighbours, and the right-hand-side
+ * and pressure means run over fluid cells. Needs VAPOR_SOLVER_MIXED_REFINEMENT;
+ * a mask without fluid cells is VAPOR_INVALID_ARGUMENT. */
+vapor_status vapor_stage_set_solid(vapor_stage *stage, const uint8_t *mask);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 
 /* Advection of one staggered field that allocates no device memory. No

@@ -262,8 +262,37 @@ void applyGradient64(const Grid<T>& g, const double* p, T dt, F* u, F* v, F* w) 
 // diagonal = number of existing neighbours, every coupling -1. Stored
 // implicitly; the operator order matches StencilLinearSystem.
 // ---------------------------------------------------------------------------
+// Solid obstacles (extension, no reference counterpart): while a projection
+// with a solid mask runs, tSolid points at its n^3 mask (x fastest, nonzero =
+// solid). Solid cells are not unknowns (pressure 0, residual excluded); the
+// diagonal of a fluid cell counts its fluid neighbours; faces touching a
+// solid are closed (velocity 0).
+thread_local const uint8_t* tSolid = nullptr;
+inline bool solidAt(int n, int x, int y, int z) {
+    return tSolid && tSolid[size_t(x) + size_t(n) * (size_t(y) + size_t(n) * z)] != 0;
+}
+
 inline int neighbourCount(int n, int x, int y, int z) {
-    return (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+    if (!tSolid) return (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+    if (solidAt(n, x, y, z)) return 0;
+    return (x > 0 && !solidAt(n, x - 1, y, z)) + (x + 1 < n && !solidAt(n, x + 1, y, z)) +
+           (y > 0 && !solidAt(n, x, y - 1, z)) + (y + 1 < n && !solidAt(n, x, y + 1, z)) +
+           (z > 0 && !solidAt(n, x, y, z - 1)) + (z + 1 < n && !solidAt(n, x, y, z + 1));
+}
+
+// Zero every face that touches a solid cell (no-op without a mask).
+template <class T, class F>
+void enforceSolids(const Grid<T>& g, F* u, F* v, F* w) {
+    if (!tSolid) return;
+    const int n = g.n;
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                if (!solidAt(n, x, y, z)) continue;
+                u[g.index(FACE_X, x, y, z)] = u[g.index(FACE_X, x + 1, y, z)] = F(0);
+                v[g.index(FACE_Y, x, y, z)] = v[g.index(FACE_Y, x, y + 1, z)] = F(0);
+                w[g.index(FACE_Z, x, y, z)] = w[g.index(FACE_Z, x, y, z + 1)] = F(0);
+            }
 }
 
 // FP64 infinity norm of b - A x (StencilLinearSystem.cpp:53-70).
@@ -275,6 +304,7 @@ double residualInf(int n, const X* x, const B* b) {
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
                 const size_t id = size_t(i) + size_t(n) * (size_t(j) + size_t(n) * k);
+                if (solidAt(n, i, j, k)) continue;
                 double ax = double(float(neighbourCount(n, i, j, k))) * double(x[id]);
                 if (i > 0) ax += -1.0 * double(x[id - 1]);
                 if (i + 1 < n) ax += -1.0 * double(x[id + 1]);
@@ -398,6 +428,10 @@ inline bool refinementSolve(int n, float omega, float floorDiag, std::vector<dou
             for (int j = 0; j < n; ++j)
                 for (int i = 0; i < n; ++i) {
                     const size_t id = size_t(i) + size_t(n) * (size_t(j) + size_t(n) * k);
+                    if (solidAt(n, i, j, k)) {
+                        res[id] = 0.0;
+                        continue;
+                    }
                     double ax = double(neighbourCount(n, i, j, k)) * x64[id];
                     if (i > 0) ax -= x64[id - 1];
                     if (i + 1 < n) ax -= x64[id + 1];
@@ -434,7 +468,7 @@ inline bool refinementSolve(int n, float omega, float floorDiag, std::vector<dou
         for (int k = 0; k < n; ++k)
             for (int j = 0; j < n; ++j)
                 for (int i = 0; i < n; ++i) {
-                    if (((i + j + k) & 1) == 0) continue;
+                    if (((i + j + k) & 1) == 0 || solidAt(n, i, j, k)) continue;
                     const size_t id = size_t(i) + size_t(n) * (size_t(j) + size_t(n) * k);
                     const float diag = float(neighbourCount(n, i, j, k));
                     float off = 0.f;
@@ -475,21 +509,29 @@ int project(const Grid<T>& g, F* u, F* v, F* w, T dt, T omega, T floorDiag, cons
     const int n = g.n;
     const size_t count = size_t(n) * n * n;
     enforceWalls(g, u, v, w);
+    enforceSolids(g, u, v, w);
     std::vector<T> b(count);
     result = {};
+    size_t fluid = 0;
     for (int z = 0; z < n; ++z)
         for (int y = 0; y < n; ++y)
             for (int x = 0; x < n; ++x) {
+                const size_t i = g.index(CELL, x, y, z);
+                if (solidAt(n, x, y, z)) {
+                    b[i] = T(0);
+                    continue;
+                }
+                ++fluid;
                 const T d = divergenceAt(g, u, v, w, x, y, z);
                 if (!std::isfinite(double(d))) return VAPOR_NON_FINITE;
-                const size_t i = g.index(CELL, x, y, z);
                 result.divergence_before = std::max(result.divergence_before, float(std::abs(d)));
                 b[i] = -d * scale;
             }
     double sum = 0.0;
     for (size_t i = 0; i < count; ++i) sum += double(b[i]);
-    result.removed_rhs_mean = sum / double(count);
-    for (auto& value : b) value -= T(result.removed_rhs_mean);
+    result.removed_rhs_mean = sum / double(fluid);
+    for (size_t i = 0; i < count; ++i)
+        if (!tSolid || !tSolid[i]) b[i] -= T(result.removed_rhs_mean);
     pressure.assign(count, T(0));
     if (solverKind == VAPOR_SOLVER_MIXED_REFINEMENT && sizeof(T) == sizeof(float)) {
         std::vector<double> x64(count, 0.0);
@@ -499,8 +541,9 @@ int project(const Grid<T>& g, F* u, F* v, F* w, T dt, T omega, T floorDiag, cons
         result.residual_available = 1;
         double pm = 0.0;
         for (double value : x64) pm += value;
-        pm /= double(count);
-        for (auto& value : x64) value -= pm;
+        pm /= double(fluid);
+        for (size_t i = 0; i < count; ++i)
+            if (!tSolid || !tSolid[i]) x64[i] -= pm;
         result.linear_solve.final_residual = residualInf(n, x64.data(), bf.data());
         const double target = std::max(o.absolute_tolerance, o.relative_tolerance * result.linear_solve.initial_residual);
         result.linear_solve.converged = result.linear_solve.final_residual <= target;
@@ -512,14 +555,16 @@ int project(const Grid<T>& g, F* u, F* v, F* w, T dt, T omega, T floorDiag, cons
         result.residual_available = 1;
         double pm = 0.0;
         for (size_t i = 0; i < count; ++i) pm += double(pressure[i]);
-        pm /= double(count);
-        for (auto& value : pressure) value -= T(pm);
+        pm /= double(fluid);
+        for (size_t i = 0; i < count; ++i)
+            if (!tSolid || !tSolid[i]) pressure[i] -= T(pm);
         result.linear_solve.final_residual = residualInf(n, pressure.data(), b.data());
         const double target = std::max(o.absolute_tolerance, o.relative_tolerance * result.linear_solve.initial_residual);
         result.linear_solve.converged = result.linear_solve.final_residual <= target;
         applyGradient(g, pressure.data(), dt, u, v, w);
     }
     enforceWalls(g, u, v, w);
+    enforceSolids(g, u, v, w);
     const T after = maxDivergence(g, u, v, w);
     if (std::isnan(double(after))) return VAPOR_NON_FINITE;
     result.divergence_after = float(after);
@@ -803,6 +848,15 @@ VO_EXPORT vapor_status vapor_mac3d_default_params(vapor_mac3d_params* o) {
         const int status = project(g, u, v, w, dt, omega, floorDiag, *o, solverKind, *r, pressure);         \
         if (pressureOut && pressure.size() == size_t(n) * n * n)                                            \
             std::copy(pressure.begin(), pressure.end(), pressureOut);                                       \
+        return status;                                                                                      \
+    }                                                                                                       \
+    VO_EXPORT int vo_project_masked_##SUF(int n, T box, T* u, T* v, T* w, T dt, T omega, T floorDiag,       \
+                                          const vapor_linear_solve_options* o, int solverKind,              \
+                                          const uint8_t* solid, vapor_projection_result* r, T* pressureOut) {\
+        tSolid = solid;                                                                                     \
+        const int status = vo_project_##SUF(n, box, u, v, w, dt, omega, floorDiag, o, solverKind, r,        \
+                                            pressureOut);                                                   \
+        tSolid = nullptr;                                                                                   \
         return status;                                                                                      \
     }                                                                                                       \
     VO_EXPORT void* vo_sim_create_##SUF(int n, T box) { return new Simulation<T>(n, box); }                 \

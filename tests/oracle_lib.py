@@ -41,6 +41,8 @@ def _setup_oracle(lib):
         f("vo_sor_iteration", None, C.c_int, T, T, P, P)
         f("vo_project", C.c_int, C.c_int, T, P, P, P, T, T, T, C.POINTER(LinearSolveOptions), C.c_int,
           C.POINTER(ProjectionResult), P)
+        f("vo_project_masked", C.c_int, C.c_int, T, P, P, P, T, T, T, C.POINTER(LinearSolveOptions), C.c_int,
+          _vp, C.POINTER(ProjectionResult), P)
         f("vo_sim_create", _vp, C.c_int, T)
         f("vo_sim_destroy", None, _vp)
         f("vo_sim_set_params", None, _vp, C.POINTER(MacParams))
@@ -281,14 +283,30 @@ def ref_project(n, box, u, v, w, dt, omega, floor, opts):
     return st, r, u, v, w, p
 
 
-def oracle_project(n, box, u, v, w, dt, omega, floor, opts, solver_kind=0, dtype=np.float32):
+def oracle_project(n, box, u, v, w, dt, omega, floor, opts, solver_kind=0, dtype=np.float32, solid=None):
+    """The oracle's projection; `solid` (n^3 uint8, x fastest, nonzero = solid)
+    adds obstacles: closed faces, fluid-only unknowns and means."""
     suf = "f32" if np.dtype(dtype) == np.float32 else "f64"
     u, v, w = [np.array(a, dtype=dtype, copy=True) for a in (u, v, w)]
     p = np.zeros((n, n, n), dtype)
     r = ProjectionResult()
-    st = getattr(oracle(), f"vo_project_{suf}")(n, box, u, v, w, dt, omega, floor, C.byref(opts), solver_kind,
-                                               C.byref(r), p)
+    if solid is None:
+        st = getattr(oracle(), f"vo_project_{suf}")(n, box, u, v, w, dt, omega, floor, C.byref(opts), solver_kind,
+                                                   C.byref(r), p)
+    else:
+        mask = np.ascontiguousarray(solid, dtype=np.uint8)
+        assert mask.size == n ** 3
+        st = getattr(oracle(), f"vo_project_masked_{suf}")(n, box, u, v, w, dt, omega, floor, C.byref(opts),
+                                                          solver_kind, mask.ctypes.data, C.byref(r), p)
     return st, r, u, v, w, p
+
+
+def sphere_mask(n, centre, radius):
+    """Cells whose centres lie inside a sphere (box 1), as an n^3 uint8 mask."""
+    c = (np.arange(n) + 0.5) / n
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    d2 = (xx - centre[0]) ** 2 + (yy - centre[1]) ** 2 + (zz - centre[2]) ** 2
+    return (d2 < radius * radius).astype(np.uint8)
 
 
 def random_fields(n, seed, scale=1.0, density=True):

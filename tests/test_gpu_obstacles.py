@@ -1,0 +1,71 @@
+"""Solid obstacles in the staged projection (extension, no reference
+counterpart): GPU against the oracle's restatement of the same rules."""
+import numpy as np
+import pytest
+
+import vapor_b200 as vb
+from oracle_lib import oracle_project, random_fields, sphere_mask
+from vapor_b200.abi import LinearSolveOptions, ProjectionOptions
+
+pytestmark = pytest.mark.gpu
+
+
+def _stage(n, mask):
+    st = vb.StageBackend(n, 1.0)
+    st.set_solver_kind(vb.abi.SOLVER_MIXED_REFINEMENT)
+    st.set_solid(mask)
+    return st
+
+
+def _opts(rel):
+    return LinearSolveOptions.defaults(max_iterations=20000, relative_tolerance=rel, absolute_tolerance=0.0)
+
+
+def test_empty_mask_is_the_plain_projection():
+    n = 24
+    _, u, v, w = random_fields(n, seed=61)
+    outs = []
+    for mask in (None, np.zeros((n, n, n), np.uint8)):
+        st = _stage(n, mask)
+        fields = [a.copy() for a in (u, v, w)]
+        r, p = st.project(*fields, ProjectionOptions(0.01, 1.9, _opts(1e-7)), 6.0, want_pressure=True)
+        outs.append((r.linear_solve.iterations, fields, p))
+    assert outs[0][0] == outs[1][0]
+    for a, b in zip(outs[0][1] + [outs[0][2]], outs[1][1] + [outs[1][2]]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [20, 33])
+def test_sphere_obstacle_matches_the_oracle(n):
+    """Same rules as the oracle (closed faces, fluid-only unknowns and means).
+    The FP64 fluid means are sums in a different order, so the bar is the
+    north star's 1e-5 relative; iteration counts agree within one check."""
+    mask = sphere_mask(n, (0.5, 0.45, 0.55), 0.22)
+    _, u, v, w = random_fields(n, seed=70 + n)
+    opts = _opts(1e-8)
+    st, ro, ue, ve, we, pe = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=1, solid=mask)
+    assert st == 0 and ro.linear_solve.converged
+    stage = _stage(n, mask)
+    ug, vg, wg = [a.copy() for a in (u, v, w)]
+    r, pg = stage.project(ug, vg, wg, ProjectionOptions(0.01, 1.9, opts), 6.0, want_pressure=True)
+    ls = r.linear_solve
+    assert ls.converged and ls.final_residual <= 1e-8 * ls.initial_residual
+    assert abs(ls.iterations - ro.linear_solve.iterations) <= 8
+    for a, b in ((ug, ue), (vg, ve), (wg, we), (pg, pe)):
+        assert np.abs(a - b).max() <= 1e-5 * max(1.0, float(np.abs(b).max()))
+    s = mask.astype(bool)
+    assert np.all(pg[s] == 0)
+    assert np.all(ug[:, :, :-1][s] == 0) and np.all(ug[:, :, 1:][s] == 0)
+    assert np.all(vg[:, :-1, :][s] == 0) and np.all(vg[:, 1:, :][s] == 0)
+    assert np.all(wg[:-1][s] == 0) and np.all(wg[1:][s] == 0)
+
+
+def test_obstacle_rejections():
+    n = 16
+    stage = vb.StageBackend(n, 1.0)
+    with pytest.raises(vb.InvalidArgument):
+        stage.set_solid(np.ones((n, n, n), np.uint8))  # no fluid left
+    stage.set_solid(sphere_mask(n, (0.5, 0.5, 0.5), 0.2))
+    _, u, v, w = random_fields(n, seed=5)
+    with pytest.raises(vb.InvalidArgument):  # the reference's SOR kind has no obstacles
+        stage.project(u.copy(), v.copy(), w.copy(), ProjectionOptions(0.01, 1.9, _opts(1e-6)), 6.0)

@@ -330,3 +330,47 @@ def test_fp64_oracle_tracks_fp32(alg):
     for x, y in zip(a.fields(), b.fields()):
         scale = max(1.0, float(np.abs(y).max()))
         assert np.abs(x.astype(np.float64) - y).max() <= 1e-4 * scale
+
+
+def test_solid_mask_without_solids_is_the_plain_projection():
+    """The obstacle path with an empty mask reproduces the plain projection bit for bit."""
+    from oracle_lib import oracle_project, random_fields
+    from vapor_b200.abi import LinearSolveOptions
+    n = 12
+    _, u, v, w = random_fields(n, seed=41)
+    opts = LinearSolveOptions.defaults(max_iterations=400, relative_tolerance=1e-6, absolute_tolerance=0.0)
+    for kind in (0, 1):
+        a = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=kind)
+        b = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=kind,
+                           solid=np.zeros((n, n, n), np.uint8))
+        assert a[0] == b[0] == 0
+        assert a[1].linear_solve.iterations == b[1].linear_solve.iterations
+        for x, y in zip(a[2:], b[2:]):
+            assert bits_equal(x, y)
+
+
+def test_sphere_obstacle_projection_closes_its_faces():
+    """Sphere obstacle: faces touching solid cells are zero, pressure is zero
+    inside, the fluid divergence drops to the solve tolerance, and the FP32
+    mixed-precision result tracks the FP64 oracle."""
+    from oracle_lib import oracle_project, random_fields, sphere_mask
+    from vapor_b200.abi import LinearSolveOptions
+    n = 20
+    solid = sphere_mask(n, (0.5, 0.45, 0.5), 0.2)
+    assert 0 < solid.sum() < n ** 3
+    _, u, v, w = random_fields(n, seed=43)
+    opts = LinearSolveOptions.defaults(max_iterations=20000, relative_tolerance=1e-8, absolute_tolerance=0.0)
+    st, r, uo, vo, wo, p = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=1, solid=solid)
+    assert st == 0 and r.linear_solve.converged
+    s = solid.astype(bool)
+    assert np.all(p[s] == 0)
+    # faces of solid cells
+    assert np.all(uo[:, :, :-1][s] == 0) and np.all(uo[:, :, 1:][s] == 0)
+    assert np.all(vo[:, :-1, :][s] == 0) and np.all(vo[:, 1:, :][s] == 0)
+    assert np.all(wo[:-1][s] == 0) and np.all(wo[1:][s] == 0)
+    assert r.divergence_after <= 1e-5 * r.divergence_before
+    st64, r64, u64, v64, w64, p64 = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=0,
+                                                   dtype=np.float64, solid=solid)
+    assert st64 == 0 and r64.linear_solve.converged
+    for a, b in ((uo, u64), (vo, v64), (wo, w64)):
+        assert np.abs(a - b).max() <= 1e-5 * max(1.0, np.abs(b).max())

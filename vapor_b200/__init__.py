@@ -106,6 +106,7 @@ def _declare(lib):
     f("vapor_stage_advect_scalar_device", _vp, C.c_float, C.c_float, C.c_int32, _vp, _vp, _vp, _vp)
     f("vapor_stage_set_solver_kind", _vp, C.c_int32)
     f("vapor_stage_stream", _vp, C.POINTER(_vp))
+    f("vapor_stage_set_solid", _vp, _vp)
     f("vapor_advect_noalloc", C.c_int32, C.c_float, C.c_int32, C.c_float, C.c_float, C.c_int32,
       _vp, _vp, _vp, _vp, _vp, _vp)
     f("vapor_unet_parameter_count", res=C.c_int64)
@@ -346,6 +347,16 @@ class StageBackend:
     def set_solver_kind(self, kind):
         check(library().vapor_stage_set_solver_kind(self._h, int(kind)))
 
+    def set_solid(self, mask):
+        """Solid obstacles: n^3 uint8 mask (z, y, x order, nonzero = solid) or None."""
+        if mask is None:
+            check(library().vapor_stage_set_solid(self._h, None))
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.size != self.n ** 3:
+            raise ValueError(f"mask needs {self.n ** 3} cells")
+        check(library().vapor_stage_set_solid(self._h, m.ctypes.data))
+
     def set_preconditioner(self, net):
         """Coarse-grid network of the FPCG solver (None: smoothing only)."""
         check(library().vapor_stage_set_preconditioner(self._h, net.handle if net is not None else None))
@@ -366,6 +377,13 @@ class StageBackend:
         check(library().vapor_stage_project(self._h, *ptrs, C.byref(options), float(diagonal_floor), C.byref(r),
                                             p.ctypes.data if p is not None else None))
         return r, p
+
+    def project_device(self, u_ptr, v_ptr, w_ptr, options, diagonal_floor=0.0, pressure_ptr=None):
+        """The same projection on device pointers (in place); returns the result."""
+        r = ProjectionResult()
+        check(library().vapor_stage_project_device(self._h, u_ptr, v_ptr, w_ptr, C.byref(options),
+                                                   float(diagonal_floor), C.byref(r), pressure_ptr))
+        return r
 
     def advect_face(self, axis, dt, cfl, method, source, flow, output):
         f = field_sizes(self.n)[1]

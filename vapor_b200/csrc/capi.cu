@@ -279,6 +279,9 @@ VB_API vapor_status vapor_stage_set_solver_kind(vapor_stage* stage, int32_t kind
                         "Unknown solver kind");
                 stage->stage.solver_kind = kind);
 }
+VB_API vapor_status vapor_stage_set_solid(vapor_stage* stage, const uint8_t* mask) {
+    STAGE_GUARD(stage->stage.set_solid(mask));
+}
 VB_API vapor_status vapor_stage_stream(vapor_stage* stage, void** stream) {
     STAGE_GUARD(require(stream != nullptr, "null output"); *stream = (void*)stage->stage.stream());
 }

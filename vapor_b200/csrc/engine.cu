@@ -44,6 +44,7 @@ template struct DevArray<float>;
 template struct DevArray<double>;
 template struct DevArray<uint32_t>;
 template struct DevArray<uint16_t>;
+template struct DevArray<uint8_t>;
 
 Stream::Stream() { VB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
 Stream::~Stream() {
@@ -246,6 +247,39 @@ static cudaGraphConditionalHandle new_condition(cudaStream_t s) {
     return h;
 }
 
+void Workspace::set_solid(const uint8_t* mask) {
+    VB_CUDA(cudaStreamSynchronize(stream_));
+    if (!mask) {
+        solid_.release();
+        solid_diag_.release();
+        fluid_ = 0.0;
+        return;
+    }
+    const int n = n_;
+    const size_t cells = size_t(n) * n * n;
+    const RBLayout L = rb_layout(n);
+    auto solid = [&](int x, int y, int z) { return mask[(size_t(z) * n + y) * n + x] != 0; };
+    std::vector<uint8_t> nat(cells), diag(rb_count(n), 0);
+    size_t fluid = 0;
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const bool s = solid(x, y, z);
+                nat[(size_t(z) * n + y) * n + x] = s ? 1 : 0;
+                if (s) continue;
+                ++fluid;
+                diag[rb_index(L, x, y, z)] = uint8_t((x > 0 && !solid(x - 1, y, z)) + (x + 1 < n && !solid(x + 1, y, z)) +
+                                                     (y > 0 && !solid(x, y - 1, z)) + (y + 1 < n && !solid(x, y + 1, z)) +
+                                                     (z > 0 && !solid(x, y, z - 1)) + (z + 1 < n && !solid(x, y, z + 1)));
+            }
+    if (fluid == 0) fail(VAPOR_INVALID_ARGUMENT, "the solid mask leaves no fluid cell");
+    solid_.allocate(cells);
+    solid_diag_.allocate(diag.size());
+    VB_CUDA(cudaMemcpy(solid_.p, nat.data(), cells, cudaMemcpyHostToDevice));
+    VB_CUDA(cudaMemcpy(solid_diag_.p, diag.data(), diag.size(), cudaMemcpyHostToDevice));
+    fluid_ = double(fluid);
+}
+
 void Workspace::ensure_fpcg(bool coarse) {
     const size_t count = rb_count(n_);
     for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_})
@@ -359,7 +393,14 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
                         float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
                         const vapor_linear_solve_options& o, int solver_kind, unet::UNet* warm,
                         unet::UNet* coarse) {
-    const ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
+    ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
+    if (fluid_ > 0.0) {
+        if (solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
+            fail(VAPOR_INVALID_ARGUMENT, "solid obstacles need the mixed-precision solver (VAPOR_SOLVER_MIXED_REFINEMENT)");
+        a.diag = solid_diag_.p;
+        a.solid = solid_.p;
+        a.fluid = fluid_;
+    }
     cudaStream_t s = stream_;
     PhaseTimer& t = timer_;
     const bool fpcg = solver_kind == VAPOR_SOLVER_FPCG;

@@ -127,6 +127,11 @@ public:
     PhaseTimer& timer() { return timer_; }
     void ensure_mixed();
     void ensure_fpcg(bool coarse);
+    // Solid obstacles (extension): n^3 host mask, x fastest, nonzero = solid;
+    // null clears. Faces touching a solid are closed, solid cells are not
+    // unknowns, means run over fluid cells. Mixed-precision solver only.
+    void set_solid(const uint8_t* mask);
+    bool has_solid() const { return fluid_ > 0.0; }
     // While true, project() records CUDA-graph nodes (the solve loops become
     // conditional while nodes) instead of driving the loop from the host.
     void set_capturing(bool on) { capturing_ = on; }
@@ -146,6 +151,9 @@ private:
     DevArray<float> cg_rc_;             // FPCG coarse right-hand side ((n/4)^3, natural layout)
     DevArray<float> cg_rows_;           // FPCG restriction scratch (n^2 * n/4 row sums)
     DevArray<double> cg_partials_;
+    DevArray<uint8_t> solid_;           // natural-layout solid mask (obstacles)
+    DevArray<uint8_t> solid_diag_;      // split-layout fluid-neighbour counts, 0 = solid
+    double fluid_ = 0.0;                // fluid cells when a mask is set, else 0
     CgControl* cg_ = nullptr;           // device
     int partial_capacity_ = 0;
     ProjControl* ctrl_ = nullptr;       // device
@@ -249,7 +257,8 @@ public:
 
     void reset();
     int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR;
-    unet::UNet* coarse = nullptr;  // FPCG coarse-grid network (bound to this stage's stream per call)
+    unet::UNet* coarse = nullptr;
+    void set_solid(const uint8_t* mask) { ws_.set_solid(mask); }  // FPCG coarse-grid network (bound to this stage's stream per call)
     void project(float* u, float* v, float* w, const vapor_projection_options& options, float diagonal_floor,
                  vapor_projection_result* result, float* pressure_out, bool device_pointers);
     void advect(int loc, float dt, float cfl, int method, const float* src, const float* fu, const float* fv,

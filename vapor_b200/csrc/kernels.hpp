@@ -103,6 +103,12 @@ struct ProjectionArgs {
     float omega;
     float diagonal_floor;
     vapor_linear_solve_options options;
+    // Solid obstacles (extension; all null/zero without a mask): `diag` is
+    // the split-layout diagonal (fluid-neighbour count, 0 = solid cell),
+    // `solid` the natural-layout mask, `fluid` the number of fluid cells.
+    const uint8_t* diag = nullptr;
+    const uint8_t* solid = nullptr;
+    double fluid = 0.0;
 };
 // Graph while-loop control: when `active`, kernels that decide whether the
 // solve continues also set this conditional handle.

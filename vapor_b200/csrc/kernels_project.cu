@@ -70,7 +70,7 @@ __global__ void k_begin_projection(ProjControl* ctrl, vapor_linear_solve_options
 __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const float* __restrict__ u,
                                                   const float* __restrict__ v, const float* __restrict__ w,
                                                   float* __restrict__ b, double* __restrict__ partials,
-                                                  ProjControl* ctrl) {
+                                                  ProjControl* ctrl, const uint8_t* __restrict__ solid) {
     __shared__ double s_sum[32];
     __shared__ float s_max[32];
     __shared__ int s_key[32];
@@ -84,12 +84,18 @@ __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const flo
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode_cell(c, n, x, y, z);
-        const float u0 = x == 0 ? 0.f : u[index_of(n, FACE_X, x, y, z)];
-        const float u1 = x + 1 == n ? 0.f : u[index_of(n, FACE_X, x + 1, y, z)];
-        const float v0 = y == 0 ? 0.f : v[index_of(n, FACE_Y, x, y, z)];
-        const float v1 = y + 1 == n ? 0.f : v[index_of(n, FACE_Y, x, y + 1, z)];
-        const float w0 = z == 0 ? 0.f : w[index_of(n, FACE_Z, x, y, z)];
-        const float w1 = z + 1 == n ? 0.f : w[index_of(n, FACE_Z, x, y, z + 1)];
+        if (solid && solid[c]) {  // not an unknown: b = 0, outside every reduction
+            b[rb_index(L, x, y, z)] = 0.f;
+            continue;
+        }
+        // faces on walls or touching a solid are closed (read as zero)
+        auto open = [&](int xx, int yy, int zz) { return !solid || !solid[(size_t(zz) * n + yy) * n + xx]; };
+        const float u0 = (x == 0 || !open(x - 1, y, z)) ? 0.f : u[index_of(n, FACE_X, x, y, z)];
+        const float u1 = (x + 1 == n || !open(x + 1, y, z)) ? 0.f : u[index_of(n, FACE_X, x + 1, y, z)];
+        const float v0 = (y == 0 || !open(x, y - 1, z)) ? 0.f : v[index_of(n, FACE_Y, x, y, z)];
+        const float v1 = (y + 1 == n || !open(x, y + 1, z)) ? 0.f : v[index_of(n, FACE_Y, x, y + 1, z)];
+        const float w0 = (z == 0 || !open(x, y, z - 1)) ? 0.f : w[index_of(n, FACE_Z, x, y, z)];
+        const float w1 = (z + 1 == n || !open(x, y, z + 1)) ? 0.f : w[index_of(n, FACE_Z, x, y, z + 1)];
         const float div = (u1 - u0 + v1 - v0 + w1 - w0) / g.h;
         if (!isfinite(div)) bad = 1u;
         div_max = maxf_ref(div_max, fabsf(div));
@@ -164,7 +170,8 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
                                                      RelaxTable wr, float* __restrict__ xs,
                                                      const float* __restrict__ bs,
                                                      const ProjControl* __restrict__ ctrl, int guarded,
-                                                     int sweep_index, int subtract_mean) {
+                                                     int sweep_index, int subtract_mean,
+                                                     const uint8_t* __restrict__ diag_arr) {
     if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
     const int n = g.n;
     const RBLayout L = rb_layout(n);
@@ -225,7 +232,8 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
         const int xc = 2 * (i0 + k) + s;
         res[k] = xo[k];
         if (xc >= n) continue;
-        const float diag = float((xc > 0) + (xc + 1 < n) + ny);
+        const float diag = diag_arr ? float(diag_arr[size_t(colour) * L.stride + row + i0 + k])
+                                    : float((xc > 0) + (xc + 1 < n) + ny);
         if (diag == 0.f) continue;
         float off = 0.f;
         if (xc > 0) off += -1.f * xl[k];
@@ -261,7 +269,8 @@ template <bool EXACT, bool RESID>
 __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
                                                       RelaxTable wr, float* __restrict__ xs,
                                                       const float* __restrict__ bs, ProjControl* ctrl,
-                                                      int guarded, int sweep_index, int subtract_mean, int zb) {
+                                                      int guarded, int sweep_index, int subtract_mean, int zb,
+                                                      const uint8_t* __restrict__ diag) {
     if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
     const int n = g.n;
     const int hw = (n + 1) >> 1;
@@ -276,6 +285,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, flo
         float* __restrict__ own = xs + colour * stride + y * hw + i0;
         const float* __restrict__ oth = xs + (1 - colour) * stride + y * hw + i0;
         const float* __restrict__ rhs = bs + colour * stride + y * hw + i0;
+        const uint8_t* __restrict__ dg = diag ? diag + colour * stride + y * hw + i0 : nullptr;
         const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
         const int z0 = blockIdx.y * zb;
         const int z1 = min(n, z0 + zb);
@@ -309,12 +319,16 @@ __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, flo
             const float zm[4] = {cm.x, cm.y, cm.z, cm.w};
             const float zp[4] = {cp.x, cp.y, cp.z, cp.w};
             const int ny = nyz + int(z > 0) + int(z + 1 < n);
+            uchar4 dm = make_uchar4(0, 0, 0, 0);
+            if (dg) dm = *reinterpret_cast<const uchar4*>(dg + zoff);
+            const int dmask[4] = {dm.x, dm.y, dm.z, dm.w};
             float res[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int xc = 2 * (i0 + k) + sh;
                 const bool left = xc > 0, right = xc + 1 < n;
-                const int d = int(left) + int(right) + ny;
+                // solid neighbours hold 0, so summing them changes nothing
+                const int d = dg ? dmask[k] : int(left) + int(right) + ny;
                 const float diag = float(d);
                 float off = 0.f;
                 off += -1.f * (left ? xl[k] : 0.f);
@@ -360,7 +374,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, flo
 template <int VEC>
 __global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __restrict__ bs,
                                                         const float* __restrict__ es, float* __restrict__ r32,
-                                                        ProjControl* ctrl, int gated) {
+                                                        ProjControl* ctrl, int gated,
+                                                        const uint8_t* __restrict__ diag) {
     __shared__ double s_max[32];
     if (gated && !ctrl->recentre) return;
     const double* __restrict__ xin = ctrl->x64[ctrl->x64_cur];
@@ -402,7 +417,13 @@ __global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __r
         for (int k = 0; k < VEC; ++k) {
             const int xc = 2 * (i0 + k) + s;
             if (xc >= n) continue;
-            double ax = double((xc > 0) + (xc + 1 < n) + ny) * xo[k];
+            const int dcell = diag ? int(diag[own + i0 + k]) : (xc > 0) + (xc + 1 < n) + ny;
+            if (diag && dcell == 0) {  // solid cell: not an unknown
+                xout[own + i0 + k] = xo[k];
+                r32[own + i0 + k] = 0.f;
+                continue;
+            }
+            double ax = double(dcell) * xo[k];
             if (xc > 0) ax -= xl[k];
             if (xc + 1 < n) ax -= xl[k + 1];
             if (y > 0) ax -= ym[k];
@@ -435,7 +456,7 @@ __global__ void __launch_bounds__(kThreads) k_refine_rb(Grid g, const float* __r
 template <int VEC>
 __global__ void __launch_bounds__(kThreads) k_error_residual(Grid g, const float* __restrict__ es,
                                                              const float* __restrict__ r32, ProjControl* ctrl,
-                                                             int first_colour) {
+                                                             int first_colour, const uint8_t* __restrict__ diag) {
     __shared__ float s_max[32];
     const int n = g.n;
     const RBLayout L = rb_layout(n);
@@ -471,7 +492,9 @@ __global__ void __launch_bounds__(kThreads) k_error_residual(Grid g, const float
         for (int k = 0; k < VEC; ++k) {
             const int xc = 2 * (i0 + k) + s;
             if (xc >= n) continue;
-            const float diag = float((xc > 0) + (xc + 1 < n) + ny);
+            const int dcell = diag ? int(diag[own + i0 + k]) : (xc > 0) + (xc + 1 < n) + ny;
+            if (dcell == 0) continue;
+            const float dg = float(dcell);
             float off = 0.f;
             if (xc > 0) off += -1.f * xl[k];
             if (xc + 1 < n) off += -1.f * xl[k + 1];
@@ -479,7 +502,7 @@ __global__ void __launch_bounds__(kThreads) k_error_residual(Grid g, const float
             if (y + 1 < n) off += -1.f * yp[k];
             if (z > 0) off += -1.f * zm[k];
             if (z + 1 < n) off += -1.f * zp[k];
-            const float res = r32[own + i0 + k] - off - diag * xo[k];
+            const float res = r32[own + i0 + k] - off - dg * xo[k];
             if (!isfinite(res)) bad = 1u;
             const float aa = fabsf(res);
             rmax = rmax < aa ? aa : rmax;
@@ -550,7 +573,8 @@ __global__ void k_psum64_finish(ProjControl* ctrl, const double* __restrict__ pa
 // Final FP64 residual of x64 - mean (StencilLinearSystem.cpp:53-70 order) and
 // the float pressure copy (split layout).
 __global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const float* __restrict__ b,
-                                                         float* __restrict__ p32, ProjControl* ctrl) {
+                                                         float* __restrict__ p32, ProjControl* ctrl,
+                                                         const uint8_t* __restrict__ diag) {
     __shared__ double s_max[32];
     const double* __restrict__ x = ctrl->x64[ctrl->x64_cur];
     const int n = g.n;
@@ -563,10 +587,19 @@ __global__ void __launch_bounds__(kThreads) k_residual64(Grid g, const float* __
     for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
         int i, j, k;
         decode_cell(c, n, i, j, k);
-        auto xv = [&](int a, int bb, int cc) { return x[rb_index(L, a, bb, cc)] - pm; };
         const size_t me = rb_index(L, i, j, k);
+        if (diag && diag[me] == 0) {  // solid cell: pressure 0, no residual
+            p32[me] = 0.f;
+            continue;
+        }
+        // solid neighbours enter as 0 (their x64 is 0 and is not shifted)
+        auto xv = [&](int a, int bb, int cc) {
+            const size_t id = rb_index(L, a, bb, cc);
+            return (diag && diag[id] == 0) ? 0.0 : x[id] - pm;
+        };
         const double xc = x[me] - pm;
-        double ax = double(float(neighbours(n, i, j, k))) * xc;
+        const int dcell = diag ? int(diag[me]) : neighbours(n, i, j, k);
+        double ax = double(float(dcell)) * xc;
         if (i > 0) ax += -1.0 * xv(i - 1, j, k);
         if (i + 1 < n) ax += -1.0 * xv(i + 1, j, k);
         if (j > 0) ax += -1.0 * xv(i, j - 1, k);
@@ -593,7 +626,8 @@ __global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt,
                                                          const float* __restrict__ w, float* __restrict__ uo,
                                                          float* __restrict__ vo, float* __restrict__ wo,
                                                          float* __restrict__ uh, float* __restrict__ vh,
-                                                         float* __restrict__ wh, ProjControl* ctrl) {
+                                                         float* __restrict__ wh, ProjControl* ctrl,
+                                                         const uint8_t* __restrict__ solid) {
     __shared__ float s_max[32];
     const int n = g.n;
     const size_t cells = size_t(n) * n * n;
@@ -612,12 +646,15 @@ __global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt,
         const size_t ix0 = index_of(n, FACE_X, x, y, z), ix1 = ix0 + 1;
         const size_t iy0 = index_of(n, FACE_Y, x, y, z), iy1 = iy0 + n;
         const size_t iz0 = c, iz1 = c + nn;
-        const float ux0 = x == 0 ? 0.f : float(double(u[ix0]) - dtd * (pc - pv(x - 1, y, z)) * hInv);
-        const float ux1 = x + 1 == n ? 0.f : float(double(u[ix1]) - dtd * (pv(x + 1, y, z) - pc) * hInv);
-        const float vy0 = y == 0 ? 0.f : float(double(v[iy0]) - dtd * (pc - pv(x, y - 1, z)) * hInv);
-        const float vy1 = y + 1 == n ? 0.f : float(double(v[iy1]) - dtd * (pv(x, y + 1, z) - pc) * hInv);
-        const float wz0 = z == 0 ? 0.f : float(double(w[iz0]) - dtd * (pc - pv(x, y, z - 1)) * hInv);
-        const float wz1 = z + 1 == n ? 0.f : float(double(w[iz1]) - dtd * (pv(x, y, z + 1) - pc) * hInv);
+        // faces on walls or touching a solid cell are closed
+        const bool me_solid = solid && solid[c];
+        auto shut = [&](int xx, int yy, int zz) { return me_solid || (solid && solid[(size_t(zz) * n + yy) * n + xx]); };
+        const float ux0 = (x == 0 || shut(x - 1, y, z)) ? 0.f : float(double(u[ix0]) - dtd * (pc - pv(x - 1, y, z)) * hInv);
+        const float ux1 = (x + 1 == n || shut(x + 1, y, z)) ? 0.f : float(double(u[ix1]) - dtd * (pv(x + 1, y, z) - pc) * hInv);
+        const float vy0 = (y == 0 || shut(x, y - 1, z)) ? 0.f : float(double(v[iy0]) - dtd * (pc - pv(x, y - 1, z)) * hInv);
+        const float vy1 = (y + 1 == n || shut(x, y + 1, z)) ? 0.f : float(double(v[iy1]) - dtd * (pv(x, y + 1, z) - pc) * hInv);
+        const float wz0 = (z == 0 || shut(x, y, z - 1)) ? 0.f : float(double(w[iz0]) - dtd * (pc - pv(x, y, z - 1)) * hInv);
+        const float wz1 = (z + 1 == n || shut(x, y, z + 1)) ? 0.f : float(double(w[iz1]) - dtd * (pv(x, y, z + 1) - pc) * hInv);
         uo[ix0] = ux0;
         vo[iy0] = vy0;
         wo[iz0] = wz0;
@@ -905,9 +942,10 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
     count_launch();
     k_begin_projection<<<1, 1, 0, s>>>(ctrl, a.options, x64a, x64b);
     count_launch();
-    k_rhs<<<blocks, kThreads, 0, s>>>(a.g, scale, u, v, w, b, partials, ctrl);
+    k_rhs<<<blocks, kThreads, 0, s>>>(a.g, scale, u, v, w, b, partials, ctrl, a.solid);
     count_launch();
-    k_rhs_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, double(cells), a.options.absolute_tolerance,
+    k_rhs_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, a.solid ? a.fluid : double(cells),
+                                    a.options.absolute_tolerance,
                                     a.options.relative_tolerance, cond.active,
                                     (cudaGraphConditionalHandle)cond.handle);
 }
@@ -937,18 +975,18 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
         const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
         const int zb = sor_planes(n, bx);
         const dim3 grid(bx, (n + zb - 1) / zb);
-        if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
-        else if (exact) k_sor_rbz<true, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
-        else if (measure) k_sor_rbz<false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
-        else k_sor_rbz<false, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb);
+        if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        else if (exact) k_sor_rbz<true, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        else if (measure) k_sor_rbz<false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        else k_sor_rbz<false, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
     } else if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n);
-        if (exact) k_sor_rb<4, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
-        else k_sor_rb<4, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
+        if (exact) k_sor_rb<4, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, a.diag);
+        else k_sor_rb<4, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, a.diag);
     } else {
         const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n);
-        if (exact) k_sor_rb<1, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
-        else k_sor_rb<1, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m);
+        if (exact) k_sor_rb<1, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, a.diag);
+        else k_sor_rb<1, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, a.diag);
     }
 }
 
@@ -965,10 +1003,10 @@ static void refine_launch(const ProjectionArgs& a, const float* b, const float* 
     count_launch();
     if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n, 2);
-        k_refine_rb<4><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated);
+        k_refine_rb<4><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated, a.diag);
     } else {
         const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n, 2);
-        k_refine_rb<1><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated);
+        k_refine_rb<1><<<grid, kThreads, 0, s>>>(a.g, b, e, r32, ctrl, gated, a.diag);
     }
 }
 
@@ -990,10 +1028,10 @@ void launch_error_check(const ProjectionArgs& a, const float* e, const float* r3
         count_launch();
         if (L.hw % 4 == 0) {
             const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n, 1);
-            k_error_residual<4><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1);
+            k_error_residual<4><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1, a.diag);
         } else {
             const dim3 grid((L.hw * n + kThreads - 1) / kThreads, n, 1);
-            k_error_residual<1><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1);
+            k_error_residual<1><<<grid, kThreads, 0, s>>>(a.g, e, r32, ctrl, 1, a.diag);
         }
     }
     count_launch();
@@ -1030,9 +1068,9 @@ void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32,
     count_launch();
     k_psum64<<<blocks, kThreads, 0, s>>>(a.g, ctrl, partials);
     count_launch();
-    k_psum64_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, double(cells));
+    k_psum64_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, a.solid ? a.fluid : double(cells));
     count_launch();
-    k_residual64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, p32, ctrl);
+    k_residual64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, p32, ctrl, a.diag);
     count_launch();
     k_final_check<<<1, 1, 0, s>>>(ctrl);
 }
@@ -1043,7 +1081,7 @@ void launch_gradient64(const ProjectionArgs& a, const float* u_in, const float* 
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     count_launch();
     k_gradient64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, a.dt, u_in, v_in, w_in, u_out, v_out, w_out,
-                                                              u_hat, v_hat, w_hat, ctrl);
+                                                              u_hat, v_hat, w_hat, ctrl, a.solid);
 }
 
 void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,
