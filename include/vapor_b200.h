@@ -335,6 +335,27 @@ vapor_status vapor_advect_noalloc(int32_t n, float box, int32_t loc, float dt, f
                                   const float *flow_v, const float *flow_w, float *output,
                                   void *stream);
 
+/* Tuning (extension): z-planes per thread of the red-black colour sweep for
+ * grids of size n (0 = automatic: at least four waves of blocks). Results do
+ * not depend on it; set it before creating the simulations whose steps are
+ * recorded into graphs. vapor_b200/autotune.py measures and chooses it. */
+vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes);
+
+/* ---- Batched scenes (extension, no reference counterpart) ----
+ * Steps many resident simulations (uneven grid sizes allowed, each with its
+ * own parameters) with one CUDA-graph launch: every scene's whole step,
+ * tolerance-driven solve loops included, is a parallel branch of one graph,
+ * so small grids fill the GPU together. The batch orders itself after each
+ * scene's earlier work and each scene's later work after the batch; the
+ * scenes stay usable one by one (upload, download, diagnostics). The batch
+ * does not own the simulations: destroy it before them. */
+typedef struct vapor_batch vapor_batch;
+vapor_status vapor_batch_create(int32_t count, vapor_mac3d *const *sims, vapor_batch **out);
+vapor_status vapor_batch_destroy(vapor_batch *batch);
+vapor_status vapor_batch_advance(vapor_batch *batch, float dt);
+vapor_status vapor_batch_synchronize(vapor_batch *batch);
+vapor_status vapor_batch_stream(vapor_batch *batch, void **stream);
+
 /* ---- Learned warm start for the pressure solve ----
  * No counterpart in the reference, whose projection starts every solve from
  * zero pressure (CpuPressureSolver3D.cpp:46). The model is a fixed 3-level 3D

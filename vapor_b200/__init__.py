@@ -107,6 +107,12 @@ def _declare(lib):
     f("vapor_stage_set_solver_kind", _vp, C.c_int32)
     f("vapor_stage_stream", _vp, C.POINTER(_vp))
     f("vapor_stage_set_solid", _vp, _vp)
+    f("vapor_tune_sor_planes", C.c_int32, C.c_int32)
+    f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
+    f("vapor_batch_destroy", _vp)
+    f("vapor_batch_advance", _vp, C.c_float)
+    f("vapor_batch_synchronize", _vp)
+    f("vapor_batch_stream", _vp, C.POINTER(_vp))
     f("vapor_advect_noalloc", C.c_int32, C.c_float, C.c_int32, C.c_float, C.c_float, C.c_int32,
       _vp, _vp, _vp, _vp, _vp, _vp)
     f("vapor_unet_parameter_count", res=C.c_int64)
@@ -323,6 +329,40 @@ class MacSimulation3D:
         """Learned coarse-grid correction of the FPCG solver (None: smoothing only)."""
         check(library().vapor_mac3d_set_preconditioner(self._h, net.handle if net is not None else None))
         self._coarse = net
+
+
+def tune_sor_planes(n, planes):
+    """z-planes per thread of the colour sweep for grids of size n (0: automatic)."""
+    check(library().vapor_tune_sor_planes(int(n), int(planes)))
+
+
+class Batch:
+    """Steps several MacSimulation3D scenes with one CUDA-graph launch."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)  # keeps the scenes alive while batched
+        arr = (_vp * len(self.sims))(*[s.handle for s in self.sims])
+        h = _vp()
+        check(library().vapor_batch_create(len(self.sims), arr, C.byref(h)))
+        self._h = h
+
+    def advance(self, dt):
+        check(library().vapor_batch_advance(self._h, float(dt)))
+
+    def synchronize(self):
+        check(library().vapor_batch_synchronize(self._h))
+
+    def stream(self):
+        s = _vp()
+        check(library().vapor_batch_stream(self._h, C.byref(s)))
+        return s.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().vapor_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
 
 
 class StageBackend:

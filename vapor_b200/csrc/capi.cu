@@ -17,6 +17,10 @@ struct vapor_stage {
     vb::Stage stage;
     vapor_stage(int n, float box) : stage(n, box) {}
 };
+struct vapor_batch {
+    vb::Batch batch;
+    explicit vapor_batch(std::vector<vb::Simulation*> sims) : batch(std::move(sims)) {}
+};
 struct vapor_unet {
     vb::Stream stream;
     vb::unet::UNet net;
@@ -284,6 +288,49 @@ VB_API vapor_status vapor_stage_set_solid(vapor_stage* stage, const uint8_t* mas
 }
 VB_API vapor_status vapor_stage_stream(vapor_stage* stage, void** stream) {
     STAGE_GUARD(require(stream != nullptr, "null output"); *stream = (void*)stage->stage.stream());
+}
+
+VB_API vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes) {
+    return guarded([&] {
+        require(n > 0 && planes >= 0 && planes <= 64, "invalid tuning value");
+        vb::set_sor_planes(n, planes);
+    });
+}
+
+// ---- batched scenes ----
+VB_API vapor_status vapor_batch_create(int32_t count, vapor_mac3d* const* sims, vapor_batch** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output");
+        *out = nullptr;
+        require(count > 0 && sims != nullptr, "a batch needs at least one simulation");
+        std::vector<vb::Simulation*> v;
+        for (int32_t i = 0; i < count; ++i) {
+            require(sims[i] != nullptr, "null simulation in batch");
+            v.push_back(&sims[i]->sim);
+        }
+        *out = new vapor_batch(std::move(v));
+    });
+}
+VB_API vapor_status vapor_batch_destroy(vapor_batch* batch) {
+    return guarded([&] { delete batch; });
+}
+VB_API vapor_status vapor_batch_advance(vapor_batch* batch, float dt) {
+    return guarded([&] {
+        require(batch != nullptr, "null batch handle");
+        batch->batch.advance(dt);
+    });
+}
+VB_API vapor_status vapor_batch_synchronize(vapor_batch* batch) {
+    return guarded([&] {
+        require(batch != nullptr, "null batch handle");
+        batch->batch.synchronize();
+    });
+}
+VB_API vapor_status vapor_batch_stream(vapor_batch* batch, void** stream) {
+    return guarded([&] {
+        require(batch != nullptr && stream != nullptr, "null handle or output");
+        *stream = (void*)batch->batch.stream();
+    });
 }
 
 // ---- learned warm start ----

@@ -774,7 +774,7 @@ void Simulation::release_graphs() {
     }
 }
 
-void Simulation::advance(float dt) {
+void Simulation::prepare_step(float dt) {
     validate_step(dt);
     // Scratch that a captured step needs is allocated before any capture.
     {
@@ -802,6 +802,21 @@ void Simulation::advance(float dt) {
             coarse_->prepare(ws_.n() / 4);
         }
     }
+}
+
+void Simulation::record_step_for_batch(float dt) {
+    ws_.set_capturing(true);
+    try {
+        record_step(dt);
+    } catch (...) {
+        ws_.set_capturing(false);
+        throw;
+    }
+    ws_.set_capturing(false);
+}
+
+void Simulation::advance(float dt) {
+    prepare_step(dt);
     cudaStream_t s = ws_.stream();
     if (!use_graphs_ || ws_.timer().enabled()) {
         record_step(dt);
@@ -847,6 +862,104 @@ void Simulation::advance(float dt) {
     }
     VB_CUDA(cudaGraphLaunch(slot.exec, s));
     cur_ = 1 - cur_;
+}
+
+// ---- Batch: many scenes' steps in one CUDA graph -------------------------
+
+Batch::Batch(std::vector<Simulation*> sims) : sims_(std::move(sims)) {
+    if (sims_.empty()) fail(VAPOR_INVALID_ARGUMENT, "a batch needs at least one simulation");
+    for (size_t i = 0; i < sims_.size(); ++i) {
+        if (!sims_[i]) fail(VAPOR_INVALID_ARGUMENT, "null simulation in batch");
+        for (size_t j = 0; j < i; ++j)
+            if (sims_[j] == sims_[i]) fail(VAPOR_INVALID_ARGUMENT, "a simulation appears twice in the batch");
+    }
+    events_.resize(sims_.size() + 1, nullptr);
+    for (auto& e : events_) VB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+Batch::~Batch() {
+    if (stream_.s) cudaStreamSynchronize(stream_.s);
+    for (auto& g : graphs_)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& e : events_)
+        if (e) cudaEventDestroy(e);
+}
+
+// Orders stream `after` behind everything enqueued so far on `before`.
+void Batch::order(cudaStream_t before, cudaStream_t after, cudaEvent_t e) {
+    VB_CUDA(cudaEventRecord(e, before));
+    VB_CUDA(cudaStreamWaitEvent(after, e, 0));
+}
+
+void Batch::advance(float dt) {
+    for (Simulation* sim : sims_) sim->prepare_step(dt);
+    // Key: dt, and for every scene its step parity and graph key.
+    std::vector<uint8_t> key(sizeof(float));
+    std::memcpy(key.data(), &dt, sizeof(float));
+    for (Simulation* sim : sims_) {
+        const std::vector<uint8_t> k = sim->step_key(dt);
+        key.insert(key.end(), k.begin(), k.end());
+    }
+    Slot* slot = nullptr;
+    for (auto& g : graphs_)
+        if (g.exec && g.key == key) slot = &g;
+    cudaStream_t s = stream_.s;
+    // the batch launch waits for each scene's earlier work (uploads, resets)
+    for (size_t i = 0; i < sims_.size(); ++i) order(sims_[i]->stream(), s, events_[i]);
+    if (!slot) {
+        slot = &graphs_[next_];
+        next_ = 1 - next_;
+        if (slot->exec) {
+            cudaGraphExecDestroy(slot->exec);
+            slot->exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        VB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            // fork: every scene's stream joins the capture, records its step
+            // as a parallel branch, and joins back
+            VB_CUDA(cudaEventRecord(events_.back(), s));
+            for (Simulation* sim : sims_) VB_CUDA(cudaStreamWaitEvent(sim->stream(), events_.back(), 0));
+            for (Simulation* sim : sims_) sim->record_step_for_batch(dt);
+            for (size_t i = 0; i < sims_.size(); ++i) order(sims_[i]->stream(), s, events_[i]);
+        } catch (...) {
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            (void)cudaGetLastError();
+            throw;
+        }
+        VB_CUDA(cudaStreamEndCapture(s, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&slot->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            slot->exec = nullptr;
+            (void)cudaGetLastError();
+            VB_CUDA(e);
+        }
+        slot->key = key;
+    }
+    VB_CUDA(cudaGraphLaunch(slot->exec, s));
+    for (size_t i = 0; i < sims_.size(); ++i) {
+        sims_[i]->flip_after_batch();
+        order(s, sims_[i]->stream(), events_[i]);  // later per-scene work follows the batch
+    }
+}
+
+void Batch::synchronize() { VB_CUDA(cudaStreamSynchronize(stream_.s)); }
+
+std::vector<uint8_t> Simulation::step_key(float dt) const {
+    GraphKey key{};
+    key.dt = dt;
+    key.box = ws_.box();
+    key.params = params;
+    key.warm = warm_;
+    key.warm_buffers = warm_ ? warm_->generation() : 0ull;
+    key.coarse = coarse_;
+    key.coarse_buffers = coarse_ ? coarse_->generation() : 0ull;
+    std::vector<uint8_t> out(sizeof(GraphKey) + sizeof(int));
+    std::memcpy(out.data(), &key, sizeof(GraphKey));
+    std::memcpy(out.data() + sizeof(GraphKey), &cur_, sizeof(int));
+    return out;
 }
 
 void Simulation::upload(const float* d, const float* u, const float* v, const float* w) {

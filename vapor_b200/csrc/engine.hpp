@@ -182,6 +182,13 @@ public:
     void reset();
     void set_box(float box);
     void advance(float dt);
+    // Batched stepping (Batch): validation and scratch allocation before a
+    // capture, the step recorded into the current capture, the step's cache
+    // key, and the parity flip once a batch graph holding the step launched.
+    void prepare_step(float dt);
+    void record_step_for_batch(float dt);
+    std::vector<uint8_t> step_key(float dt) const;
+    void flip_after_batch() { cur_ = 1 - cur_; }
     void upload(const float* d, const float* u, const float* v, const float* w);
     void download(float* d, float* u, float* v, float* w);
     void synchronize();
@@ -248,6 +255,35 @@ private:
 };
 
 // Staged stage plugins on caller-owned spans (host or device).
+// Many scenes stepped by one CUDA-graph launch: each scene's whole step
+// (solve loops included) is a parallel branch of one graph, recorded from
+// the scenes' own streams, so independent grids of uneven sizes fill the GPU
+// together. Graphs are cached per dt, scene parameters and parities. The
+// batch does not own the simulations; destroy it first.
+class Batch {
+public:
+    explicit Batch(std::vector<Simulation*> sims);
+    ~Batch();
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    void advance(float dt);
+    void synchronize();
+    cudaStream_t stream() const { return stream_.s; }
+    size_t size() const { return sims_.size(); }
+
+private:
+    static void order(cudaStream_t before, cudaStream_t after, cudaEvent_t e);
+    struct Slot {
+        std::vector<uint8_t> key;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Simulation*> sims_;
+    Stream stream_;
+    std::vector<cudaEvent_t> events_;
+    Slot graphs_[2];
+    int next_ = 0;
+};
+
 class Stage {
 public:
     Stage(int n, float box);

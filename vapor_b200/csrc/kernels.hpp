@@ -135,6 +135,9 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
                       bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true,
                       bool measure = false);
 bool sor_fuses_measure(int n);
+// Autotuner hook: planes per thread of the z-marching colour sweep for grid
+// size n (planes <= 0 restores the automatic choice).
+void set_sor_planes(int n, int planes);
 // Mixed precision: x64[1-cur] = x64[cur] + e (FP64), r32 = float(b' - A x)
 // with the FP64 residual norm into ctrl->res_bits.
 void launch_refine_residual(const ProjectionArgs& a, const float* b, const float* e, float* r32,

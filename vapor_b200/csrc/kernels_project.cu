@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <map>
+#include <mutex>
 
 namespace vb {
 namespace {
@@ -955,8 +957,25 @@ bool sor_fuses_measure(int n) {
     return L.hw % 4 == 0 && 2 * L.stride < (size_t(1) << 31);
 }
 
-// Planes per thread of the z-marching sweep: at least 4 waves of blocks.
+// Planes per thread of the z-marching sweep chosen by the autotuner for a
+// grid size (0: automatic). Read when a sweep is launched or recorded.
+std::mutex g_tuning_mutex;
+std::map<int, int> g_sor_planes;
+
+void set_sor_planes(int n, int planes) {
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    if (planes <= 0) g_sor_planes.erase(n);
+    else g_sor_planes[n] = planes;
+}
+
+// Planes per thread of the z-marching sweep: the tuned value, else at least
+// 4 waves of blocks.
 static int sor_planes(int n, int blocks_x) {
+    {
+        std::lock_guard<std::mutex> lock(g_tuning_mutex);
+        const auto it = g_sor_planes.find(n);
+        if (it != g_sor_planes.end()) return std::max(1, std::min(it->second, n));
+    }
     const long target_blocks = 148L * 5 * 4;
     const long per_plane = long(blocks_x);
     int zb = int(std::max(1L, (per_plane * n) / target_blocks));
