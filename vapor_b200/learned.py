@@ -189,6 +189,30 @@ def train_coarse(net, n=64, rollouts=8, steps=60, random_pairs=1, lr=1e-3, lr_fi
     return history
 
 
+def train_random(net, n=64, pairs=2000, slopes=(-3.0, 0.0), lr=1e-3, lr_final=1e-4, seed=0, log=None):
+    """Trains the coarse-grid network on projections of seeded random velocity
+    fields only (spectral slope drawn from `slopes`, random solenoidal and
+    gradient mix): a broad right-hand-side distribution, so the network learns
+    the coarse Poisson inverse rather than the shapes of one flow."""
+    stage = StageBackend(n, 1.0)
+    stage.set_solver_kind(SOLVER_MIXED_REFINEMENT)
+    opts = ProjectionOptions(DT, omega_for(n), LinearSolveOptions.defaults(
+        max_iterations=20000, relative_tolerance=1e-6, absolute_tolerance=0.0))
+    rng = np.random.default_rng(seed + 424242)
+    history = []
+    t0 = time.perf_counter()
+    for k in range(pairs):
+        u, v, w = spectral_fields(n, int(rng.integers(1 << 31)), slope=float(rng.uniform(*slopes)),
+                                  gradient_fraction=float(rng.uniform(0.2, 1.0)))
+        stage.project(u, v, w, opts, 6.0)
+        history.append(stage.train_network(net, _lr(k, pairs, lr, lr_final)))
+        if log and (k % 100 == 0 or k == pairs - 1):
+            log(json.dumps({"pair": k, "loss": float(np.mean(history[-50:])),
+                            "elapsed_s": round(time.perf_counter() - t0, 1)}))
+    stage.close()
+    return history
+
+
 def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6, phases=False,
                  arms=("sor", "fpcg", "fpcg_learned")):
     """Per-step sweeps/iterations and device time on the benchmark plume for
@@ -292,6 +316,16 @@ def main():
     tc.add_argument("--lr", type=float, default=1e-3)
     tc.add_argument("--lr-final", type=float, default=1e-4)
     tc.add_argument("--seed", type=int, default=0)
+    tr = sub.add_parser("train-random")
+    tr.add_argument("--out", default=COARSE_WEIGHTS)
+    tr.add_argument("--init", default=None)
+    tr.add_argument("--n", type=int, default=64)
+    tr.add_argument("--pairs", type=int, default=2000)
+    tr.add_argument("--slope-min", type=float, default=-3.0)
+    tr.add_argument("--slope-max", type=float, default=0.0)
+    tr.add_argument("--lr", type=float, default=1e-3)
+    tr.add_argument("--lr-final", type=float, default=1e-4)
+    tr.add_argument("--seed", type=int, default=0)
     cf = sub.add_parser("compare-fpcg")
     cf.add_argument("--weights", default=COARSE_WEIGHTS)
     cf.add_argument("--n", type=int, default=256)
@@ -299,6 +333,7 @@ def main():
     cf.add_argument("--steps", type=int, default=3)
     cf.add_argument("--phases", action="store_true", help="add a per-phase breakdown of one eager step")
     cf.add_argument("--arms", default="sor,fpcg,fpcg_learned")
+    cf.add_argument("--seed", type=int, default=2024)
     bn = sub.add_parser("bench-net")
     bn.add_argument("--n", type=int, default=64)
     bn.add_argument("--reps", type=int, default=20)
@@ -322,12 +357,18 @@ def main():
         net.save(args.out)
         tail = hist[-50:] if hist else [float("nan")]
         print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(tail))}))
+    elif args.cmd == "train-random":
+        net = WarmStartNet.load(args.init) if args.init else WarmStartNet(seed=args.seed)
+        hist = train_random(net, n=args.n, pairs=args.pairs, slopes=(args.slope_min, args.slope_max), lr=args.lr,
+                            lr_final=args.lr_final, seed=args.seed, log=print)
+        net.save(args.out)
+        print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(hist[-50:]))}))
     elif args.cmd == "bench-net":
         print(json.dumps(bench_net(n=args.n, reps=args.reps)))
     elif args.cmd == "compare-fpcg":
         net = WarmStartNet.load(args.weights) if os.path.exists(args.weights) else WarmStartNet(seed=0)
         print(json.dumps(compare_fpcg(net, n=args.n, warmup=args.warmup, steps=args.steps, phases=args.phases,
-                                      arms=tuple(args.arms.split(",")))))
+                                      arms=tuple(args.arms.split(",")), seed=args.seed)))
     else:
         net = WarmStartNet.load(args.weights)
         print(json.dumps(compare(net, n=args.n, warmup=args.warmup, steps=args.steps)))
