@@ -407,6 +407,18 @@ vapor_status vapor_mac3d_evaluate_warm_start(vapor_mac3d *sim, vapor_unet *net, 
  * simulation or stage at a time (its activation buffers are shared state). */
 vapor_status vapor_mac3d_set_preconditioner(vapor_mac3d *sim, vapor_unet *net);
 vapor_status vapor_stage_set_preconditioner(vapor_stage *stage, vapor_unet *net);
+/* Training data for the coarse-grid network: every FPCG coarse right-hand
+ * side ((n/4)^3 floats, natural layout) of later steps of `sim` is copied to
+ * record (*counter % capacity) of the device ring `log`, then *counter is
+ * incremented on the device. NULL log and counter disable it. */
+vapor_status vapor_mac3d_set_coarse_log(vapor_mac3d *sim, float *log, int32_t capacity, int32_t *counter);
+/* Mixed-precision solve of A x = rhs on the stage's grid for a given
+ * right-hand side (device memory, n^3 floats, x fastest; its mean is removed
+ * as for a projection); the zero-mean solution into `pressure` (device, may
+ * be NULL). The stage keeps (rhs, x) for vapor_stage_train_network. */
+vapor_status vapor_stage_solve_rhs(vapor_stage *stage, const float *rhs,
+                                   const vapor_projection_options *options, float diagonal_floor,
+                                   vapor_projection_result *result, float *pressure);
 /* One Adam step of `net` on the stage's last projection (its right-hand side
  * and converged pressure, on the stage's own n^3 grid); the loss as for
  * vapor_mac3d_train_warm_start. Used to train the coarse-grid network on

@@ -103,3 +103,55 @@ def test_trained_coarse_network_cuts_the_iterations():
     assert plain["converged"] and learned["converged"]
     assert learned["final_relative_residual"] <= 1e-6
     assert learned["iterations_per_step"] <= 0.6 * plain["iterations_per_step"], out
+
+
+def test_solve_rhs_and_coarse_log():
+    """The training hooks: a stage solve of a given right-hand side meets the
+    FP64 tolerance (checked again here in FP64), and the FPCG solver logs one
+    coarse right-hand side per preconditioner application."""
+    import torch
+    from vapor_b200.learned import WarmStartNet
+    n = 16
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((n, n, n)).astype(np.float32)
+    rhs -= rhs.mean(dtype=np.float64)
+    stage = vb.StageBackend(n, 1.0)
+    opts = ProjectionOptions(0.01, 1.9, LinearSolveOptions.defaults(max_iterations=20000, relative_tolerance=1e-8,
+                                                                    absolute_tolerance=0.0))
+    b = torch.from_numpy(rhs).cuda()
+    p = torch.zeros_like(b)
+    r = stage.solve_rhs(b.data_ptr(), opts, 6.0, p.data_ptr())
+    assert r.linear_solve.converged
+    assert r.linear_solve.final_residual <= 1e-8 * r.linear_solve.initial_residual
+    x = p.cpu().numpy().astype(np.float64)
+    ax = 6.0 * x
+    cnt = np.full(x.shape, 6.0)
+    for axis in range(3):
+        for side in (0, -1):
+            idx = [slice(None)] * 3
+            idx[axis] = side
+            cnt[tuple(idx)] -= 1
+    ax = cnt * x
+    for axis in range(3):
+        ax -= np.roll(x, 1, axis) * (np.arange(n) > 0).reshape([-1 if a == axis else 1 for a in range(3)])
+        ax -= np.roll(x, -1, axis) * (np.arange(n) < n - 1).reshape([-1 if a == axis else 1 for a in range(3)])
+    # the returned pressure is the FP64 solution rounded to FP32
+    res = np.abs(rhs.astype(np.float64) - rhs.astype(np.float64).mean() - ax).max()
+    assert res <= 1e-5 * np.abs(rhs).max()
+
+    prm = algorithm_params(3)
+    prm.use_solve_options = 1
+    prm.solve = LinearSolveOptions.defaults(max_iterations=500, relative_tolerance=1e-6, absolute_tolerance=0.0)
+    prm.solver_kind = vb.abi.SOLVER_FPCG
+    sim = vb.MacSimulation3D(32, 1.0, prm)
+    net = WarmStartNet(seed=4)
+    sim.set_preconditioner(net)
+    log = torch.zeros((64, 8 ** 3), dtype=torch.float32, device="cuda")
+    counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sim.set_coarse_log(log.data_ptr(), 64, counter.data_ptr())
+    sim.advance(0.01)
+    sim.synchronize()
+    its = sim.last_projection().linear_solve.iterations
+    assert int(counter.item()) >= its + 1  # every application, two projections per Reflection step
+    assert float(log[0].abs().max()) > 0
+    sim.set_coarse_log(None, 0, None)

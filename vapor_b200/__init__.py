@@ -107,6 +107,8 @@ def _declare(lib):
     f("vapor_stage_set_solver_kind", _vp, C.c_int32)
     f("vapor_stage_stream", _vp, C.POINTER(_vp))
     f("vapor_stage_set_solid", _vp, _vp)
+    f("vapor_stage_solve_rhs", _vp, _vp, C.POINTER(ProjectionOptions), C.c_float, C.POINTER(ProjectionResult), _vp)
+    f("vapor_mac3d_set_coarse_log", _vp, _vp, C.c_int32, _vp)
     f("vapor_tune_sor_planes", C.c_int32, C.c_int32)
     f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_batch_destroy", _vp)
@@ -325,6 +327,10 @@ class MacSimulation3D:
         check(library().vapor_mac3d_evaluate_warm_start(self._h, net.handle, C.byref(loss)))
         return loss.value
 
+    def set_coarse_log(self, log_ptr, capacity, counter_ptr):
+        """Copies every FPCG coarse right-hand side into a device ring (0/None disables)."""
+        check(library().vapor_mac3d_set_coarse_log(self._h, log_ptr or None, int(capacity), counter_ptr or None))
+
     def set_preconditioner(self, net):
         """Learned coarse-grid correction of the FPCG solver (None: smoothing only)."""
         check(library().vapor_mac3d_set_preconditioner(self._h, net.handle if net is not None else None))
@@ -417,6 +423,13 @@ class StageBackend:
         check(library().vapor_stage_project(self._h, *ptrs, C.byref(options), float(diagonal_floor), C.byref(r),
                                             p.ctypes.data if p is not None else None))
         return r, p
+
+    def solve_rhs(self, rhs_ptr, options, diagonal_floor=6.0, pressure_ptr=None):
+        """Mixed-precision solve of A x = rhs (device pointer, n^3 floats); returns the result."""
+        r = ProjectionResult()
+        check(library().vapor_stage_solve_rhs(self._h, rhs_ptr, C.byref(options), float(diagonal_floor), C.byref(r),
+                                              pressure_ptr))
+        return r
 
     def project_device(self, u_ptr, v_ptr, w_ptr, options, diagonal_floor=0.0, pressure_ptr=None):
         """The same projection on device pointers (in place); returns the result."""

@@ -286,6 +286,12 @@ VB_API vapor_status vapor_stage_set_solver_kind(vapor_stage* stage, int32_t kind
 VB_API vapor_status vapor_stage_set_solid(vapor_stage* stage, const uint8_t* mask) {
     STAGE_GUARD(stage->stage.set_solid(mask));
 }
+VB_API vapor_status vapor_stage_solve_rhs(vapor_stage* stage, const float* rhs_device,
+                                          const vapor_projection_options* options, float diagonal_floor,
+                                          vapor_projection_result* result, float* pressure_device) {
+    STAGE_GUARD(require(options != nullptr, "null options");
+                stage->stage.solve_rhs(rhs_device, *options, diagonal_floor, result, pressure_device));
+}
 VB_API vapor_status vapor_stage_stream(vapor_stage* stage, void** stream) {
     STAGE_GUARD(require(stream != nullptr, "null output"); *stream = (void*)stage->stage.stream());
 }
@@ -398,6 +404,12 @@ VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float*
 }
 VB_API vapor_status vapor_mac3d_set_warm_start(vapor_mac3d* sim, vapor_unet* net) {
     SIM_GUARD(sim->sim.set_warm_start(net ? &net->net : nullptr));
+}
+VB_API vapor_status vapor_mac3d_set_coarse_log(vapor_mac3d* sim, float* log_device, int32_t capacity,
+                                               int32_t* counter_device) {
+    SIM_GUARD(require((log_device == nullptr) == (counter_device == nullptr), "log and counter go together");
+              require(log_device == nullptr || capacity > 0, "capacity must be positive");
+              sim->sim.set_coarse_log(log_device, capacity, counter_device));
 }
 VB_API vapor_status vapor_mac3d_set_preconditioner(vapor_mac3d* sim, vapor_unet* net) {
     SIM_GUARD(sim->sim.set_preconditioner(net ? &net->net : nullptr));

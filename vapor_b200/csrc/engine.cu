@@ -330,6 +330,8 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
             launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
+            if (coarse_log_)
+                launch_log_coarse(cg_rc_.p, cg_rc_.n, coarse_log_, coarse_log_capacity_, coarse_log_counter_, st);
             coarse->set_stream(st);
             const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
             coarse->set_stream(s);
@@ -392,7 +394,7 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
 void Workspace::project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo,
                         float* uh, float* vh, float* wh, float dt, float omega, float diagonal_floor,
                         const vapor_linear_solve_options& o, int solver_kind, unet::UNet* warm,
-                        unet::UNet* coarse) {
+                        unet::UNet* coarse, const float* rhs_field) {
     ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
     if (fluid_ > 0.0) {
         if (solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
@@ -443,7 +445,7 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     LoopCond rhs_cond = cond;
     if (mixed) rhs_cond.active = 0;  // the mixed loop is decided by its first re-centring pass
     launch_rhs(a, ui, vi, wi, b_.p, partials_.p, partial_capacity_, ctrl_, mixed ? x64_[0].p : nullptr,
-               mixed ? x64_[1].p : nullptr, rhs_cond, s);
+               mixed ? x64_[1].p : nullptr, rhs_cond, s, rhs_field);
     VB_CUDA(cudaMemsetAsync(p_.p, 0, p_.bytes(), s));
     t.end(VAPOR_PHASE_RHS, 3);
 
@@ -451,7 +453,7 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
         project_fpcg(a, warm, coarse, cond, handle);
         t.begin(VAPOR_PHASE_GRADIENT);
         launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
-        launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        if (ui) launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
         t.end(VAPOR_PHASE_GRADIENT, 5);
     } else if (mixed) {
         // FP32 red-black sweeps on the error equation A e = r32. Every check
@@ -503,7 +505,7 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
         }
         t.begin(VAPOR_PHASE_GRADIENT);
         launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
-        launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
+        if (ui) launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
         t.end(VAPOR_PHASE_GRADIENT, 5);
     } else {
         if (warm) warm->infer_into(n_, b_.p, ctrl_, p_.p, nullptr);  // x0 = network prediction
@@ -1017,6 +1019,25 @@ static bool overlaps(const float* a, size_t na, const float* b, size_t nb) {
 }
 
 // Projection3D::project contract (CpuPressureSolver3D.cpp:25-33, SOR.cpp:15-27).
+void Stage::solve_rhs(const float* rhs_device, const vapor_projection_options& o, float floor_diag,
+                      vapor_projection_result* result, float* pressure_device) {
+    if (!rhs_device) fail(VAPOR_INVALID_ARGUMENT, "a right-hand side is required");
+    if (!std::isfinite(o.relaxation) || o.relaxation <= 0.f || o.relaxation >= 2.f)
+        fail(VAPOR_INVALID_ARGUMENT, "SOR relaxation factor must be between 0 and 2");
+    if (!valid_options(o.linear_solve)) fail(VAPOR_INVALID_ARGUMENT, "Invalid linear solve options");
+    ws_.clear_errors();
+    ws_.ensure_mixed();
+    ws_.project(nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 1.f, o.relaxation,
+                floor_diag, o.linear_solve, VAPOR_SOLVER_MIXED_REFINEMENT, nullptr, nullptr, rhs_device);
+    const vapor_projection_result r = ws_.last_result();
+    if (pressure_device) {
+        launch_unsplit_pressure(ws_.grid(), ws_.pressure(), ws_.control(), pressure_device, ws_.stream());
+        VB_CUDA(cudaGetLastError());
+    }
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+    if (result) *result = r;
+}
+
 void Stage::project(float* u, float* v, float* w, const vapor_projection_options& o, float floor_diag,
                     vapor_projection_result* result, float* pressure_out, bool device_pointers) {
     const Grid g = ws_.grid();

@@ -109,7 +109,15 @@ public:
     void project(const float* ui, const float* vi, const float* wi, float* uo, float* vo, float* wo, float* uh,
                  float* vh, float* wh, float dt, float omega, float diagonal_floor,
                  const vapor_linear_solve_options& options, int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR,
-                 unet::UNet* warm_start = nullptr, unet::UNet* coarse = nullptr);
+                 unet::UNet* warm_start = nullptr, unet::UNet* coarse = nullptr,
+                 const float* rhs_field = nullptr);
+    // Logs every FPCG coarse right-hand side into a device ring (training data
+    // for the coarse network); null disables. See launch_log_coarse.
+    void set_coarse_log(float* log, int capacity, int* counter) {
+        coarse_log_ = log;
+        coarse_log_capacity_ = capacity;
+        coarse_log_counter_ = counter;
+    }
     float* rhs() { return b_.p; }
     void advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
                 const float* w, float* out, float post_scale);
@@ -154,6 +162,9 @@ private:
     DevArray<uint8_t> solid_;           // natural-layout solid mask (obstacles)
     DevArray<uint8_t> solid_diag_;      // split-layout fluid-neighbour counts, 0 = solid
     double fluid_ = 0.0;                // fluid cells when a mask is set, else 0
+    float* coarse_log_ = nullptr;       // FPCG coarse right-hand-side ring (device), optional
+    int coarse_log_capacity_ = 0;
+    int* coarse_log_counter_ = nullptr;
     CgControl* cg_ = nullptr;           // device
     int partial_capacity_ = 0;
     ProjControl* ctrl_ = nullptr;       // device
@@ -189,6 +200,11 @@ public:
     void record_step_for_batch(float dt);
     std::vector<uint8_t> step_key(float dt) const;
     void flip_after_batch() { cur_ = 1 - cur_; }
+    void set_coarse_log(float* log, int capacity, int* counter) {
+        VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+        release_graphs();
+        ws_.set_coarse_log(log, capacity, counter);
+    }
     void upload(const float* d, const float* u, const float* v, const float* w);
     void download(float* d, float* u, float* v, float* w);
     void synchronize();
@@ -294,7 +310,12 @@ public:
     void reset();
     int solver_kind = VAPOR_SOLVER_RED_BLACK_SOR;
     unet::UNet* coarse = nullptr;
-    void set_solid(const uint8_t* mask) { ws_.set_solid(mask); }  // FPCG coarse-grid network (bound to this stage's stream per call)
+    void set_solid(const uint8_t* mask) { ws_.set_solid(mask); }
+    // Mixed-precision solve of A x = rhs for a given right-hand side (device,
+    // natural layout, n^3); the pressure (zero mean) into pressure_device if
+    // given. The workspace keeps (b, x) for network training.
+    void solve_rhs(const float* rhs_device, const vapor_projection_options& o, float floor_diag,
+                   vapor_projection_result* result, float* pressure_device);  // FPCG coarse-grid network (bound to this stage's stream per call)
     void project(float* u, float* v, float* w, const vapor_projection_options& options, float diagonal_floor,
                  vapor_projection_result* result, float* pressure_out, bool device_pointers);
     void advect(int loc, float dt, float cfl, int method, const float* src, const float* fu, const float* fv,

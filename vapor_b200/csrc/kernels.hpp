@@ -121,7 +121,8 @@ struct LoopCond {
 // x64a/x64b are the mixed-precision buffers (may be null).
 void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const float* w, float* b,
                 double* partials, int partial_capacity, ProjControl* ctrl, double* x64a, double* x64b,
-                LoopCond cond, cudaStream_t s);
+                LoopCond cond, cudaStream_t s,
+                const float* field = nullptr);
 // One red-black colour sweep over x (parity 0 updates i+j+k even). With
 // `subtract_mean` the right-hand side is b - ctrl->rhs_mean_f, else b. A
 // guarded sweep returns at once when the solve is done or when
@@ -219,6 +220,9 @@ void launch_cg_direction(size_t count, float* p, const float* z, const CgControl
 // rc = 4^3 block sums of r - A z on the (n/4)^3 grid (natural layout); n % 4 == 0.
 // `rows` holds n^3 / 4 floats of scratch.
 void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s);
+// Appends the coarse right-hand side (cells floats) to a device ring of
+// `capacity` records: record *counter % capacity, then ++*counter.
+void launch_log_coarse(const float* rc, size_t cells, float* log, int capacity, int* counter, cudaStream_t s);
 // z += gamma (P zc - mean zc), gamma by the Galerkin condition on the coarse grid.
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
                               cudaStream_t s);

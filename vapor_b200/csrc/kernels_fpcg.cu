@@ -439,6 +439,15 @@ __global__ void __launch_bounds__(kThreads) k_prolong_add(int n, float* __restri
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_log_coarse(const float* __restrict__ rc, size_t cells,
+                                                         float* __restrict__ log, int capacity,
+                                                         const int* __restrict__ counter) {
+    const size_t slot = size_t(*counter % capacity);
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cells; i += size_t(gridDim.x) * blockDim.x)
+        log[slot * cells + i] = rc[i];
+}
+__global__ void k_log_advance(int* counter) { *counter += 1; }
+
 int blocks_for(size_t count) {
     return int(std::min<size_t>((count + kThreads - 1) / kThreads, size_t(kDotBlocks)));
 }
@@ -526,6 +535,13 @@ void launch_restrict_residual(int n, const float* r, const float* z, float* rows
     else k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
     count_launch();
     k_restrict_blocks<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, rows, rc);
+}
+
+void launch_log_coarse(const float* rc, size_t cells, float* log, int capacity, int* counter, cudaStream_t s) {
+    count_launch();
+    k_log_coarse<<<blocks_for(cells), kThreads, 0, s>>>(rc, cells, log, capacity, counter);
+    count_launch();
+    k_log_advance<<<1, 1, 0, s>>>(counter);
 }
 
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,

@@ -72,7 +72,8 @@ __global__ void k_begin_projection(ProjControl* ctrl, vapor_linear_solve_options
 __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const float* __restrict__ u,
                                                   const float* __restrict__ v, const float* __restrict__ w,
                                                   float* __restrict__ b, double* __restrict__ partials,
-                                                  ProjControl* ctrl, const uint8_t* __restrict__ solid) {
+                                                  ProjControl* ctrl, const uint8_t* __restrict__ solid,
+                                                  const float* __restrict__ field) {
     __shared__ double s_sum[32];
     __shared__ float s_max[32];
     __shared__ int s_key[32];
@@ -88,6 +89,16 @@ __global__ void __launch_bounds__(kThreads) k_rhs(Grid g, float scale, const flo
         decode_cell(c, n, x, y, z);
         if (solid && solid[c]) {  // not an unknown: b = 0, outside every reduction
             b[rb_index(L, x, y, z)] = 0.f;
+            continue;
+        }
+        if (field) {  // a given right-hand side (natural layout) instead of a divergence
+            const float rhs = field[c];
+            if (!isfinite(rhs)) bad = 1u;
+            b[rb_index(L, x, y, z)] = rhs;
+            sum += double(rhs);
+            const int key = float_order_key(rhs);
+            kmax = max(kmax, key);
+            kmin = min(kmin, key);
             continue;
         }
         // faces on walls or touching a solid are closed (read as zero)
@@ -937,14 +948,14 @@ int reduction_blocks(size_t count) {
 
 void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const float* w, float* b,
                 double* partials, int partial_capacity, ProjControl* ctrl, double* x64a, double* x64b,
-                LoopCond cond, cudaStream_t s) {
+                LoopCond cond, cudaStream_t s, const float* field) {
     const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
     const int blocks = std::min(reduction_blocks(cells), partial_capacity);
     const float scale = a.g.h * a.g.h / a.dt;
     count_launch();
     k_begin_projection<<<1, 1, 0, s>>>(ctrl, a.options, x64a, x64b);
     count_launch();
-    k_rhs<<<blocks, kThreads, 0, s>>>(a.g, scale, u, v, w, b, partials, ctrl, a.solid);
+    k_rhs<<<blocks, kThreads, 0, s>>>(a.g, scale, u, v, w, b, partials, ctrl, a.solid, field);
     count_launch();
     k_rhs_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, a.solid ? a.fluid : double(cells),
                                     a.options.absolute_tolerance,

@@ -213,6 +213,65 @@ def train_random(net, n=64, pairs=2000, slopes=(-3.0, 0.0), lr=1e-3, lr_final=1e
     return history
 
 
+def train_onpolicy(net, n=256, rounds=4, warmup=3, steps=3, capacity=512, random_per_record=0.25, lr=3e-4,
+                   lr_final=3e-5, seed=0, log=None):
+    """Fine-tunes the coarse-grid network on the inputs it actually receives:
+    each round runs seeded plume steps at n with the FPCG solver and the
+    current network, logging every coarse right-hand side ((n/4)^3), then
+    solves each logged right-hand side on the coarse grid with the plain
+    mixed-precision solver and takes one Adam step on the pair; a fraction of
+    random spectral pairs keeps the network general."""
+    import torch
+    nc = n // 4
+    stage = StageBackend(nc, 1.0)
+    stage.set_solver_kind(SOLVER_MIXED_REFINEMENT)
+    opts = ProjectionOptions(DT, omega_for(nc), LinearSolveOptions.defaults(
+        max_iterations=20000, relative_tolerance=1e-6, absolute_tolerance=0.0))
+    buf = torch.zeros((capacity, nc ** 3), dtype=torch.float32, device="cuda")
+    counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rng = np.random.default_rng(seed + 777)
+    history, k = [], 0
+    total = rounds * capacity * (1 + random_per_record)
+    t0 = time.perf_counter()
+    for rnd in range(rounds):
+        sc = training_scene(seed * 7919 + 1000 + rnd)
+        p = scene_params(default_params(), n, rel=1e-6, max_iterations=20000, sources=sc["sources"],
+                         radius=sc["radius"], buoyancy=sc["buoyancy"])
+        p.solver_kind = SOLVER_FPCG
+        sim = MacSimulation3D(n, 1.0, p)
+        sim.upload(*swirl_fields(n, sc["swirl_seed"]))
+        sim.set_preconditioner(net)
+        for _ in range(warmup):
+            sim.advance(DT)
+        counter.zero_()
+        sim.synchronize()
+        sim.set_coarse_log(buf.data_ptr(), capacity, counter.data_ptr())
+        for _ in range(steps):
+            sim.advance(DT)
+        sim.synchronize()
+        sim.set_coarse_log(None, 0, None)
+        its = sim.last_projection().linear_solve.iterations
+        sim.set_preconditioner(None)
+        sim.close()
+        count = min(int(counter.item()), capacity)
+        for i in rng.permutation(count):
+            stage.solve_rhs(buf[int(i)].data_ptr(), opts)
+            history.append(stage.train_network(net, _lr(k, total, lr, lr_final)))
+            k += 1
+            if rng.random() < random_per_record:
+                u, v, w = spectral_fields(nc, int(rng.integers(1 << 31)), slope=float(rng.uniform(-3.0, 0.0)),
+                                          gradient_fraction=float(rng.uniform(0.2, 1.0)))
+                stage.project(u, v, w, opts, 6.0)
+                history.append(stage.train_network(net, _lr(k, total, lr, lr_final)))
+                k += 1
+        if log:
+            log(json.dumps({"round": rnd, "records": count, "last_cg_iterations": its,
+                            "loss": float(np.mean(history[-50:])) if history else None,
+                            "elapsed_s": round(time.perf_counter() - t0, 1)}))
+    stage.close()
+    return history
+
+
 def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6, phases=False,
                  arms=("sor", "fpcg", "fpcg_learned")):
     """Per-step sweeps/iterations and device time on the benchmark plume for
@@ -326,6 +385,16 @@ def main():
     tr.add_argument("--lr", type=float, default=1e-3)
     tr.add_argument("--lr-final", type=float, default=1e-4)
     tr.add_argument("--seed", type=int, default=0)
+    op = sub.add_parser("train-onpolicy")
+    op.add_argument("--out", default=COARSE_WEIGHTS)
+    op.add_argument("--init", default=COARSE_WEIGHTS)
+    op.add_argument("--n", type=int, default=256)
+    op.add_argument("--rounds", type=int, default=4)
+    op.add_argument("--steps", type=int, default=3)
+    op.add_argument("--capacity", type=int, default=512)
+    op.add_argument("--lr", type=float, default=3e-4)
+    op.add_argument("--lr-final", type=float, default=3e-5)
+    op.add_argument("--seed", type=int, default=0)
     cf = sub.add_parser("compare-fpcg")
     cf.add_argument("--weights", default=COARSE_WEIGHTS)
     cf.add_argument("--n", type=int, default=256)
@@ -363,6 +432,13 @@ def main():
                             lr_final=args.lr_final, seed=args.seed, log=print)
         net.save(args.out)
         print(json.dumps({"saved": args.out, "pairs": len(hist), "final_loss_mean50": float(np.mean(hist[-50:]))}))
+    elif args.cmd == "train-onpolicy":
+        net = WarmStartNet.load(args.init)
+        hist = train_onpolicy(net, n=args.n, rounds=args.rounds, steps=args.steps, capacity=args.capacity,
+                              lr=args.lr, lr_final=args.lr_final, seed=args.seed, log=print)
+        net.save(args.out)
+        print(json.dumps({"saved": args.out, "pairs": len(hist),
+                          "final_loss_mean50": float(np.mean(hist[-50:])) if hist else None}))
     elif args.cmd == "bench-net":
         print(json.dumps(bench_net(n=args.n, reps=args.reps)))
     elif args.cmd == "compare-fpcg":
