@@ -62,57 +62,62 @@ __global__ void __launch_bounds__(kThreads) k_apply_A(int n, const float* __rest
 }
 
 // Row-pair access (n % 8 == 0): thread t owns slots 4j..4j+3 of both colours
-// in row (y, z), i.e. the 8 cells x = 8j .. 8j+7; cell x = 8j + m has colour
-// (x + y + z) & 1 and slot 4j + (m >> 1). Loads are float4 per colour and
-// row, index arithmetic is 32-bit, and no thread divides 64-bit values.
-struct RowPair {
-    float v[2][4];  // [colour][slot - 4j]
+// in row (y, z), i.e. the 8 cells x = 8j .. 8j+7. In that row the cells with
+// even x have colour (y + z) & 1, those with odd x the other colour, so the
+// two colour rows are read as E (even x: cell 8j + 2k) and O (odd x: cell
+// 8j + 2k + 1) by swapping row pointers: every register index is static.
+// Loads are float4 per colour and row, index arithmetic is 32-bit.
+struct RowEO {
+    float e[4], o[4];
 };
-__device__ __forceinline__ RowPair load_pair(const float* __restrict__ a, int stride, int off) {
-    RowPair p;
-    const float4 c0 = *reinterpret_cast<const float4*>(a + off);
-    const float4 c1 = *reinterpret_cast<const float4*>(a + stride + off);
-    p.v[0][0] = c0.x; p.v[0][1] = c0.y; p.v[0][2] = c0.z; p.v[0][3] = c0.w;
-    p.v[1][0] = c1.x; p.v[1][1] = c1.y; p.v[1][2] = c1.z; p.v[1][3] = c1.w;
-    return p;
+__device__ __forceinline__ RowEO load_eo(const float* __restrict__ a, int stride, int off, int sy) {
+    const float* even = a + (sy ? stride : 0) + off;  // colour (y + z) & 1 holds the even x
+    const float* odd = a + (sy ? 0 : stride) + off;
+    const float4 ev = *reinterpret_cast<const float4*>(even);
+    const float4 od = *reinterpret_cast<const float4*>(odd);
+    RowEO r;
+    r.e[0] = ev.x; r.e[1] = ev.y; r.e[2] = ev.z; r.e[3] = ev.w;
+    r.o[0] = od.x; r.o[1] = od.y; r.o[2] = od.z; r.o[3] = od.w;
+    return r;
 }
-__device__ __forceinline__ RowPair zero_pair() {
-    RowPair p;
+__device__ __forceinline__ RowEO zero_eo() {
+    RowEO r;
 #pragma unroll
-    for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) p.v[c][k] = 0.f;
-    return p;
+    for (int k = 0; k < 4; ++k) r.e[k] = r.o[k] = 0.f;
+    return r;
 }
 
-// (A a) at the 8 cells of a row pair, in the residual's operation order:
-// count * a, minus x-, x+, y-, y+, z-, z+ (missing neighbours skipped).
+// (A a) at the 8 cells of a row pair (out[m] for x = 8j + m), in the
+// residual's operation order: count * a, minus x-, x+, y-, y+, z-, z+
+// (missing neighbours skipped). The x-parity split is the same in every row,
+// so the y and z neighbours of an even cell are the neighbour rows' even cells.
 __device__ __forceinline__ void apply_pair(const float* __restrict__ a, int n, int hw, int j, int y, int z,
                                            float out[8]) {
     const int plane = n * hw, stride = n * plane;
     const int off = z * plane + y * hw + 4 * j;
-    const RowPair me = load_pair(a, stride, off);
-    const RowPair ym = y > 0 ? load_pair(a, stride, off - hw) : zero_pair();
-    const RowPair yp = y + 1 < n ? load_pair(a, stride, off + hw) : zero_pair();
-    const RowPair zm = z > 0 ? load_pair(a, stride, off - plane) : zero_pair();
-    const RowPair zp = z + 1 < n ? load_pair(a, stride, off + plane) : zero_pair();
+    const RowEO me = load_eo(a, stride, off, (y + z) & 1);
+    const RowEO ym = y > 0 ? load_eo(a, stride, off - hw, (y + z - 1) & 1) : zero_eo();
+    const RowEO yp = y + 1 < n ? load_eo(a, stride, off + hw, (y + z + 1) & 1) : zero_eo();
+    const RowEO zm = z > 0 ? load_eo(a, stride, off - plane, (y + z - 1) & 1) : zero_eo();
+    const RowEO zp = z + 1 < n ? load_eo(a, stride, off + plane, (y + z + 1) & 1) : zero_eo();
     const int x0 = 8 * j;
-    // x-neighbours outside the run: cell x0 - 1 (slot 4j - 1) and x0 + 8 (slot 4j + 4)
-    const float left = x0 > 0 ? a[((x0 - 1 + y + z) & 1) * stride + off - 1] : 0.f;
-    const float right = x0 + 8 < n ? a[((x0 + 8 + y + z) & 1) * stride + off + 4] : 0.f;
+    // x-neighbours outside the run: cell x0 - 1 (odd, slot 4j - 1) and x0 + 8 (even, slot 4j + 4)
+    const int sy = (y + z) & 1;
+    const float left = x0 > 0 ? a[(sy ? 0 : stride) + off - 1] : 0.f;
+    const float right = x0 + 8 < n ? a[(sy ? stride : 0) + off + 4] : 0.f;
     const int nyz = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-        const int x = x0 + m;
-        const int c = (x + y + z) & 1, k = m >> 1;
-        const float v = me.v[c][k];
+        const int x = x0 + m, k = m >> 1;
+        const bool even = (m & 1) == 0;
+        const float v = even ? me.e[k] : me.o[k];
         float ax = float((x > 0) + (x + 1 < n) + nyz) * v;
-        if (x > 0) ax -= m > 0 ? me.v[1 - c][(m - 1) >> 1] : left;
-        if (x + 1 < n) ax -= m < 7 ? me.v[1 - c][(m + 1) >> 1] : right;
-        if (y > 0) ax -= ym.v[1 - c][k];
-        if (y + 1 < n) ax -= yp.v[1 - c][k];
-        if (z > 0) ax -= zm.v[1 - c][k];
-        if (z + 1 < n) ax -= zp.v[1 - c][k];
+        if (x > 0) ax -= even ? (m > 0 ? me.o[k - 1 < 0 ? 0 : k - 1] : left) : me.e[k];
+        if (x + 1 < n) ax -= even ? me.o[k] : (m < 7 ? me.e[k + 1 > 3 ? 3 : k + 1] : right);
+        if (y > 0) ax -= even ? ym.e[k] : ym.o[k];
+        if (y + 1 < n) ax -= even ? yp.e[k] : yp.o[k];
+        if (z > 0) ax -= even ? zm.e[k] : zm.o[k];
+        if (z + 1 < n) ax -= even ? zp.e[k] : zp.o[k];
         out[m] = ax;
     }
 }
@@ -131,18 +136,14 @@ __global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __
         float q[8];
         apply_pair(ps, n, hw, j, y, z, q);
         const int off = z * plane + y * hw + 4 * j;
-        float o[2][4];
+        const int sy = (y + z) & 1;
+        float* qe = qs + (sy ? stride : 0) + off;  // even-x cells of this row
+        float* qo = qs + (sy ? 0 : stride) + off;
+        const RowEO pp = load_eo(ps, stride, off, sy);
+        *reinterpret_cast<float4*>(qe) = make_float4(q[0], q[2], q[4], q[6]);
+        *reinterpret_cast<float4*>(qo) = make_float4(q[1], q[3], q[5], q[7]);
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int c = (8 * j + m + y + z) & 1;
-            o[c][m >> 1] = q[m];
-        }
-        const float4 p0 = *reinterpret_cast<const float4*>(ps + off);
-        const float4 p1 = *reinterpret_cast<const float4*>(ps + stride + off);
-        *reinterpret_cast<float4*>(qs + off) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
-        *reinterpret_cast<float4*>(qs + stride + off) = make_float4(o[1][0], o[1][1], o[1][2], o[1][3]);
-        acc += double(p0.x) * o[0][0] + double(p0.y) * o[0][1] + double(p0.z) * o[0][2] + double(p0.w) * o[0][3];
-        acc += double(p1.x) * o[1][0] + double(p1.y) * o[1][1] + double(p1.z) * o[1][2] + double(p1.w) * o[1][3];
+        for (int k = 0; k < 4; ++k) acc += double(pp.e[k]) * q[2 * k] + double(pp.o[k]) * q[2 * k + 1];
     }
     const double b = block_sum(acc, s_sum);
     if (threadIdx.x == 0) {
@@ -164,13 +165,10 @@ __global__ void __launch_bounds__(kThreads) k_restrict_pairs(int n, const float*
     if (y >= n) return;
     float az[8];
     apply_pair(zs, n, hw, j, y, z, az);
-    const RowPair rr = load_pair(r, stride, z * plane + y * hw + 4 * j);
+    const RowEO rr = load_eo(r, stride, z * plane + y * hw + 4 * j, (y + z) & 1);
     float sum[2] = {0.f, 0.f};
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const int c = (8 * j + m + y + z) & 1;
-        sum[m >> 2] += rr.v[c][m >> 1] - az[m];
-    }
+    for (int m = 0; m < 8; ++m) sum[m >> 2] += ((m & 1) ? rr.o[m >> 1] : rr.e[m >> 1]) - az[m];
     const int base = (z * n + y) * nc + 2 * j;
     rows[base] = sum[0];
     rows[base + 1] = sum[1];
