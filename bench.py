@@ -195,6 +195,11 @@ def run_reference(args):
 REFERENCE_SWEEPS_PER_STEP = 6000
 
 
+# DRAM bytes (read 100.70 MB + written 10.73 MB) of one k_sor_rbz colour
+# launch at 256^3, from an ncu --set full capture on the benchmark plume.
+SOR_TRAFFIC_256 = 100.695296e6 + 10.727936e6
+
+
 def network_flops(nc):
     """FLOPs of one U-Net forward on an nc^3 grid: the ten 3x3x3 convolutions
     (27 taps x cin x cout multiply-adds per voxel of their level)."""
@@ -323,7 +328,10 @@ def main():
         nbytes = 6.0 * cells
         achieved = nbytes / (launch_ms * 1e-3) / 1e9
         return {"bound": "hbm", "kernel": "k_sor_rbz (red-black colour sweep)", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": SOR_TRAFFIC_256 * cells / 256 ** 3,
+                "traffic_note": "dram bytes read + written per launch from an ncu --set full capture at 256^3, "
+                                "scaled by cells for other sizes",
                 "bytes_per_launch": nbytes, "avg_launch_us": launch_ms * 1e3}
 
     # Network (tensor cores): FLOPs of the coarse U-Net per application over
