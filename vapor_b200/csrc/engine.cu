@@ -321,9 +321,11 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     t.end(VAPOR_PHASE_RESIDUAL, 2);
     auto precondition = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_SOR);
-        VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
+        // the first colour sweep starts from z = 0 (and clears the other colour)
+        const bool fused_start = sor_fuses_measure(n_);
+        if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
         for (int j = 0; j < kFpcgSmoothing; ++j) {
-            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false, fused_start && j == 0);
             launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
         }
         t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);

@@ -132,9 +132,12 @@ void launch_rhs(const ProjectionArgs& a, const float* u, const float* v, const f
 // `measure` (colour 1 only) also records max |b' - off - diag x| of the updated
 // cells into ctrl->res32_bits when sor_fuses_measure(n); otherwise
 // launch_error_check measures the same value in a separate pass.
+// `from_zero` (fast relaxation without measuring, z-marching kernel only):
+// the sweep starts from x = 0 and also writes the other colour as 0, so x
+// needs no clearing first. Callers check sor_fuses_measure(n).
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, ProjControl* ctrl,
                       bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true,
-                      bool measure = false);
+                      bool measure = false, bool from_zero = false);
 bool sor_fuses_measure(int n);
 // Autotuner hook: planes per thread of the z-marching colour sweep for grid
 // size n (planes <= 0 restores the automatic choice).

@@ -278,7 +278,10 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
 // which leaves the reference's sum unchanged (x + (-1 * 0) == x bitwise for
 // every x, including signed zeros), so results equal k_sor_rb's bit for bit.
 // Needs hw % 4 == 0 and 2 * n^2 * hw < 2^31.
-template <bool EXACT, bool RESID>
+// FROM_ZERO: the sweep starts from x = 0 (both colours): the other colour is
+// not read but written as 0, and the own colour is not read (0 + (b - 0 -
+// d * 0) * w == 0 + b * w). Replaces clearing x and the first colour sweep.
+template <bool EXACT, bool RESID, bool FROM_ZERO = false>
 __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
                                                       RelaxTable wr, float* __restrict__ xs,
                                                       const float* __restrict__ bs, ProjControl* ctrl,
@@ -306,19 +309,23 @@ __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, flo
         const int nyz = int(has_ym) + int(has_yp);
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
         auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
-        float4 cm = z0 > 0 ? ld4(oth + (z0 - 1) * plane) : zero4;
-        float4 cc = ld4(oth + z0 * plane);
+        float4 cm = (!FROM_ZERO && z0 > 0) ? ld4(oth + (z0 - 1) * plane) : zero4;
+        float4 cc = FROM_ZERO ? zero4 : ld4(oth + z0 * plane);
         const float w3 = wr.w[3], w4 = wr.w[4], w5 = wr.w[5], w6 = wr.w[6];
         for (int z = z0; z < z1; ++z) {
             const int zoff = z * plane;
-            const float4 cp = z + 1 < n ? ld4(oth + zoff + plane) : zero4;
-            const float4 m4 = has_ym ? ld4(oth + zoff - hw) : zero4;
-            const float4 p4 = has_yp ? ld4(oth + zoff + hw) : zero4;
-            const float4 a4 = ld4(own + zoff);
+            const float4 cp = (!FROM_ZERO && z + 1 < n) ? ld4(oth + zoff + plane) : zero4;
+            const float4 m4 = (!FROM_ZERO && has_ym) ? ld4(oth + zoff - hw) : zero4;
+            const float4 p4 = (!FROM_ZERO && has_yp) ? ld4(oth + zoff + hw) : zero4;
+            const float4 a4 = FROM_ZERO ? zero4 : ld4(own + zoff);
+            if (FROM_ZERO) *reinterpret_cast<float4*>(const_cast<float*>(oth) + zoff) = zero4;
             const float4 b4 = __ldg(reinterpret_cast<const float4*>(rhs + zoff));
             const int sh = (y + z + colour) & 1;
             float xl[5];
-            if (sh == 0) {
+            if (FROM_ZERO) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) xl[k] = 0.f;
+            } else if (sh == 0) {
                 xl[0] = i0 > 0 ? oth[zoff - 1] : 0.f;
                 xl[1] = cc.x; xl[2] = cc.y; xl[3] = cc.z; xl[4] = cc.w;
             } else {
@@ -994,7 +1001,8 @@ static int sor_planes(int n, int blocks_x) {
 }
 
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, ProjControl* ctrl,
-                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact, bool measure) {
+                      bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact, bool measure,
+                      bool from_zero) {
     const int n = a.g.n;
     const RBLayout L = rb_layout(n);
     RelaxTable wr;
@@ -1005,7 +1013,9 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
         const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
         const int zb = sor_planes(n, bx);
         const dim3 grid(bx, (n + zb - 1) / zb);
-        if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        if (from_zero && !exact && !measure)
+            k_sor_rbz<false, false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        else if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
         else if (exact) k_sor_rbz<true, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
         else if (measure) k_sor_rbz<false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
         else k_sor_rbz<false, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
