@@ -281,8 +281,10 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
 // FROM_ZERO: the sweep starts from x = 0 (both colours): the other colour is
 // not read but written as 0, and the own colour is not read (0 + (b - 0 -
 // d * 0) * w == 0 + b * w). Replaces clearing x and the first colour sweep.
-template <bool EXACT, bool RESID, bool FROM_ZERO = false>
-__global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
+// PLAIN: no solid mask and n even (selected by the launcher), which allows
+// the interior-x form of the update below.
+template <bool EXACT, bool RESID, bool FROM_ZERO = false, bool PLAIN = false>
+__global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
                                                       RelaxTable wr, float* __restrict__ xs,
                                                       const float* __restrict__ bs, ProjControl* ctrl,
                                                       int guarded, int sweep_index, int subtract_mean, int zb,
@@ -339,40 +341,73 @@ __global__ void __launch_bounds__(kThreads, 5) k_sor_rbz(Grid g, int colour, flo
             const float zm[4] = {cm.x, cm.y, cm.z, cm.w};
             const float zp[4] = {cp.x, cp.y, cp.z, cp.w};
             const int ny = nyz + int(z > 0) + int(z + 1 < n);
-            uchar4 dm = make_uchar4(0, 0, 0, 0);
-            if (dg) dm = *reinterpret_cast<const uchar4*>(dg + zoff);
-            const int dmask[4] = {dm.x, dm.y, dm.z, dm.w};
             float res[4];
+            if (PLAIN) {
+                // No mask, n even: every slot is a cell, the neighbours outside
+                // the box were loaded as 0 (adding -1 * 0 leaves the sum's bits
+                // unchanged), and only cell 0 at x = 0 and cell 3 at x = n - 1
+                // have one x-neighbour less. Same operations as the general path.
+                const int d0 = 2 + ny;
+                const float diag0 = float(d0), diag1 = float(d0 - 1);
+                const float w0 = EXACT ? maxf_ref(diag0, floor_diag) : wr.w[d0];
+                const float w1 = EXACT ? maxf_ref(diag1, floor_diag) : wr.w[d0 - 1];
+                const bool ledge = i0 == 0 && sh == 0, redge = i0 + 4 >= hw && sh == 1;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int xc = 2 * (i0 + k) + sh;
-                const bool left = xc > 0, right = xc + 1 < n;
-                // solid neighbours hold 0, so summing them changes nothing
-                const int d = dg ? dmask[k] : int(left) + int(right) + ny;
-                const float diag = float(d);
-                float off = 0.f;
-                off += -1.f * (left ? xl[k] : 0.f);
-                off += -1.f * (right ? xl[k + 1] : 0.f);
-                off += -1.f * ym[k];
-                off += -1.f * yp[k];
-                off += -1.f * zm[k];
-                off += -1.f * zp[k];
-                const float bi = subtract_mean ? bv[k] - bm : bv[k];
-                float r;
-                if (EXACT) {
-                    const float relax = maxf_ref(diag, floor_diag);
-                    r = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
-                } else {
-                    const float w = d == 6 ? w6 : (d == 5 ? w5 : (d == 4 ? w4 : w3));
-                    r = xo[k] + (bi - off - diag * xo[k]) * w;
+                for (int k = 0; k < 4; ++k) {
+                    const bool edge = (k == 0 && ledge) || (k == 3 && redge);
+                    const float diag = edge ? diag1 : diag0;
+                    float off = 0.f;
+                    off += -1.f * xl[k];
+                    off += -1.f * xl[k + 1];
+                    off += -1.f * ym[k];
+                    off += -1.f * yp[k];
+                    off += -1.f * zm[k];
+                    off += -1.f * zp[k];
+                    const float bi = subtract_mean ? bv[k] - bm : bv[k];
+                    float r;
+                    if (EXACT) r = xo[k] + omega * (bi - off - diag * xo[k]) / (edge ? w1 : w0);
+                    else r = xo[k] + (bi - off - diag * xo[k]) * (edge ? w1 : w0);
+                    res[k] = r;
+                    if (RESID) {
+                        const float rr = bi - off - diag * r;
+                        rmax = fmaxf(rmax, fabsf(rr));
+                    }
                 }
-                const bool valid = xc < n && d > 0;
-                res[k] = valid ? r : xo[k];
-                if (RESID && valid) {
-                    // residual of this cell after its update: the other
-                    // colour (all its neighbours) does not change in this sweep
-                    const float rr = bi - off - diag * r;
-                    rmax = fmaxf(rmax, fabsf(rr));
+            } else {  // general form: any n, optional solid mask
+                uchar4 dm = make_uchar4(0, 0, 0, 0);
+                if (dg) dm = *reinterpret_cast<const uchar4*>(dg + zoff);
+                const int dmask[4] = {dm.x, dm.y, dm.z, dm.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int xc = 2 * (i0 + k) + sh;
+                    const bool left = xc > 0, right = xc + 1 < n;
+                    // solid neighbours hold 0, so summing them changes nothing
+                    const int d = dg ? dmask[k] : int(left) + int(right) + ny;
+                    const float diag = float(d);
+                    float off = 0.f;
+                    off += -1.f * (left ? xl[k] : 0.f);
+                    off += -1.f * (right ? xl[k + 1] : 0.f);
+                    off += -1.f * ym[k];
+                    off += -1.f * yp[k];
+                    off += -1.f * zm[k];
+                    off += -1.f * zp[k];
+                    const float bi = subtract_mean ? bv[k] - bm : bv[k];
+                    float r;
+                    if (EXACT) {
+                        const float relax = maxf_ref(diag, floor_diag);
+                        r = xo[k] + omega * (bi - off - diag * xo[k]) / relax;
+                    } else {
+                        const float w = d == 6 ? w6 : (d == 5 ? w5 : (d == 4 ? w4 : w3));
+                        r = xo[k] + (bi - off - diag * xo[k]) * w;
+                    }
+                    const bool valid = xc < n && d > 0;
+                    res[k] = valid ? r : xo[k];
+                    if (RESID && valid) {
+                        // residual of this cell after its update: the other
+                        // colour (all its neighbours) does not change in this sweep
+                        const float rr = bi - off - diag * r;
+                        rmax = fmaxf(rmax, fabsf(rr));
+                    }
                 }
             }
             *reinterpret_cast<float4*>(own + zoff) = make_float4(res[0], res[1], res[2], res[3]);
@@ -1013,12 +1048,27 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
         const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
         const int zb = sor_planes(n, bx);
         const dim3 grid(bx, (n + zb - 1) / zb);
-        if (from_zero && !exact && !measure)
-            k_sor_rbz<false, false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
-        else if (exact && measure) k_sor_rbz<true, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
-        else if (exact) k_sor_rbz<true, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
-        else if (measure) k_sor_rbz<false, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
-        else k_sor_rbz<false, false><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, zb, a.diag);
+        const bool plain = a.diag == nullptr && n % 2 == 0;
+#define VB_SOR_RBZ(E, R, Z, P)                                                                                \
+    k_sor_rbz<E, R, Z, P><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, \
+                                                    sweep_index, m, zb, a.diag)
+        if (from_zero && !exact && !measure) {
+            if (plain) VB_SOR_RBZ(false, false, true, true);
+            else VB_SOR_RBZ(false, false, true, false);
+        } else if (exact && measure) {
+            if (plain) VB_SOR_RBZ(true, true, false, true);
+            else VB_SOR_RBZ(true, true, false, false);
+        } else if (exact) {
+            if (plain) VB_SOR_RBZ(true, false, false, true);
+            else VB_SOR_RBZ(true, false, false, false);
+        } else if (measure) {
+            if (plain) VB_SOR_RBZ(false, true, false, true);
+            else VB_SOR_RBZ(false, true, false, false);
+        } else {
+            if (plain) VB_SOR_RBZ(false, false, false, true);
+            else VB_SOR_RBZ(false, false, false, false);
+        }
+#undef VB_SOR_RBZ
     } else if (L.hw % 4 == 0) {
         const dim3 grid((L.hw / 4 * n + kThreads - 1) / kThreads, n);
         if (exact) k_sor_rb<4, true><<<grid, kThreads, 0, s>>>(a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, g, sweep_index, m, a.diag);
