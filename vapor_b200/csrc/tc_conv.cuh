@@ -1,21 +1,12 @@
-// 3x3x3 convolution as an implicit GEMM on the 5th-generation tensor cores
-// (tcgen05, sm_100a): BF16 operands staged in shared memory, FP32 accumulator
-// in tensor memory (TMEM), one elected thread issues the MMAs.
-//
-//   out[v, co] = act( bias[co] + sum_{tap, ci} in[v + tap, ci] * w[tap][co][ci] )
-//
-// GEMM view: M = 128 consecutive voxels (linear x-fastest order, any grid
-// shape), N = C_out (16, 32 or 64), K = 27 taps x C_in in chunks of 16
-// channels. Activations are channels-last BF16 with a channel stride; out of
-// range neighbours read as zero (zero padding). Each K step stages
-//   A: 128 x 16 BF16 (the shifted voxel rows of one channel chunk) and
-//   B: N x 16 BF16 (the tap's weights for that chunk)
-// in the canonical no-swizzle K-major layout (8-row core matrices of 16 bytes:
-// element (r, k) at (r/8)*256 + (k/8)*128 + (r%8)*16 + (k%8)*2, i.e. stride
-// byte offset 256, leading byte offset 128), double-buffered so the copy of
-// step s+1 overlaps the MMA of step s. Stage reuse waits on an mbarrier that
-// tcgen05.commit arrives on; every wait is bounded and a timeout sets an error
-// flag instead of spinning.
+// PTX helpers for the tcgen05 convolutions of the learned network
+// (unet_kernels.cu): cp.async staging with zero fill, mbarriers with bounded
+// waits, tensor-memory allocation, shared-memory matrix descriptors of the
+// canonical K-major layout without swizzle (8-row core matrices of 16-byte
+// rows; the descriptor carries the byte distance between the two K halves,
+// LBO, and between consecutive 8-row groups, SBO), the BF16 instruction
+// descriptor, tcgen05.mma / commit and tcgen05.ld. One elected thread issues
+// the MMAs; FP32 accumulators live in tensor memory. Every wait is bounded and
+// reports a timeout instead of spinning.
 #pragma once
 
 #include <cuda_bf16.h>

@@ -1,12 +1,15 @@
-// Kernels of the learned pressure warm start: a 3-level 3D U-Net
-// (16/32/64 channels, 3x3x3 convolutions, BF16 weights and activations, FP32
-// accumulation) and its training (backward + Adam).
+// Kernels of the learned pressure components: a 3-level 3D U-Net (16/32/64
+// channels, 3x3x3 convolutions, BF16 weights and activations, FP32
+// accumulation), its inference as warm start or FPCG coarse-grid correction,
+// and its training (backward + Adam).
 //
 // The 3x3x3 convolutions - forward, and backward with respect to the input
 // (a convolution with the spatially flipped, channel-transposed weights) - run
-// on the tensor cores through k_conv3_tc (PTX helpers in tc_conv.cuh). Weight gradients,
-// pooling, upsampling, the 1x1 output head, the loss and Adam are memory-bound
-// or small and run on CUDA cores.
+// on the tensor cores: k_conv3_zm (z-marching, weights resident) when the
+// layer's weights and halo ring fit in shared memory, else k_conv3_tc (one
+// plane per CTA, channel chunks streamed); PTX helpers in tc_conv.cuh. Weight
+// gradients, pooling, upsampling, the 1x1 output head, the loss and Adam are
+// memory-bound or small and run on CUDA cores.
 #include <cuda_bf16.h>
 
 #include <algorithm>

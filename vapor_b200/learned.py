@@ -1,5 +1,5 @@
-"""Learned warm start for the pressure solve: network handle, training from
-plain-solver plume rollouts, and the sweep-count comparison.
+"""Learned pressure components: network handle, training drivers and the
+comparisons against the plain solver.
 
 The network is the library's 3-level 3D U-Net (16/32/64 channels, 3x3x3
 convolutions on tcgen05 tensor cores, BF16 weights and activations, FP32
@@ -12,13 +12,18 @@ tolerance, so the plain solver remains both the fallback and the judge.
   python -m vapor_b200.learned compare --weights weights.npy [--n 256 --steps 4]
   python -m vapor_b200.learned train-coarse --out coarse.npy [--n 64 --rollouts 8 --steps 60]
   python -m vapor_b200.learned compare-fpcg --weights coarse.npy [--n 256 --steps 3]
+  python -m vapor_b200.learned train-random --out coarse.npy [--n 64 --pairs 3000]
+  python -m vapor_b200.learned train-onpolicy --init coarse.npy --out coarse.npy [--n 256 --rounds 4]
+  python -m vapor_b200.learned bench-net [--n 64]
 
 The same network also serves as the coarse-grid correction of the flexible
 PCG solver (VAPOR_SOLVER_FPCG): applied on the grid coarsened 4x per axis to
 the restricted residual, scaled by the Galerkin condition, prolonged and
 smoothed. For that role it is trained at the coarse resolution (64^3 for a
-256^3 solve) on plume projections and on projections of seeded random
-velocity fields with a k^-5/3 spectrum.
+256^3 solve): first on projections of seeded random velocity fields
+(train-random), then on the coarse right-hand sides the solver actually feeds
+it, logged during FPCG solves and solved on the coarse grid by the plain
+solver (train-onpolicy).
 """
 import argparse
 import ctypes as C
