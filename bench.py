@@ -46,7 +46,7 @@ METRIC = "256^3 steps/s: learned-warm-start vs plain GPU solve at rel div 1e-6; 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256)
@@ -73,16 +73,22 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.mark = 0
 
     def start(self):
         exe = shutil.which("nvidia-smi")
         if not exe:
             return
         self.proc = subprocess.Popen([exe, f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                      "--format=csv,noheader,nounits", "-lms", "50"],
                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # the timed region starts once the sampler is live; earlier samples are dropped
+        deadline = time.perf_counter() + 5.0
+        while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.mark = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -98,7 +104,8 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = self.lines[self.mark:] or self.lines[-1:]
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -195,9 +202,9 @@ def run_reference(args):
 REFERENCE_SWEEPS_PER_STEP = 6000
 
 
-# DRAM bytes (read 100.70 MB + written 10.73 MB) of one k_sor_rbz colour
+# DRAM bytes (read 100.67 MB + written 10.11 MB) of one k_sor_rbz colour
 # launch at 256^3, from an ncu --set full capture on the benchmark plume.
-SOR_TRAFFIC_256 = 100.695296e6 + 10.727936e6
+SOR_TRAFFIC_256 = 100.673536e6 + 10.114048e6
 
 
 def network_flops(nc):

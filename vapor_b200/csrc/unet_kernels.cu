@@ -36,6 +36,70 @@ struct TmemColumns {
     static constexpr int value = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
 };
 
+// The 27 MMAs (M = 128, N, K = 16) of one 16-channel chunk into the
+// accumulator at TMEM address d. a_desc addresses the chunk's halo rows of
+// plane z-1; the planes z and z+1 sit dz_bytes[1], dz_bytes[2] further; rows
+// (next y) are 320 bytes apart and the 10 voxels of a row 16 bytes apart. b_desc
+// addresses tap 0 of the chunk's weights, taps N * 32 bytes apart. Descriptor
+// addresses are in 16-byte units in the low bits, so an offset is a plain add.
+template <int N>
+__device__ __forceinline__ void issue_taps(uint32_t d, uint64_t a_desc, const uint32_t (&dz_bytes)[3],
+                                           uint64_t b_desc, uint32_t idesc, bool accumulate) {
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int t = dz * 9 + dy * 3 + dx;
+                const uint64_t ad = a_desc + ((dz_bytes[dz] + uint32_t(dy * 320 + dx * 16)) >> 4);
+                const uint64_t bd = b_desc + uint32_t(t * N * 2);  // t * N * 32 bytes
+                tc::mma_bf16(d, ad, bd, idesc, accumulate || t > 0);
+            }
+}
+
+// Epilogue of one tile of 128 voxels (8 x by 16 y in plane z): accumulator
+// columns [0, N) at TMEM address acc, plus bias, optional ReLU, into the
+// output (BF16 or FP32, out_stride channels per voxel from out_offset). Warp w
+// reads TMEM lanes 32 (w & 3) .. + 31 (voxel m = lane index, x = m & 7,
+// y = m >> 3) and the column half w >> 2, 8 columns (16 or 32 bytes) a store.
+template <int N>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t acc, const float* s_bias, int x0, int y0,
+                                              int z, int warp, int lane) {
+    constexpr int kHalf = N / 2;
+    const int q = warp & 3, h = warp >> 2;
+    const int m = q * 32 + lane;
+    const int x = x0 + (m & 7), y = y0 + (m >> 3);
+    const bool vin = x < a.W && y < a.H;
+    const long v = (long(z) * a.H + y) * a.W + x;
+    const uint32_t lane_base = uint32_t(q * 32) << 16;
+#pragma unroll
+    for (int j = 0; j < kHalf / 8; ++j) {
+        const int c0 = h * kHalf + j * 8;
+        float val[8];
+        tc::tmem_ld8(acc + lane_base + uint32_t(c0), val);
+        if (vin) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                val[i] += s_bias[c0 + i];
+                if (a.relu) val[i] = fmaxf(val[i], 0.f);
+            }
+            const long o = v * a.out_stride + a.out_offset + c0;
+            if (a.out_fp32) {
+                float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.out) + o);
+                dst[0] = make_float4(val[0], val[1], val[2], val[3]);
+                dst[1] = make_float4(val[4], val[5], val[6], val[7]);
+            } else {
+                __align__(16) __nv_bfloat16 hv[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) hv[i] = __float2bfloat16_rn(val[i]);
+                *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o) =
+                    *reinterpret_cast<const uint4*>(hv);
+            }
+        }
+    }
+}
+
 // Implicit-GEMM 3x3x3 convolution on tcgen05 with a halo tile in shared
 // memory. A CTA computes M = 128 voxels: 8 consecutive x by 16 consecutive y
 // in one z plane (row m = 8 * yi + xi, TMEM lane m). For each 16-channel
@@ -79,10 +143,10 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     const int stages = (T::kTwoStages && chunks > 1) ? 2 : 1;
 
     if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
-    const uint32_t bar_addr[2] = {tc::smem_addr(&bars[0]), tc::smem_addr(&bars[1])};
+    const uint32_t bar0 = tc::smem_addr(&bars[0]);  // stage st's barrier at bar0 + 8 st
     if (tid == 0) {
-        tc::mbar_init(bar_addr[0], 1);
-        tc::mbar_init(bar_addr[1], 1);
+        tc::mbar_init(bar0, 1);
+        tc::mbar_init(bar0 + 8, 1);
         tc::fence_mbarrier_init();
     }
     for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
@@ -93,15 +157,16 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
     const uint32_t sbase = tc::smem_addr(smem);
     bool ok = true;
-    int issued[2] = {0, 0};  // commits per stage (phase tracking)
+    int issued0 = 0, issued1 = 0;  // commits per stage (phase tracking)
 
     for (int cc = 0; cc < chunks; ++cc) {
         const int st = stages == 2 ? (cc & 1) : 0;
         const uint32_t abase = sbase + uint32_t(st * T::kStage);
         const uint32_t bbase = abase + T::kA;
         // the stage's previous MMAs must be done before it is overwritten
-        if (issued[st] > 0) {
-            const bool mine = tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
+        const int before = st ? issued1 : issued0;
+        if (before > 0) {
+            const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(before - 1) & 1u, kWaitLimit);
             if (!__syncthreads_and(mine)) {
                 ok = false;
                 break;
@@ -126,64 +191,29 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
         __syncthreads();
         if (tid == 0) {
             tc::tc_fence_after();
-#pragma unroll 1
-            for (int t = 0; t < 27; ++t) {
-                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-                const uint32_t a_addr = abase + uint32_t((dz * 18 + dy) * T::kRowBytes + dx * 16);
-                const uint32_t b_addr = bbase + uint32_t(t * N * 32);
-                tc::mma_bf16(tmem, tc::smem_desc(a_addr, 160, T::kRowBytes), tc::smem_desc(b_addr, 128, 256),
-                             idesc, cc > 0 || t > 0);
-            }
-            tc::mma_commit(bar_addr[st]);
+            constexpr uint32_t kDz[3] = {0u, 18u * T::kRowBytes, 36u * T::kRowBytes};
+            issue_taps<N>(tmem, tc::smem_desc(abase, 160, T::kRowBytes), kDz, tc::smem_desc(bbase, 128, 256), idesc,
+                          cc > 0);
+            tc::mma_commit(bar0 + uint32_t(8 * st));
         }
-        ++issued[st];
+        if (st) ++issued1;
+        else ++issued0;
     }
     if (ok) {
         // the last commit covers every earlier MMA of this thread
         const int st = stages == 2 ? ((chunks - 1) & 1) : 0;
-        const bool mine = tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
+        const int commits = st ? issued1 : issued0;
+        const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(commits - 1) & 1u, kWaitLimit);
         ok = __syncthreads_and(mine);
     }
     tc::tc_fence_after();
     if (ok) {
-        if (warp < 4) {
-            const int m = warp * 32 + lane;
-            const int x = x0 + (m & 7), y = y0 + (m >> 3);
-            const bool vin = x < a.W && y < a.H;
-            const long v = (long(z) * a.H + y) * a.W + x;
-            const uint32_t lane_base = uint32_t(warp * 32) << 16;
-#pragma unroll
-            for (int c0 = 0; c0 < N; c0 += 16) {
-                float acc[16];
-                tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
-                if (vin) {
-                    float val[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        val[i] = acc[i] + s_bias[c0 + i];
-                        if (a.relu) val[i] = fmaxf(val[i], 0.f);
-                    }
-                    const long o = v * a.out_stride + a.out_offset + c0;
-                    if (a.out_fp32) {
-                        float* dst = static_cast<float*>(a.out) + o;
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) dst[i] = val[i];
-                    } else {
-                        __align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(val[i]);
-                        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o);
-                        dst[0] = reinterpret_cast<const uint4*>(h)[0];
-                        dst[1] = reinterpret_cast<const uint4*>(h)[1];
-                    }
-                }
-            }
-        }
+        conv_epilogue<N>(a, tmem, s_bias, x0, y0, z, warp, lane);
     } else {
         if (tid == 0) atomicOr(a.error, 1u);
         // drain: wait (bounded) for every commit still in flight
-        for (int st = 0; st < stages; ++st)
-            if (issued[st] > 0) tc::mbar_wait(bar_addr[st], uint32_t(issued[st] - 1) & 1u, kWaitLimit);
+        if (issued0 > 0) tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
+        if (issued1 > 0) tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -192,24 +222,29 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
 
 // The same convolution marching in z: a CTA computes zt consecutive planes of
 // its 8 x 16 tile. All of the layer's weights stay in shared memory
-// ([chunk][tap][N/8][2][8][16 B]) and the input halo is a ring of 4 planes
+// ([chunk][tap][N/8][2][8][16 B]) and the input halo is a ring of planes
 // (each [chunk][18 rows][320 B] as above), so every input plane is loaded
-// once per CTA instead of three times per output plane, and plane z + 2
-// loads while plane z's 27 x chunks MMAs and epilogue run. Used when the
-// weights and the ring fit in shared memory (ConvMarch<N>::fits).
+// once per CTA. Two TMEM accumulators alternate between planes: the MMAs of
+// plane z + 1 are issued before the epilogue of plane z drains the other
+// accumulator. The ring has `ring` = 4 or 6 planes: the MMAs of planes z and
+// z + 1 read 4 of them and the others load ahead (plane z + ring - 2 is
+// requested at plane z; with 6 planes the loads run two planes ahead of
+// their use). Used when the weights and the ring fit in shared memory
+// (ConvMarch<N>::fits).
 template <int N>
 struct ConvMarch {
-    static constexpr int kPlane = 18 * 320;  // one chunk of one halo plane
-    static int smem(int cin) { return 27 * N * cin * 2 + 4 * (cin / 16) * kPlane + 1024; }
-    static bool fits(int cin) { return smem(cin) <= 200 * 1024; }
+    static constexpr int kPlane = 18 * 320;                       // one chunk of one halo plane
+    static constexpr uint32_t kCols = TmemColumns<2 * N>::value;  // two accumulators
+    static constexpr uint32_t kAcc1 = kCols / 2;                  // column of the second
+    static int smem(int cin, int ring) { return 27 * N * cin * 2 + ring * (cin / 16) * kPlane + 1024; }
+    static bool fits(int cin, int ring) { return smem(cin, ring) <= 200 * 1024; }
 };
 
 template <int N>
-__global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt) {
-    using T = ConvTile<N>;
+__global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) {
     using Z = ConvMarch<N>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
     __shared__ float s_bias[N];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -220,11 +255,12 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt) {
     const uint32_t sbase = tc::smem_addr(smem);
     const uint32_t wbase = sbase;
     const uint32_t rbase = sbase + uint32_t(27 * N * a.cin * 2);
-    const uint32_t bar_addr = tc::smem_addr(&bar);
+    const uint32_t bar0 = tc::smem_addr(&bars[0]);  // accumulator k's barrier at bar0 + 8 k
 
-    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), Z::kCols);
     if (tid == 0) {
-        tc::mbar_init(bar_addr, 1);
+        tc::mbar_init(bar0, 1);
+        tc::mbar_init(bar0 + 8, 1);
         tc::fence_mbarrier_init();
     }
     for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
@@ -235,9 +271,12 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt) {
         const __nv_bfloat16* wsrc = a.w + (long(t) * N + co) * a.cin + cc * 16 + half * 8;
         tc::cp_async16(wbase + uint32_t(ct * N * 32 + (co >> 3) * 256 + half * 128 + (co & 7) * 16), wsrc, true);
     }
-    // halo plane zz (all chunks) into ring slot zz & 3; rows outside the grid read as zero
+    // halo plane zz >= -1 (all chunks) into ring slot (zz mod ring); rows
+    // outside the grid read as zero
+    const uint32_t plane_bytes = uint32_t(chunks * Z::kPlane);
+    auto slot_of = [&](int zz) { return uint32_t((zz + ring) % ring) * plane_bytes; };
     auto load_plane = [&](int zz) {
-        const uint32_t slot = rbase + uint32_t((zz & 3) * chunks * Z::kPlane);
+        const uint32_t slot = rbase + slot_of(zz);
         for (int i = tid; i < chunks * 18 * 20; i += blockDim.x) {
             const int half = i & 1, v = (i >> 1) % 10, rc = (i >> 1) / 10;  // rc = chunk * 18 + ry
             const int ry = rc % 18, cc = rc / 18;
@@ -248,90 +287,82 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt) {
             tc::cp_async16(slot + uint32_t(rc * 320 + half * 160 + v * 16), src, valid);
         }
     };
+    // one cp.async group: the weights and planes z0 - 1 .. z0 + 1; then one
+    // group per plane ahead (z0 + 2 .. z0 + ring - 3; empty past z1)
+    auto wait_ahead = [&]() {  // all but the ring - 4 newest groups have landed
+        if (ring == 6) tc::cp_async_wait_group<2>();
+        else tc::cp_async_wait_group<0>();
+    };
     load_plane(z0 - 1);
     load_plane(z0);
     load_plane(z0 + 1);
-    tc::cp_async_wait_all();
+    tc::cp_async_commit();
+    for (int zz = z0 + 2; zz <= z0 + ring - 3; ++zz) {
+        if (zz <= z1) load_plane(zz);
+        tc::cp_async_commit();
+    }
+    wait_ahead();
     tc::fence_proxy_async();
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = tmem_slot;
     constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
+    const uint64_t a_desc = tc::smem_desc(rbase, 160, 320);
+    const uint64_t b_desc = tc::smem_desc(wbase, 128, 256);
+    // one thread: the MMAs of plane z into accumulator k, committed to barrier k
+    auto issue = [&](int z, int k) {
+        tc::tc_fence_after();
+        const uint32_t dz_bytes[3] = {slot_of(z - 1), slot_of(z), slot_of(z + 1)};
+#pragma unroll 1
+        for (int cc = 0; cc < chunks; ++cc)
+            issue_taps<N>(tmem + uint32_t(k) * Z::kAcc1, a_desc + uint32_t(cc * (Z::kPlane >> 4)), dz_bytes,
+                          b_desc + uint32_t(cc * 27 * N * 2), idesc, cc > 0);
+        tc::mma_commit(bar0 + uint32_t(8 * k));
+    };
     bool ok = true;
-    int phase = 0;
+    int issued0 = 1, issued1 = 0;  // commits per barrier, counted by every thread
+    if (tid == 0) issue(z0, 0);
     for (int z = z0; z < z1; ++z) {
-        if (z + 2 <= z1) load_plane(z + 2);  // overlaps this plane's MMAs and epilogue
-        if (tid == 0) {
-            tc::tc_fence_after();
-#pragma unroll 1
-            for (int cc = 0; cc < chunks; ++cc)
-#pragma unroll 1
-                for (int t = 0; t < 27; ++t) {
-                    const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-                    const uint32_t a_addr = rbase + uint32_t((((z + dz - 1) & 3) * chunks + cc) * Z::kPlane +
-                                                             dy * 320 + dx * 16);
-                    const uint32_t b_addr = wbase + uint32_t((cc * 27 + t) * N * 32);
-                    tc::mma_bf16(tmem, tc::smem_desc(a_addr, 160, 320), tc::smem_desc(b_addr, 128, 256), idesc,
-                                 cc > 0 || t > 0);
-                }
-            tc::mma_commit(bar_addr);
+        const int k = (z - z0) & 1;
+        const bool next = z + 1 < z1;
+        if (next) {
+            // into the ring slot of plane z - 2, last read by the MMAs of
+            // plane z - 1 (complete)
+            const int zz = z + ring - 2;
+            if (zz <= z1) load_plane(zz);
+            tc::cp_async_commit();
+            wait_ahead();  // plane z + 2 has landed
+            tc::fence_proxy_async();
         }
-        const bool mine = tc::mbar_wait(bar_addr, uint32_t(phase) & 1u, kWaitLimit);
-        ++phase;
+        // plane z + 2 is visible to the tensor core and the epilogue of plane
+        // z - 1 has read accumulator k ^ 1
+        tc::tc_fence_before();
+        __syncthreads();
+        if (next) {
+            if (tid == 0) issue(z + 1, k ^ 1);
+            if (k) ++issued0;
+            else ++issued1;
+        }
+        const int commits = k ? issued1 : issued0;
+        const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * k), uint32_t(commits - 1) & 1u, kWaitLimit);
         if (!__syncthreads_and(mine)) {
             ok = false;
             break;
         }
         tc::tc_fence_after();
-        if (warp < 4) {
-            const int m = warp * 32 + lane;
-            const int x = x0 + (m & 7), y = y0 + (m >> 3);
-            const bool vin = x < a.W && y < a.H;
-            const long v = (long(z) * a.H + y) * a.W + x;
-            const uint32_t lane_base = uint32_t(warp * 32) << 16;
-#pragma unroll
-            for (int c0 = 0; c0 < N; c0 += 16) {
-                float acc[16];
-                tc::tmem_ld16(tmem + lane_base + uint32_t(c0), acc);
-                if (vin) {
-                    float val[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        val[i] = acc[i] + s_bias[c0 + i];
-                        if (a.relu) val[i] = fmaxf(val[i], 0.f);
-                    }
-                    const long o = v * a.out_stride + a.out_offset + c0;
-                    if (a.out_fp32) {
-                        float* dst = static_cast<float*>(a.out) + o;
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) dst[i] = val[i];
-                    } else {
-                        __align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(val[i]);
-                        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o);
-                        dst[0] = reinterpret_cast<const uint4*>(h)[0];
-                        dst[1] = reinterpret_cast<const uint4*>(h)[1];
-                    }
-                }
-            }
-        }
-        // the next plane's MMAs overwrite TMEM and read the plane loaded above
-        tc::cp_async_wait_all();
-        tc::fence_proxy_async();
-        tc::tc_fence_before();
-        __syncthreads();
+        conv_epilogue<N>(a, tmem + uint32_t(k) * Z::kAcc1, s_bias, x0, y0, z, warp, lane);
     }
     if (!ok) {
         if (tid == 0) atomicOr(a.error, 1u);
-        // drain the commit whose wait timed out (phase - 1), bounded
-        tc::mbar_wait(bar_addr, uint32_t(phase - 1) & 1u, kWaitLimit);
+        // drain every commit still in flight, bounded
+        tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
+        if (issued1 > 0) tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
         tc::cp_async_wait_all();
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, T::kCols);
+    if (warp == 0) tc::tmem_dealloc(tmem, Z::kCols);
 }
 
 // ---- CUDA-core kernels -------------------------------------------------------
@@ -779,9 +810,27 @@ __global__ void k_to_bf16(long count, const float* __restrict__ a, __nv_bfloat16
 
 int blocks_for(long count) { return int(std::max<long>(1, std::min<long>((count + 255) / 256, 148L * 16))); }
 
-// Shared memory of the halo and weight stages bounds the blocks per SM (at
-// most 7, for N = 16 with one stage), so the tensor memory the blocks of one
-// launch allocate (at most 7 x 32, 3 x 64 or 2 x 128 columns) fits in 512.
+// Streaming multiprocessors of the current device.
+int device_sm_count() {
+    int dev = 0, sms = 0;
+    VB_CUDA(cudaGetDevice(&dev));
+    VB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+// CTAs of 256 threads that one SM holds at once with `smem` bytes of dynamic
+// shared memory: 228 KB per SM, 1 KB reserved per CTA plus its static shared
+// memory (barriers, bias; under 512 bytes), 64 K registers at up to 40 per
+// thread, 8 CTAs of 256 threads.
+int resident_ctas(int smem) {
+    constexpr int kSmemPerSm = 228 * 1024, kPerCta = 1024 + 512;
+    return std::max(1, std::min({8, 65536 / (256 * 40), kSmemPerSm / (smem + kPerCta)}));
+}
+
+// Shared memory bounds the blocks per SM, so the tensor memory the blocks of
+// one launch allocate fits in 512 columns: k_conv3_tc at most 7 x 32, 5 x 32,
+// 3 x 64 or 2 x 128 (N = 16, 32, 64, 96); k_conv3_zm, with two accumulators,
+// at most 6 x 32, 4 x 64, 3 x 128, 2 x 128 or 2 x 256 (N = 16, 32, 48, 64, 96).
 template <int N>
 void configure_n() {
     VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -795,13 +844,20 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
         fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
     const unsigned gx = unsigned((a.W + 7) / 8), gy = unsigned((a.H + 15) / 16);
     count_launch();
-    if (ConvMarch<N>::fits(a.cin)) {
-        // planes per CTA: the largest power of two up to 8 that keeps at least
-        // two CTAs per SM
-        int zt = 8;
-        while (zt > 1 && long(gx) * gy * ((a.D + zt - 1) / zt) < 2L * 148) zt >>= 1;
+    if (ConvMarch<N>::fits(a.cin, 4)) {
+        // planes per CTA: the smallest power of two (up to 16) whose grid runs
+        // in one wave of resident CTAs; the 6-plane ring when it fits, keeps
+        // that plane count and the CTAs march at least 4 planes
+        auto planes_for = [&](int ring) {
+            const long slots = long(resident_ctas(ConvMarch<N>::smem(a.cin, ring))) * device_sm_count();
+            int zt = 1;
+            while (zt < 16 && long(gx) * gy * ((a.D + zt - 1) / zt) > slots) zt <<= 1;
+            return zt;
+        };
+        const int zt = planes_for(4);
+        const int ring = (zt >= 4 && ConvMarch<N>::fits(a.cin, 6) && planes_for(6) == zt) ? 6 : 4;
         const dim3 grid(gx, gy, unsigned((a.D + zt - 1) / zt));
-        k_conv3_zm<N><<<grid, 256, ConvMarch<N>::smem(a.cin), s>>>(a, zt);
+        k_conv3_zm<N><<<grid, 256, ConvMarch<N>::smem(a.cin, ring), s>>>(a, zt, ring);
     } else {
         const dim3 grid(gx, gy, unsigned(a.D));
         k_conv3_tc<N><<<grid, 256, ConvTile<N>::smem(a.cin / 16), s>>>(a);
