@@ -378,7 +378,7 @@ def main():
         "gpu_launches": launches,
         "gpu_launches_note": "kernels per step counted on the eager replay of the same step, times steps",
         "roofline": sor_roofline(phases),
-        "roofline_tensor": {"bound": "tensor", "kernel": "coarse U-Net forward (k_conv3_tc, 10 convolutions)",
+        "roofline_tensor": {"bound": "tensor", "kernel": "coarse U-Net forward (k_conv3_zm and k_conv3_tc, 10 convolutions)",
                             "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
                             "peak_kind": "measured sustained", "flops_per_application": net_flops,
                             "ms_per_application": coarse_ms,
