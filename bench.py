@@ -202,9 +202,9 @@ def run_reference(args):
 REFERENCE_SWEEPS_PER_STEP = 6000
 
 
-# DRAM bytes (read 100.67 MB + written 10.11 MB) of one k_sor_rbz colour
+# DRAM bytes (read 100.67 MB + written 8.95 MB) of one k_sor_rbz colour
 # launch at 256^3, from an ncu --set full capture on the benchmark plume.
-SOR_TRAFFIC_256 = 100.673536e6 + 10.114048e6
+SOR_TRAFFIC_256 = 100.673792e6 + 8.947968e6
 
 
 def network_flops(nc):
