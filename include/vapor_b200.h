@@ -317,7 +317,7 @@ vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
  * counterpart in the reference: it is for callers that may not allocate at
  * the call site (a frame loop that cannot absorb cudaFree's device-wide
  * synchronization, a host that owns all device memory and hands plugins only
- * their buffers, a stream that another component is recording into). Same
+ * their buffers). Same
  * arithmetic as vapor_stage_advect_face_device / _scalar_device (results are
  * bit-identical), with the MacCormack forward pass kept in a fixed 4 MiB
  * array inside this library's device image instead of an allocated buffer.

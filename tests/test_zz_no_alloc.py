@@ -1,8 +1,8 @@
 """vapor_advect_noalloc: MacCormack/semi-Lagrangian advection whose scratch is
 a fixed array in the library's device image, for callers that must not
 allocate device memory while they advect (a frame loop that cannot afford the
-device-wide synchronization of cudaFree, a host that owns all device memory and
-only lends buffers to plugins, or a caller whose stream is being recorded).
+device-wide synchronization of cudaFree, or a host that owns all device memory
+and only lends buffers to plugins).
 
 Checked through the C ABI against the existing staged entry point
 (vapor_stage_advect_*_device) on two calls in a row, bit for bit (the bar of

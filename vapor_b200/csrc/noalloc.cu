@@ -5,8 +5,7 @@
 // hard time budget cannot afford; a host that owns all device memory itself
 // (a renderer or engine with a fixed memory budget, or a plugin host that
 // forbids a plugin from allocating) gives its plugins only the buffers it
-// passes in; and allocation is not permitted while another component is
-// recording work into a CUDA stream. For those callers this entry point takes
+// passes in. For those callers this entry point takes
 // the MacCormack forward-pass scratch from a fixed array in this library's
 // device image instead of allocating it.
 //
