@@ -119,7 +119,9 @@ __global__ void k_emit_apply(Grid g, EmitterBox e, const float* __restrict__ noi
         if (e.profile) {
             float q2;
             inside(e, g.h, x, y, z, &q2);
-            const float weight = expf(-3.5f * q2);
+            // exp in double, rounded once to float: the oracle's CPU
+            // evaluation gives the same float
+            const float weight = float(exp(double(-3.5f * q2)));
             const float prof = minf_ref(1.f, e.strength * 3.f * weight);
             cell = maxf_ref(cell, prof);
         } else {
