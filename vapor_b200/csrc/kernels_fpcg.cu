@@ -4,7 +4,7 @@
 // correction is the learned part (the U-Net maps the coarse residual to the
 // coarse pressure); without a network the preconditioner is the smoothing
 // alone. No counterpart in the reference, whose only solver is SOR
-// (SOR.cpp:22-64); results are judged by the same FP64 residual test.
+// (SOR.cpp:22-64); convergence is decided by the same FP64 residual test.
 //
 // Vectors are FP32 in the solver's red-black split layout (padding slots stay
 // zero); dot products are FP64 per-block partials summed in a fixed order by

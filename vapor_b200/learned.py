@@ -6,7 +6,8 @@ convolutions on tcgen05 tensor cores, BF16 weights and activations, FP32
 accumulation). It maps the RMS-normalized right-hand side of a projection to
 the shape of the pressure; the projection scales the prediction by the
 Galerkin condition and then runs its usual solver from it to the same
-tolerance, so the plain solver remains both the fallback and the judge.
+tolerance, so the plain solver remains both the fallback and the arbiter of
+convergence.
 
   python -m vapor_b200.learned train --out weights.npy [--n 128 --rollouts 8 --steps 100]
   python -m vapor_b200.learned compare --weights weights.npy [--n 256 --steps 4]
