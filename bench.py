@@ -339,7 +339,10 @@ def main():
                 "traffic": SOR_TRAFFIC_256 * cells / 256 ** 3,
                 "traffic_note": "dram bytes read + written per launch from an ncu --set full capture at 256^3, "
                                 "scaled by cells for other sizes",
-                "bytes_per_launch": nbytes, "avg_launch_us": launch_ms * 1e3}
+                "bytes_per_launch": nbytes, "avg_launch_us": launch_ms * 1e3,
+                "timing_note": "average colour-launch time from CUDA events around the sweep phase of an eager "
+                               "replay of the benchmarked step on the simulation's stream (the kernels inside the "
+                               "step's CUDA graph cannot be bracketed one by one); launch gaps included"}
 
     # Network (tensor cores): FLOPs of the coarse U-Net per application over
     # the coarse phase's time per application (restriction, normalization,
