@@ -75,16 +75,27 @@ def swirl_fields(n, seed, amplitude=0.5, vortices=8, sigma=0.08):
     h = 1.0 / n
 
     def comp(c, shape):
-        zz, yy, xx = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
-        pos = [(xx + (0.0 if c == 0 else 0.5)) * h, (yy + (0.0 if c == 1 else 0.5)) * h,
-               (zz + (0.0 if c == 2 else 0.5)) * h]
+        # separable coordinates broadcast over (z, y, x); each vortex adds
+        # amplitude * (a x r)_c / sigma * exp(-|r|^2 / (2 sigma^2)) (the same
+        # elementwise operations as a full-grid evaluation, plane by plane)
+        axis = [(np.arange(s, dtype=np.float64) + (0.0 if c == d else 0.5)) * h
+                for d, s in zip((2, 1, 0), shape)]  # z, y, x coordinates
+        zs, ys, xs = axis
         out = np.zeros(shape)
         for k in range(vortices):
-            r = [pos[d] - centres[k, d] for d in range(3)]
-            g = np.exp(-(r[0] ** 2 + r[1] ** 2 + r[2] ** 2) / (2 * sigma ** 2))
             a = axes[k]
-            cross = [a[1] * r[2] - a[2] * r[1], a[2] * r[0] - a[0] * r[2], a[0] * r[1] - a[1] * r[0]]
-            out += amplitude * cross[c] / sigma * g
+            rx = (xs - centres[k, 0])[None, :]
+            ry = (ys - centres[k, 1])[:, None]
+            for iz in range(shape[0]):
+                rz = zs[iz] - centres[k, 2]
+                g = np.exp(-(rx ** 2 + ry ** 2 + rz ** 2) / (2 * sigma ** 2))
+                if c == 0:
+                    cr = a[1] * rz - a[2] * ry
+                elif c == 1:
+                    cr = a[2] * rx - a[0] * rz
+                else:
+                    cr = a[0] * ry - a[1] * rx
+                out[iz] += amplitude * cr / sigma * g
         return out.astype(np.float32)
 
     u = comp(0, (n, n, n + 1))
