@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--interval", type=int, default=8, help="residual check interval (sweeps)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-sweeps", type=float, default=None,
+                    help="reference arm: SOR sweeps per step to charge (default: the plain GPU arm's, from "
+                         "vapor_b200/tuning/plain_sweeps.json for the same warm-up and steps)")
+    ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--record-plain-sweeps", action="store_true",
+                    help="write the plain arm's per-step sweep counts (vapor_b200/tuning/plain_sweeps.json)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--weights", default=os.path.join(ROOT, "vapor_b200", "weights", "coarse_unet.npy"),
                     help="coarse-grid U-Net parameters of the learned arm")
@@ -132,74 +138,164 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def reference_cpu_sample(n_target, sweeps_per_step, seed, n_sample=128):
-    """Times the reference's own CPU MAC 3D step (oracle/_ref) on a bounded
-    sample: one Reflection+MacCormack step at n_sample^3 of the same scene with
-    16 and then 48 fixed SOR sweeps, giving the non-solver cost and the cost per
-    sweep; both scale with the cell count to n_target^3. The reference has no
-    profile emitter or second source, so its sample uses its own emitter at the
-    first source position (the cost is dominated by transport and sweeps)."""
+# Fixed SOR sweep counts of the two timed reference steps: the difference of
+# their times is the cost of 64 sweeps at the full grid.
+REFERENCE_SWEEPS_LOW, REFERENCE_SWEEPS_HIGH = 16, 80
+PLAIN_SWEEPS_TABLE = os.path.join(ROOT, "vapor_b200", "tuning", "plain_sweeps.json")
+
+
+def reference_step_costs(n, seed):
+    """Times the reference's own compiled CPU MAC 3D step (oracle/_ref:
+    MacGridFluidSolver3D::advance, MacGridFluidSolver3D.cpp:192-245) at the
+    full n^3 grid on the benchmark plume's initial state: one untimed step
+    (first touch of the solver's work arrays), then one complete step with
+    REFERENCE_SWEEPS_HIGH and one with REFERENCE_SWEEPS_LOW fixed SOR sweeps.
+    A step's time is linear in its sweep count by construction (each sweep is
+    one pass of SOR.cpp:36-54 over the grid), so the two steps give the cost
+    of one sweep and the rest of the step (advection, divergence, gradient,
+    forcing). The reference has no profile emitter or second source; its
+    step uses its own emitter at the first source position. Single-threaded:
+    the reference's build enables no OpenMP and its sweep is serial."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_lib import RefSim, ref_available, default_params
+    from oracle_lib import RefSim, default_params, ref_available
     if not ref_available():
         return None
-    fields = swirl_fields(n_sample, seed)
+    sim = RefSim(n, 1.0, fields=swirl_fields(n, seed))
+    p = default_params()
+    p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = 1, 1, 1
+    p.buoyancy, p.smoke_decay, p.emitter_radius, p.source_strength = 1.5, 0.5, 0.08, 1.0
+    p.emitter_center_x, p.emitter_center_y, p.emitter_center_z = 0.3, 0.5, 0.15
+    p.emitter_kick_multiplier, p.stir_strength = 0.0, 0.0
+    p.sor_omega = omega_for(n)
     times = {}
-    for iters in (16, 48):
-        sim = RefSim(n_sample, 1.0, fields=fields)
-        p = default_params()
-        p.reflection, p.mac_cormack_vel, p.mac_cormack_smoke = 1, 1, 1
-        p.buoyancy, p.smoke_decay, p.emitter_radius, p.source_strength = 1.5, 0.5, 0.08, 1.0
-        p.emitter_center_x, p.emitter_center_y, p.emitter_center_z = 0.3, 0.5, 0.15
-        p.emitter_kick_multiplier, p.stir_strength = 0.0, 0.0
-        p.sor_omega, p.project_iterations = omega_for(n_sample), iters
+    for sweeps, timed in ((REFERENCE_SWEEPS_LOW, False), (REFERENCE_SWEEPS_HIGH, True),
+                          (REFERENCE_SWEEPS_LOW, True)):
+        p.project_iterations = sweeps  # the Reflection step runs two projections of sweeps / 2
         sim.params = p
         t0 = time.perf_counter()
-        assert sim.advance(DT) == 0
-        times[iters] = time.perf_counter() - t0
-    per_sweep = (times[48] - times[16]) / 32.0
-    fixed = times[16] - 16 * per_sweep
-    scale = (n_target / n_sample) ** 3
-    step_s = scale * (fixed + sweeps_per_step * per_sweep)
+        if sim.advance(DT) != 0:
+            raise RuntimeError("reference step failed")
+        if timed:
+            times[sweeps] = time.perf_counter() - t0
+    per_sweep = (times[REFERENCE_SWEEPS_HIGH] - times[REFERENCE_SWEEPS_LOW]) / (REFERENCE_SWEEPS_HIGH -
+                                                                               REFERENCE_SWEEPS_LOW)
+    fixed = times[REFERENCE_SWEEPS_LOW] - REFERENCE_SWEEPS_LOW * per_sweep
+    return {"n": n, "fixed_s": fixed, "per_sweep_s": per_sweep,
+            "timed_steps": [{"sweeps": s, "seconds": t} for s, t in times.items()]}
+
+
+def plain_sweeps_charged(warmup, steps):
+    """Mean SOR sweeps per step of the plain GPU arm over the same window of
+    steps (after `warmup` steps, `steps` steps) on the same seeded scene, from
+    the per-step table that `bench.py --record-plain-sweeps` wrote (the plain
+    arm is deterministic: fixed-order reductions, bit-identical replays).
+    Steps past the table's end are charged its last entry."""
+    with open(PLAIN_SWEEPS_TABLE) as f:
+        table = json.load(f)
+    per_step = table["per_step"]
+    window = [per_step[min(i, len(per_step) - 1)] for i in range(warmup, warmup + max(1, steps))]
+    return sum(window) / len(window), table
+
+
+def reference_line(costs, sweeps, source):
+    """cpu_baseline object: the reference step's measured costs charged
+    `sweeps` sweeps per step."""
+    step_s = costs["fixed_s"] + sweeps * costs["per_sweep_s"]
+    timed = costs["timed_steps"]
     return {"value": 1.0 / step_s, "unit": "steps/s", "cores": 1, "kind": "reference",
-            "sample": (f"reference CPU MAC 3D step (oracle/_ref, single-threaded) at {n_sample}^3 with 16 and 48 "
-                       f"fixed sweeps: {fixed:.2f} s non-solver + {per_sweep * 1e3:.1f} ms/sweep, scaled by "
-                       f"{scale:.0f}x cells to {n_target}^3 and {sweeps_per_step:.0f} sweeps/step"),
+            "extrapolated": True, "sweeps_charged": sweeps, "sweeps_source": source,
+            "sample": (f"reference CPU MAC 3D step (oracle/_ref, single-threaded) at {costs['n']}^3, two complete "
+                       f"steps after one untimed step: " +
+                       ", ".join(f"{t['sweeps']} sweeps {t['seconds']:.2f} s" for t in timed) +
+                       f" -> {costs['fixed_s']:.2f} s per step without the solve + "
+                       f"{costs['per_sweep_s'] * 1e3:.1f} ms per sweep; value charges {sweeps:.1f} sweeps per step "
+                       f"(linear along the sweep axis only)"),
+            "measured_ms_per_step": 1e3 * sum(t["seconds"] for t in timed) / len(timed),
             "nproc": os.cpu_count()}
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU path on the host cores."""
+    """--impl reference: the reference's CPU path on the host cores, at the
+    benchmark grid, charged the plain GPU arm's sweeps for the same steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sweeps = REFERENCE_SWEEPS_PER_STEP
-    samples = []
     t_start = time.perf_counter()
-    for _ in range(max(1, args.steps)):
-        s = reference_cpu_sample(args.n, sweeps, args.seed)
-        if s is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) missing"}))
-            return
-        samples.append(s["value"])
-    value = statistics.median(samples)
-    s["value"] = value
+    if args.reference_sweeps is not None:
+        sweeps, source = float(args.reference_sweeps), "--reference-sweeps"
+    else:
+        sweeps, table = plain_sweeps_charged(args.warmup, args.steps)
+        if table["n"] != args.n:
+            raise SystemExit(f"{PLAIN_SWEEPS_TABLE} holds {table['n']}^3 counts; pass --reference-sweeps "
+                             f"for {args.n}^3")
+        source = (f"plain GPU arm's mean sweeps per step over steps {args.warmup}..{args.warmup + args.steps - 1} "
+                  f"of the same scene ({os.path.relpath(PLAIN_SWEEPS_TABLE, ROOT)}: {table['command']})")
+    costs = reference_step_costs(args.n, args.seed)
+    if costs is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) missing"}))
+        return
+    base = reference_line(costs, sweeps, source)
+    value = base["value"]
+    timed = costs["timed_steps"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "steps": len(timed), "warmup": 1, "ms_per_step": base["measured_ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "extrapolated": True,
             "config": {"workload": f"mac3d_reflection_maccormack_{args.n}", "n": args.n,
-                       "sweeps_per_step": sweeps, "note": "reference FP32 SOR stagnates above 1e-6; "
-                       "it is given the sweep count the GPU solve needed"},
-            "cpu_baseline": s, "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
-                                       "d2h_bytes_per_step": 0},
+                       "sweeps_per_step": sweeps,
+                       "note": "steps, warmup and ms_per_step describe the reference steps that ran (fixed sweep "
+                               "counts); value charges them the plain GPU arm's sweeps per step, because the "
+                               "reference's FP32 SOR stagnates above relative residual 1e-6"},
+            "cpu_baseline": base, "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0},
             "wall_s": time.perf_counter() - t_start}
     print(json.dumps(line))
 
 
-# SOR sweeps per step the plain GPU solve needed on this workload at 256^3
-# (from the latest GPU run of this benchmark); the reference arm is charged
-# the same number of sweeps.
-REFERENCE_SWEEPS_PER_STEP = 6000
+def start_cpu_sample(args):
+    """Starts the reference CPU timing in its own process, before any CUDA
+    call, so that it runs beside the GPU arms on another host core."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-sample", "--n", str(args.n), "--seed", str(args.seed)]
+    return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+
+
+def finish_cpu_sample(proc, sweeps, timeout=600):
+    try:
+        out, err = proc.communicate(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        return {"value": None, "unavailable": f"reference CPU timing exceeded {timeout} s"}
+    if proc.returncode != 0 or not out.strip():
+        return {"value": None, "unavailable": f"reference CPU timing failed: {err.strip()[-200:]}"}
+    costs = json.loads(out.strip().splitlines()[-1])
+    if costs is None:
+        return {"value": None, "unavailable": "oracle/_ref (reference CPU build) missing"}
+    return reference_line(costs, sweeps, "plain GPU arm of this run")
+
+
+def record_plain_sweeps(args):
+    """Writes the plain arm's SOR sweeps for each of the first `steps` steps
+    of the benchmark scene (the table the reference arm charges)."""
+    import vapor_b200 as vb
+    from vapor_b200.abi import SOLVER_MIXED_REFINEMENT
+    n = args.n
+    params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega_for(n, args.omega),
+                          interval=args.interval)
+    params.solver_kind = SOLVER_MIXED_REFINEMENT
+    sim = vb.MacSimulation3D(n, 1.0, params)
+    sim.upload(*swirl_fields(n, scene_seed(args.seed, 0)))
+    per_step = []
+    for _ in range(args.steps):
+        it0 = sim.total_iterations()
+        sim.advance(DT)
+        per_step.append(int(sim.total_iterations() - it0))
+    sim.close()
+    table = {"n": n, "seed": args.seed, "relative_tolerance": args.rel, "omega": omega_for(n, args.omega),
+             "command": f"python bench.py --record-plain-sweeps --n {n} --steps {args.steps}",
+             "per_step": per_step}
+    with open(PLAIN_SWEEPS_TABLE, "w") as f:
+        json.dump(table, f, indent=1)
+    print(json.dumps(table))
 
 
 # DRAM bytes (read 100.67 MB + written 8.95 MB) of one k_sor_rbz colour
@@ -270,9 +366,16 @@ def eager_phases(vb, sim, steps):
 def main():
     args = parse()
     world, rank, local = rank_info()
+    if args.cpu_sample:
+        print(json.dumps(reference_step_costs(args.n, args.seed)))
+        return
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.record_plain_sweeps:
+        record_plain_sweeps(args)
+        return
+    cpu_proc = start_cpu_sample(args) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
 
     import torch
     import vapor_b200 as vb
@@ -391,8 +494,8 @@ def main():
                 "d2h_bytes_per_step": h2d},
         "clocks": learned["clocks"], "wall_s": learned["wall_s"],
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = reference_cpu_sample(n, plain["iterations"], args.seed)
+    if cpu_proc is not None:
+        line["cpu_baseline"] = finish_cpu_sample(cpu_proc, plain["iterations"])
     if rank == 0:
         print(json.dumps(line))
     sim.close()

@@ -51,15 +51,41 @@ def test_clock_sampler_without_samples_reports_none():
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
 def test_reference_arm_prints_one_contract_line():
+    # a small grid keeps the CPU suite fast; the driver runs it at 256^3
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "1"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                        "--warmup", "1", "--n", "32", "--reference-sweeps", "200"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "steps/s" and d["higher_is_better"] is True
     assert d["metric"] == load_bench().METRIC and d["value"] > 0.0
-    assert d["config"]["workload"] == "mac3d_reflection_maccormack_256"
+    assert d["config"]["workload"] == "mac3d_reflection_maccormack_32"
     cpu = d["cpu_baseline"]
     assert cpu["kind"] == "reference" and cpu["cores"] == 1 and cpu["value"] == d["value"] and cpu["sample"]
+    assert cpu["sweeps_charged"] == 200 and d["extrapolated"] is True
+    # steps and ms_per_step describe the reference steps that actually ran
+    assert d["steps"] == 2 and d["warmup"] == 1
+    assert d["steps"] * d["ms_per_step"] <= d["wall_s"] * 1e3
     assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_charge_is_linear_in_sweeps_only():
+    bench = load_bench()
+    costs = {"n": 256, "fixed_s": 36.0, "per_sweep_s": 0.11,
+             "timed_steps": [{"sweeps": 80, "seconds": 44.8}, {"sweeps": 16, "seconds": 37.76}]}
+    line = bench.reference_line(costs, 5000.0, "test")
+    assert line["value"] == pytest.approx(1.0 / (36.0 + 5000 * 0.11))
+    assert line["measured_ms_per_step"] == pytest.approx(1e3 * (44.8 + 37.76) / 2)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "vapor_b200", "tuning", "plain_sweeps.json")),
+                    reason="plain-arm sweep table not recorded yet")
+def test_plain_sweeps_window_matches_the_gpu_arm_steps():
+    bench = load_bench()
+    sweeps, table = bench.plain_sweeps_charged(5, 20)
+    per_step = table["per_step"]
+    window = [per_step[min(i, len(per_step) - 1)] for i in range(5, 25)]
+    assert table["n"] == 256 and sweeps == pytest.approx(sum(window) / 20)
+    assert all(isinstance(v, int) and v > 0 and v % 8 == 0 for v in per_step)
