@@ -325,8 +325,14 @@ vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
  *   on the current device, of the reference's MAC sizes for n; output must not
  *   alias source or the flow; stream may be NULL (the default stream).
  * Limit: the field may have at most 1048576 values (faces: n <= 101); larger
- * fields return VAPOR_LENGTH_ERROR. The first call on each device looks up the
- * array's address; make that first call before any stream capture begins.
+ * fields return VAPOR_LENGTH_ERROR. The 4 MiB are committed when the driver
+ * loads the array's module into a context, which under lazy module loading
+ * (CUDA_MODULE_LOADING=LAZY) is the first call in that context; that call also
+ * looks up and caches the array's address for the context. Make the first
+ * call during set-up, before any stream capture begins. Contexts other than
+ * the primary one are supported (the cache is per context); a device reset
+ * ends the context, so do not call this after cudaDeviceReset in the same
+ * process.
  * All calls share the array, so calls that can overlap on the GPU (different
  * streams, unordered threads) race and must be serialized by the caller.
  * Nothing needs to start at zero. */
@@ -384,6 +390,14 @@ vapor_status vapor_unet_forward_features(vapor_unet *net, int32_t n, const void 
  * grad_params host memory of vapor_unet_parameter_count() floats. */
 vapor_status vapor_unet_backward(vapor_unet *net, int32_t n, const float *grad_output,
                                  float *grad_params);
+/* Test hook for the tensor-core convolutions' bounded waits (no reference
+ * counterpart): with iterations > 0, the first completion wait of every CTA
+ * of the next convolutions polls an mbarrier that nothing completes that many
+ * times, runs out, and the call returns VAPOR_RUNTIME_ERROR ("timed out")
+ * after the CTA has drained its in-flight MMAs and freed its TMEM; 0 restores
+ * normal waits. The error flag is cleared when it is reported, so the next
+ * call starts clean. */
+vapor_status vapor_unet_set_wait_probe(vapor_unet *net, int32_t iterations);
 /* Use `net` (NULL: none) for the initial guess of every later projection of
  * `sim`. The network must outlive the simulation or be detached first. */
 vapor_status vapor_mac3d_set_warm_start(vapor_mac3d *sim, vapor_unet *net);

@@ -13,7 +13,7 @@ committed so the GPU tests do not need the reference at run time).
       20 iterations, 8 frames) over all 8 flag combinations, and for the
       baseline settings (8^3 and 12^3, 6 frames) over all 16 cases.
 
-Usage: python tests/golden/make_golden.py [path/to/reference]
+Usage: python tests/golden/make_golden.py <path/to/reference>
 """
 import json
 import os
@@ -64,7 +64,9 @@ def resident_params(reflection, mc_vel, mc_smoke):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <reference checkout>")
+    ref_root = sys.argv[1]
     baselines = parse_baselines(os.path.join(ref_root, "tests", "SimulationTests.cpp"))
     with open(os.path.join(HERE, "simulation_baselines.json"), "w") as f:
         json.dump({"source": "tests/SimulationTests.cpp:17-34 (taehwann/vapor)",

@@ -69,3 +69,27 @@ def test_obstacle_rejections():
     _, u, v, w = random_fields(n, seed=5)
     with pytest.raises(vb.InvalidArgument):  # the reference's SOR kind has no obstacles
         stage.project(u.copy(), v.copy(), w.copy(), ProjectionOptions(0.01, 1.9, _opts(1e-6)), 6.0)
+
+
+def test_mixed_projection_scene_error_against_the_fp64_oracle():
+    """The 256^3 mixed-precision configuration's scene (k^-5/3 solenoidal +
+    gradient velocity, seeded sphere obstacle) at 48^3: FP32 sweeps under FP64
+    refinement to relative divergence 1e-8, against the FP64 oracle solved to
+    the same tolerance. Measured max relative errors are about 1e-7 (u, v, w)
+    and 2e-7 (p); the bound is 1e-6."""
+    from oracle_lib import oracle_project
+    from vapor_b200.configs import mixed_projection
+    from vapor_b200.plume import omega_for
+    n, rel = 48, 1e-8
+    out, f = mixed_projection(n=n, seed=1, rel=rel, repeats=1, return_fields=True)
+    assert out["converged"] and out["fp64_relative_residual"] <= rel
+    u, v, w = f["input"]
+    o64 = LinearSolveOptions.defaults(max_iterations=200000, relative_tolerance=rel, absolute_tolerance=0.0)
+    st, r64, u64, v64, w64, p64 = oracle_project(n, 1.0, u, v, w, f["dt"], omega_for(n), 6.0, o64, solver_kind=0,
+                                                 dtype=np.float64, solid=f["mask"])
+    assert st == 0 and r64.linear_solve.converged
+    errs = {}
+    for name, g, ref in zip(("u", "v", "w", "p"), f["projected"], (u64, v64, w64, p64)):
+        errs[name] = float(np.abs(g.astype(np.float64) - ref).max() / max(1e-300, np.abs(ref).max()))
+    print("FP64 oracle max relative error:", errs)
+    assert max(errs.values()) <= 1e-6, errs

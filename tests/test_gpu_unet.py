@@ -29,7 +29,8 @@ def _lib():
             ("vapor_unet_get_parameters", [C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
             ("vapor_unet_set_parameters", [C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
             ("vapor_unet_forward_features", [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
-            ("vapor_unet_backward", [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int)):
+            ("vapor_unet_backward", [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p], C.c_int),
+            ("vapor_unet_set_wait_probe", [C.c_void_p, C.c_int32], C.c_int)):
         fn = getattr(lib, name)
         fn.argtypes, fn.restype = args, res
     return lib
@@ -125,6 +126,29 @@ def test_forward_matches_torch_reference(n):
     ref = ref.detach().numpy()
     err = np.abs(got - ref).max() / max(1e-6, np.abs(ref).max())
     assert err < 2e-2, err  # BF16 activations: a few rounding flips propagate
+
+
+def test_bounded_wait_that_runs_out_reports_an_error_and_recovers():
+    """The convolutions' completion waits poll an mbarrier with an iteration
+    limit. With the test hook they poll one that nothing completes, run out,
+    drain their MMAs and free TMEM: the call reports VAPOR_RUNTIME_ERROR and
+    the next normal call gives the same output as before."""
+    import torch
+    net = Net(seed=5)
+    n = 8
+    xin = torch.tensor(features(n, 9)).to(torch.bfloat16).cuda().contiguous()
+    before = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+    vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), before.data_ptr()))
+    vb.check(net.lib.vapor_unet_set_wait_probe(net.h, 64))
+    out = torch.zeros_like(before)
+    st = net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr())
+    assert st == vb.abi.VAPOR_RUNTIME_ERROR
+    msg = vb.library().vapor_last_error()
+    assert b"timed out" in msg and b"tear down" not in msg
+    vb.check(net.lib.vapor_unet_set_wait_probe(net.h, 0))
+    after = torch.zeros_like(before)
+    vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), after.data_ptr()))
+    assert torch.equal(after, before)
 
 
 def test_gradients_match_torch_autograd():

@@ -6,8 +6,9 @@ and only lends buffers to plugins).
 
 Checked through the C ABI against the existing staged entry point
 (vapor_stage_advect_*_device) on two calls in a row, bit for bit (the bar of
-the other advection tests), and the second call must not change the device's
-free memory. This file is collected last so a failure here comes after every
+the other advection tests). The second call must not change the device's
+free memory; the first may commit the fixed array itself (its module loads
+lazily) and nothing more. This file is collected last so a failure here comes after every
 other test has run; it also passes alone in a fresh process.
 """
 import ctypes as C
@@ -66,8 +67,13 @@ def test_noalloc_matches_existing_entry_point_twice(method):
                                           flow[1].data_ptr(), flow[2].data_ptr(), out.data_ptr(), None)
             assert st == 0, vb.library().vapor_last_error()
             torch.cuda.synchronize()
-            if call == 1:
-                assert torch.cuda.mem_get_info()[0] == free_before
+            free_after = torch.cuda.mem_get_info()[0]
+            if call == 0:
+                # the first call may load the array's module (lazy loading),
+                # which commits at most the 4 MiB array (2 MiB pages)
+                assert free_before - free_after <= (4 << 20) + (2 << 20)
+            else:
+                assert free_after == free_before
             outs.append(out.cpu().numpy())
         for got in outs:
             assert np.array_equal(got.view(np.uint32), expected.view(np.uint32)), f"loc {loc}"

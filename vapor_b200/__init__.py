@@ -125,6 +125,7 @@ def _declare(lib):
     f("vapor_unet_get_parameters", _vp, _vp, C.c_int64)
     f("vapor_unet_forward_features", _vp, C.c_int32, _vp, _vp)
     f("vapor_unet_backward", _vp, C.c_int32, _vp, _vp)
+    f("vapor_unet_set_wait_probe", _vp, C.c_int32)
     f("vapor_mac3d_set_warm_start", _vp, _vp)
     f("vapor_mac3d_train_warm_start", _vp, _vp, C.c_float, C.POINTER(C.c_double))
     f("vapor_mac3d_evaluate_warm_start", _vp, _vp, C.POINTER(C.c_double))

@@ -391,7 +391,7 @@ VB_API vapor_status vapor_unet_forward_features(vapor_unet* net, int32_t n, cons
     NET_GUARD(require(input_bf16 && output, "null buffer");
               net->net.forward_features(n, static_cast<const __nv_bfloat16*>(input_bf16), output);
               VB_CUDA(cudaStreamSynchronize(net->stream.s));
-              if (net->net.error_flag()) vb::fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out"));
+              net->net.check_error());
 }
 VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float* grad_output, float* grad_params) {
     NET_GUARD(require(grad_output && grad_params, "null buffer");
@@ -400,7 +400,10 @@ VB_API vapor_status vapor_unet_backward(vapor_unet* net, int32_t n, const float*
                                       vb::unet::parameter_count() * sizeof(float), cudaMemcpyDeviceToHost,
                                       net->stream.s));
               VB_CUDA(cudaStreamSynchronize(net->stream.s));
-              if (net->net.error_flag()) vb::fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out"));
+              net->net.check_error());
+}
+VB_API vapor_status vapor_unet_set_wait_probe(vapor_unet* net, int32_t iterations) {
+    NET_GUARD(require(iterations >= 0, "iterations must be non-negative"); net->net.set_wait_probe(iterations));
 }
 VB_API vapor_status vapor_mac3d_set_warm_start(vapor_mac3d* sim, vapor_unet* net) {
     SIM_GUARD(sim->sim.set_warm_start(net ? &net->net : nullptr));

@@ -988,9 +988,15 @@ void Simulation::download(float* d, float* u, float* v, float* w) {
     downloaded += (cells + 3 * faces) * sizeof(float);
 }
 
-void Simulation::synchronize() { (void)ws_.last_result(); }
+void Simulation::synchronize() { (void)last_projection(); }
 
-vapor_projection_result Simulation::last_projection() { return ws_.last_result(); }
+vapor_projection_result Simulation::last_projection() {
+    const vapor_projection_result r = ws_.last_result();
+    // a network that ran inside the step reports its bounded waits here
+    if (warm_) warm_->check_error();
+    if (coarse_) coarse_->check_error();
+    return r;
+}
 
 void Simulation::diagnostics(vapor_fluid_diagnostics* out) {
     ws_.diagnostics(vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, out);

@@ -86,6 +86,17 @@ unsigned int UNet::error_flag() {
     return e;
 }
 
+void UNet::check_error() {
+    const unsigned int e = error_flag();
+    if (!e) return;
+    VB_CUDA(cudaMemsetAsync(error_.p, 0, sizeof(uint32_t), s_));
+    VB_CUDA(cudaStreamSynchronize(s_));
+    if (e & 2u)
+        fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out and its in-flight MMAs could not be drained; "
+                                  "tear down the CUDA context");
+    fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out");
+}
+
 void UNet::ensure(int n) {
     if (n == n_) return;
     if (n % 4 != 0 || n < 8) fail(VAPOR_INVALID_ARGUMENT, "the warm-start network needs n divisible by 4 (n >= 8)");
@@ -133,6 +144,7 @@ void UNet::conv(int layer, int D, int H, int W, const __nv_bfloat16* in, int in_
     a.out_fp32 = fp32_out ? 1 : 0;
     a.relu = relu ? 1 : 0;
     a.error = error_.p;
+    a.wait_probe = wait_probe_;
     launch_conv3(a, kLayers[layer].cout, s_);
 }
 
@@ -311,7 +323,7 @@ double UNet::train_step(int n, const float* b_split, const float* p_split, const
     ++step_;
     launch_adam(parameter_count(), params_.p, m_.p, v_.p, grad_.p, bf(wbf_), lr, step_, s_);
     VB_CUDA(cudaStreamSynchronize(s_));
-    if (error_flag()) fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out");
+    check_error();
     loss = loss_host_;
     return loss;
 }
@@ -329,7 +341,7 @@ double UNet::evaluate(int n, const float* b_split, const float* p_split, const P
     launch_loss_grad(V1, out_.p, target_.p, partial_.p, scalars_.p, nullptr, s_);
     VB_CUDA(cudaMemcpyAsync(&loss_host_, scalars_.p + 2, sizeof(double), cudaMemcpyDeviceToHost, s_));
     VB_CUDA(cudaStreamSynchronize(s_));
-    if (error_flag()) fail(VAPOR_RUNTIME_ERROR, "tensor-core convolution timed out");
+    check_error();
     return loss_host_;
 }
 

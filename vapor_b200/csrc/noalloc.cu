@@ -10,8 +10,15 @@
 // device image instead of allocating it.
 //
 // The array holds kNoAllocCapacity floats (4 MiB) on every GPU that loads
-// the library, for as long as the process lives. The largest field it can
-// advect therefore has kNoAllocCapacity values (face arrays up to n = 101).
+// the library, for as long as the process lives. The driver commits it when
+// it loads this file's module into a context: at library load, or, under
+// lazy module loading (CUDA_MODULE_LOADING=LAZY, the default of recent CUDA
+// releases), during the first call in that context, which also looks up the
+// array's address. Callers should therefore make one call during set-up,
+// before any stream capture. The address is cached per CUDA context; a device
+// reset (cudaDeviceReset) ends the context it belongs to, so this entry point
+// must not be used after a reset in the same process. The largest field it can
+// advect has kNoAllocCapacity values (face arrays up to n = 101).
 // All calls share the one array: calls that overlap on the GPU (different
 // streams, or different threads without ordering) race on it and must be
 // serialized by the caller. No part of it needs clearing between calls: the
@@ -19,6 +26,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -33,26 +41,47 @@ constexpr size_t kNoAllocCapacity = size_t(1) << 20;
 // obtained with cudaGetSymbolAddress below.
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocCapacity];
 
-constexpr int kMaxDevices = 64;
+// The array's device address belongs to a CUDA context (the module holding
+// it is loaded once per context), so looked-up addresses are cached per
+// context: the runtime's primary context of each device, or any context the
+// caller made current with the driver API.
+using CtxGetCurrentFn = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
 std::mutex g_scratch_mutex;
-float* g_scratch_ptr[kMaxDevices] = {};
+std::map<void*, float*> g_scratch_ptr;
 
-// Device address of the scratch array on the current device, looked up once
-// per device (with that device current) and cached.
-float* scratch_for_current_device() {
-    int dev = 0;
-    VB_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) vb::fail(VAPOR_RUNTIME_ERROR, "device index out of range");
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+        return (e == cudaSuccess && q == cudaDriverEntryPointSuccess) ? reinterpret_cast<CtxGetCurrentFn>(f)
+                                                                        : nullptr;
+    }();
+    if (!fn) vb::fail(VAPOR_RUNTIME_ERROR, "cuCtxGetCurrent is not available from the CUDA driver");
+    return fn;
+}
+
+// Device address of the scratch array in the current context. The first call
+// in a context looks it up with that context current (under lazy module
+// loading this also loads the module and commits the array) and caches it.
+float* scratch_for_current_context() {
+    void* ctx = nullptr;
+    void* ptr = nullptr;
+    if (ctx_get_current()(&ctx) != 0) vb::fail(VAPOR_RUNTIME_ERROR, "cuCtxGetCurrent failed");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr)
-            vb::fail(VAPOR_RUNTIME_ERROR, std::string("cudaGetSymbolAddress of the no-allocation scratch failed: ") +
-                                              cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<float*>(ptr);
+    if (ctx) {
+        const auto it = g_scratch_ptr.find(ctx);
+        if (it != g_scratch_ptr.end()) return it->second;
     }
-    return g_scratch_ptr[dev];
+    // with no context current yet, this call makes the device's primary
+    // context current (the runtime's implicit initialization)
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+        vb::fail(VAPOR_RUNTIME_ERROR, std::string("cudaGetSymbolAddress of the no-allocation scratch failed: ") +
+                                          cudaGetErrorString(e));
+    if (!ctx && (ctx_get_current()(&ctx) != 0 || !ctx)) vb::fail(VAPOR_RUNTIME_ERROR, "no current CUDA context");
+    g_scratch_ptr[ctx] = static_cast<float*>(ptr);
+    return static_cast<float*>(ptr);
 }
 
 bool overlaps(const float* a, size_t na, const float* b, size_t nb) {
@@ -83,7 +112,7 @@ extern "C" __attribute__((visibility("default"))) vapor_status vapor_advect_noal
         if (overlaps(source, count, output, count) || overlaps(output, count, flow_u, faces) ||
             overlaps(output, count, flow_v, faces) || overlaps(output, count, flow_w, faces))
             vb::fail(VAPOR_INVALID_ARGUMENT, "Advection output must not alias its source or the tracer velocities");
-        float* scratch = scratch_for_current_device();
+        float* scratch = scratch_for_current_context();
         const vb::Grid g{n, box, box / float(n)};
         vb::launch_advect(g, loc, dt, cfl_limit, method == VAPOR_MACCORMACK, source, flow_u, flow_v, flow_w, scratch,
                           output, 1.f, static_cast<cudaStream_t>(stream));

@@ -34,7 +34,9 @@ struct ConvArgs {
     int out_offset;
     int out_fp32;
     int relu;
-    unsigned int* error;          // set when a bounded wait timed out
+    unsigned int* error;          // bit 1: a bounded wait timed out; bit 2: in-flight MMAs could not be drained
+    int wait_probe;               // test hook: > 0 makes each CTA's first completion wait poll a barrier
+                                  // that nothing completes, wait_probe times, so that it runs out
 };
 
 struct WGradArgs {
@@ -139,6 +141,15 @@ public:
     // prediction, 1 - cos^2 between the mean-free prediction and p*.
     double evaluate(int n, const float* b_split, const float* p_split, const ProjControl* ctrl);
     unsigned int error_flag();
+    // Waits for the network's stream, then raises VAPOR_RUNTIME_ERROR if a
+    // tensor-core wait ran out since the last check (clearing the flag, so
+    // later calls start clean). When in-flight MMAs could not be drained as
+    // well, the message says the CUDA context must be torn down.
+    void check_error();
+    // Test hook for the timeout path: > 0 makes the next convolutions' first
+    // completion wait poll a barrier that nothing completes, `iterations`
+    // times; 0 restores normal waits.
+    void set_wait_probe(int iterations) { wait_probe_ = iterations; }
     int adam_steps() const { return step_; }
     // Raw forward on device channels-last input [n^3][16] -> FP32 output.
     void forward_features(int n, const __nv_bfloat16* input16, float* out);
@@ -174,6 +185,7 @@ private:
     DevArray<double> partial_, scalars_;
     DevArray<float> scale_;
     DevArray<uint32_t> error_;
+    int wait_probe_ = 0;
 };
 
 }  // namespace unet

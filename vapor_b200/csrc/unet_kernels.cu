@@ -133,7 +133,7 @@ template <int N>
 __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
     using T = ConvTile<N>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[3];
     __shared__ uint32_t tmem_slot;
     __shared__ float s_bias[N];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -144,9 +144,11 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
 
     if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), T::kCols);
     const uint32_t bar0 = tc::smem_addr(&bars[0]);  // stage st's barrier at bar0 + 8 st
+    const uint32_t probe = bar0 + 16;               // never arrived on (timeout test hook)
     if (tid == 0) {
         tc::mbar_init(bar0, 1);
         tc::mbar_init(bar0 + 8, 1);
+        tc::mbar_init(probe, 1);
         tc::fence_mbarrier_init();
     }
     for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
@@ -166,7 +168,9 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
         // the stage's previous MMAs must be done before it is overwritten
         const int before = st ? issued1 : issued0;
         if (before > 0) {
-            const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(before - 1) & 1u, kWaitLimit);
+            const bool mine = a.wait_probe ? tc::mbar_wait(probe, 0u, a.wait_probe)
+                                           : tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(before - 1) & 1u,
+                                                           kWaitLimit);
             if (!__syncthreads_and(mine)) {
                 ok = false;
                 break;
@@ -203,7 +207,9 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
         // the last commit covers every earlier MMA of this thread
         const int st = stages == 2 ? ((chunks - 1) & 1) : 0;
         const int commits = st ? issued1 : issued0;
-        const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(commits - 1) & 1u, kWaitLimit);
+        const bool mine = a.wait_probe ? tc::mbar_wait(probe, 0u, a.wait_probe)
+                                       : tc::mbar_wait(bar0 + uint32_t(8 * st), uint32_t(commits - 1) & 1u,
+                                                       kWaitLimit);
         ok = __syncthreads_and(mine);
     }
     tc::tc_fence_after();
@@ -211,9 +217,12 @@ __global__ void __launch_bounds__(256) k_conv3_tc(ConvArgs a) {
         conv_epilogue<N>(a, tmem, s_bias, x0, y0, z, warp, lane);
     } else {
         if (tid == 0) atomicOr(a.error, 1u);
-        // drain: wait (bounded) for every commit still in flight
-        if (issued0 > 0) tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
-        if (issued1 > 0) tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
+        // drain: wait (bounded) for every commit still in flight; if that
+        // also runs out, MMAs may still write the columns freed below
+        bool drained = true;
+        if (issued0 > 0) drained &= tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
+        if (issued1 > 0) drained &= tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
+        if (!drained) atomicOr(a.error, 2u);
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -244,7 +253,7 @@ template <int N>
 __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) {
     using Z = ConvMarch<N>;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[3];
     __shared__ uint32_t tmem_slot;
     __shared__ float s_bias[N];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -256,11 +265,13 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) 
     const uint32_t wbase = sbase;
     const uint32_t rbase = sbase + uint32_t(27 * N * a.cin * 2);
     const uint32_t bar0 = tc::smem_addr(&bars[0]);  // accumulator k's barrier at bar0 + 8 k
+    const uint32_t probe = bar0 + 16;               // never arrived on (timeout test hook)
 
     if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), Z::kCols);
     if (tid == 0) {
         tc::mbar_init(bar0, 1);
         tc::mbar_init(bar0 + 8, 1);
+        tc::mbar_init(probe, 1);
         tc::fence_mbarrier_init();
     }
     for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
@@ -345,7 +356,9 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) 
             else ++issued1;
         }
         const int commits = k ? issued1 : issued0;
-        const bool mine = tc::mbar_wait(bar0 + uint32_t(8 * k), uint32_t(commits - 1) & 1u, kWaitLimit);
+        const bool mine = a.wait_probe ? tc::mbar_wait(probe, 0u, a.wait_probe)
+                                       : tc::mbar_wait(bar0 + uint32_t(8 * k), uint32_t(commits - 1) & 1u,
+                                                       kWaitLimit);
         if (!__syncthreads_and(mine)) {
             ok = false;
             break;
@@ -355,9 +368,11 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) 
     }
     if (!ok) {
         if (tid == 0) atomicOr(a.error, 1u);
-        // drain every commit still in flight, bounded
-        tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
-        if (issued1 > 0) tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
+        // drain every commit still in flight, bounded; if that also runs out,
+        // MMAs may still write the columns freed below
+        bool drained = tc::mbar_wait(bar0, uint32_t(issued0 - 1) & 1u, kWaitLimit);
+        if (issued1 > 0) drained &= tc::mbar_wait(bar0 + 8, uint32_t(issued1 - 1) & 1u, kWaitLimit);
+        if (!drained) atomicOr(a.error, 2u);
         tc::cp_async_wait_all();
     }
     tc::tc_fence_before();
