@@ -110,6 +110,8 @@ def _declare(lib):
     f("vapor_stage_solve_rhs", _vp, _vp, C.POINTER(ProjectionOptions), C.c_float, C.POINTER(ProjectionResult), _vp)
     f("vapor_mac3d_set_coarse_log", _vp, _vp, C.c_int32, _vp)
     f("vapor_tune_sor_planes", C.c_int32, C.c_int32)
+    f("vapor_tune_sor_blocking", C.c_int32)
+    f("vapor_tune_sor_blocked_chunks", C.c_int32, C.c_int32)
     f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_batch_destroy", _vp)
     f("vapor_batch_advance", _vp, C.c_float)
@@ -341,6 +343,17 @@ class MacSimulation3D:
 def tune_sor_planes(n, planes):
     """z-planes per thread of the colour sweep for grids of size n (0: automatic)."""
     check(library().vapor_tune_sor_planes(int(n), int(planes)))
+
+
+def tune_sor_blocking(iterations_per_launch):
+    """Red+black iterations per temporally blocked sweep launch (1 or 2; 0:
+    one launch per colour). Same results either way."""
+    check(library().vapor_tune_sor_blocking(int(iterations_per_launch)))
+
+
+def tune_sor_blocked_chunks(n, chunks):
+    """z chunks per blocked sweep launch for grids of size n (0: automatic)."""
+    check(library().vapor_tune_sor_blocked_chunks(int(n), int(chunks)))
 
 
 class Batch:

@@ -303,6 +303,16 @@ VB_API vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes) {
     });
 }
 
+VB_API vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch) {
+    return guarded([&] { vb::set_sor_block_iterations(iterations_per_launch); });
+}
+VB_API vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks) {
+    return guarded([&] {
+        require(n > 0 && chunks >= 0 && chunks <= n, "invalid tuning value");
+        vb::set_sor_blocked_chunks(n, chunks);
+    });
+}
+
 // ---- batched scenes ----
 VB_API vapor_status vapor_batch_create(int32_t count, vapor_mac3d* const* sims, vapor_batch** out) {
     return guarded([&] {

@@ -313,6 +313,9 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     float* e = p_.p;
     float* r = r32_.p;
     const ProjectionArgs smooth{a.g, a.dt, 1.0f, 0.0f, a.options};
+    // the smoothing pairs run as one temporally blocked launch each when the
+    // grid allows (same bits as the one-colour launches)
+    const bool blocked = sor_block_iterations(n_) == 2 && kFpcgSmoothing == 2;
     if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);
     else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
     t.begin(VAPOR_PHASE_RESIDUAL);
@@ -321,14 +324,21 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     t.end(VAPOR_PHASE_RESIDUAL, 2);
     auto precondition = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_SOR);
-        // the first colour sweep starts from z = 0 (and clears the other colour)
-        const bool fused_start = sor_fuses_measure(n_);
-        if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
-        for (int j = 0; j < kFpcgSmoothing; ++j) {
-            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false, fused_start && j == 0);
-            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+        if (blocked) {
+            // both sweeps in one launch, starting from z = 0 (z is not read)
+            launch_sor_blocked(smooth, kFpcgSmoothing, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false, true);
+            t.end(VAPOR_PHASE_SOR, 1);
+        } else {
+            // the first colour sweep starts from z = 0 (and clears the other colour)
+            const bool fused_start = sor_fuses_measure(n_);
+            if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
+            for (int j = 0; j < kFpcgSmoothing; ++j) {
+                launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false,
+                                 fused_start && j == 0);
+                launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            }
+            t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
         }
-        t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
             launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
@@ -341,11 +351,16 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
             t.end(VAPOR_PHASE_COARSE, 0);
         }
         t.begin(VAPOR_PHASE_SOR);
-        for (int j = 0; j < kFpcgSmoothing; ++j) {
-            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
-            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+        if (blocked) {
+            launch_sor_blocked(smooth, kFpcgSmoothing, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            t.end(VAPOR_PHASE_SOR, 1);
+        } else {
+            for (int j = 0; j < kFpcgSmoothing; ++j) {
+                launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+                launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            }
+            t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
         }
-        t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
     };
     auto recentre_group = [&](cudaStream_t st) {
         launch_refine_residual_gated(a, b_.p, e, r, ctrl_, st);
@@ -435,12 +450,24 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean,
                       bool measure = false) {
         t.begin(VAPOR_PHASE_SOR);
-        for (int j = 0; j < k; ++j) {
-            launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
-            launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
-                             measure && j + 1 == k);
+        const int per = sor_block_iterations(n_);
+        long long launches = 0;
+        if (per > 0) {  // several red+black iterations per launch (temporal blocking)
+            for (int j = 0; j < k; j += per) {
+                const int it = std::min(per, k - j);
+                launch_sor_blocked(a, it, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
+                                   measure && j + it == k);
+                ++launches;
+            }
+        } else {
+            for (int j = 0; j < k; ++j) {
+                launch_sor_color(a, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed);
+                launch_sor_color(a, 1, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
+                                 measure && j + 1 == k);
+            }
+            launches = 2LL * k;
         }
-        t.end(VAPOR_PHASE_SOR, 2LL * k);
+        t.end(VAPOR_PHASE_SOR, launches);
     };
 
     t.begin(VAPOR_PHASE_RHS);

@@ -139,6 +139,24 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
                       bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true,
                       bool measure = false, bool from_zero = false);
 bool sor_fuses_measure(int n);
+// Temporally blocked form of the same sweeps (kernels_sor_blocked.cu):
+// `iterations` (1 or 2) red+black iterations in one launch, starting with
+// colour `first_colour`, bit-identical to 2 * iterations one-colour launches
+// with the same flags (for first_colour 1: the plain relaxation only). A
+// guarded launch covers sweep indices sweep_index .. + iterations - 1 and
+// stops at the iteration budget; `measure` records the residual of its last
+// half-sweep (colour 1) when it ran all iterations. Needs sor_blocked_applies(n).
+bool sor_blocked_applies(int n);
+void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colour, float* x, const float* b,
+                        ProjControl* ctrl, bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s,
+                        bool exact, bool measure = false, bool from_zero = false);
+// Autotuner hook: z chunks per blocked launch for grid size n (<= 0: one
+// wave of CTAs).
+void set_sor_blocked_chunks(int n, int chunks);
+// Iterations per blocked launch that the solvers use (0: one launch per
+// colour); sor_block_iterations(n) is 0 where the blocked form does not apply.
+void set_sor_block_iterations(int iterations);
+int sor_block_iterations(int n);
 // Autotuner hook: planes per thread of the z-marching colour sweep for grid
 // size n (planes <= 0 restores the automatic choice).
 void set_sor_planes(int n, int planes);
