@@ -192,6 +192,25 @@ void Workspace::advect(int loc, float dt, float cfl, bool maccormack, const floa
     VB_CUDA(cudaGetLastError());
 }
 
+void Workspace::advect_velocity(float dt, float cfl, bool maccormack, const float* const src[3], const float* u,
+                                const float* v, const float* w, float* const out[3]) {
+    const size_t faces = size_t(n_) * n_ * (n_ + 1);
+    if (maccormack) {
+        if (capturing_ && fwd3_.n != 3 * faces) fail(VAPOR_RUNTIME_ERROR, "velocity advection scratch not prepared");
+        ensure_velocity_scratch();
+    }
+    float* fwd[3] = {fwd3_.p, fwd3_.p + faces, fwd3_.p + 2 * faces};
+    timer_.begin(VAPOR_PHASE_ADVECT);
+    launch_advect_velocity(grid(), dt, cfl, maccormack, src, u, v, w, fwd, out, stream_);
+    timer_.end(VAPOR_PHASE_ADVECT, maccormack ? 2 : 1);
+    VB_CUDA(cudaGetLastError());
+}
+
+void Workspace::ensure_velocity_scratch() {
+    const size_t faces = size_t(n_) * n_ * (n_ + 1);
+    if (fwd3_.n != 3 * faces) fwd3_.allocate(3 * faces);
+}
+
 void Workspace::ensure_mixed() {
     const size_t cells = rb_count(n_);
     for (auto& x : x64_)
@@ -709,9 +728,10 @@ void Simulation::emit(float dt) {
 }
 
 void Simulation::advect_velocity(float dt, int src, int flow, int out) {
-    for (int c = 0; c < 3; ++c)
-        ws_.advect(FACE_X + c, dt, params.cfl_mc, params.mac_cormack_vel != 0, vel_[src][c].p, vel_[flow][0].p,
-                   vel_[flow][1].p, vel_[flow][2].p, vel_[out][c].p, 1.f);
+    const float* srcs[3] = {vel_[src][0].p, vel_[src][1].p, vel_[src][2].p};
+    float* outs[3] = {vel_[out][0].p, vel_[out][1].p, vel_[out][2].p};
+    ws_.advect_velocity(dt, params.cfl_mc, params.mac_cormack_vel != 0, srcs, vel_[flow][0].p, vel_[flow][1].p,
+                        vel_[flow][2].p, outs);
 }
 
 void Simulation::validate_step(float dt) const {
@@ -823,6 +843,7 @@ void Simulation::prepare_step(float dt) {
             noise_.allocate(need);
         }
         if (params.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR) ws_.ensure_mixed();
+        if (params.mac_cormack_vel) ws_.ensure_velocity_scratch();
         if (warm_) {
             warm_->set_stream(ws_.stream());
             warm_->prepare(ws_.n());

@@ -121,6 +121,10 @@ public:
     float* rhs() { return b_.p; }
     void advect(int loc, float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
                 const float* w, float* out, float post_scale);
+    // The three velocity components in one forward and one MacCormack launch
+    // (their forward passes kept in a 3-face-array scratch).
+    void advect_velocity(float dt, float cfl, bool maccormack, const float* const src[3], const float* u,
+                         const float* v, const float* w, float* const out[3]);
     // Waits for the stream and returns the last projection result; raises
     // VAPOR_NON_FINITE if a non-finite divergence or residual was seen since
     // the last clear_errors().
@@ -135,6 +139,7 @@ public:
     PhaseTimer& timer() { return timer_; }
     void ensure_mixed();
     void ensure_fpcg(bool coarse);
+    void ensure_velocity_scratch();
     // Solid obstacles (extension): n^3 host mask, x fastest, nonzero = solid;
     // null clears. Faces touching a solid are closed, solid cells are not
     // unknowns, means run over fluid cells. Mixed-precision solver only.
@@ -152,6 +157,7 @@ private:
     float box_;
     cudaStream_t stream_;
     DevArray<float> b_, p_, fwd_;
+    DevArray<float> fwd3_;  // forward passes of the three velocity components (allocated before capture)
     DevArray<double> partials_;
     DevArray<double> x64_[2];           // mixed-precision pressure (ping-pong)
     DevArray<float> r32_;               // mixed-precision inner right-hand side (FPCG: the residual)

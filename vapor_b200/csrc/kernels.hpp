@@ -95,6 +95,12 @@ void launch_walls(const Grid& g, float* u, float* v, float* w, cudaStream_t s);
 void launch_advect(const Grid& g, int loc, float dt, float cfl_limit, bool maccormack, const float* src,
                    const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
                    cudaStream_t s);
+// The three velocity components src[c] (faces of axis c) through the flow
+// (u, v, w) into out[c], in one forward launch (into fwd[c]) and one
+// MacCormack launch; same results as three launch_advect calls.
+void launch_advect_velocity(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* const src[3],
+                            const float* u, const float* v, const float* w, float* const fwd[3],
+                            float* const out[3], cudaStream_t s);
 
 // ---- projection ----
 struct ProjectionArgs {

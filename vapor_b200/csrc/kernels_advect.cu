@@ -6,22 +6,26 @@
 // writes fwd; the MacCormack pass re-traces forward through fwd, applies the
 // 8-donor clamping limiter on the immutable source and falls back to fwd when
 // either trace leaves [0, box] or |v| dt / h exceeds the CFL limit.
+//
+// A launch covers a set of fields: the smoke (cell centres) alone, or the
+// three velocity components together (grid rows are the planes of u, then v,
+// then w), so a velocity advection is one forward launch and one MacCormack
+// launch. When the cell size is a power of two the divisions by h run as
+// multiplications by the exact 1/h (same bits, see div_h).
 #include "kernels.hpp"
+
+#include <cmath>
 
 namespace vb {
 namespace {
 
 constexpr int kThreads = 256;
 
-template <int LOC>
-__device__ __forceinline__ void decode(int n, int& x, int& y, int& z, bool& valid) {
-    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y), ez = n + (LOC == FACE_Z);
-    const int xy = blockIdx.x * blockDim.x + threadIdx.x;
-    z = blockIdx.y;
-    y = xy / ex;
-    x = xy - y * ex;
-    valid = xy < ex * ey && z < ez;
-}
+struct FieldSet {
+    const float* src[3];
+    float* fwd[3];
+    float* out[3];
+};
 
 // Sample point of location LOC: staggered axis at i*h, the others at (i+.5)h
 // (`Vec3 face{ x * dx, (y + .5f) * dx, (z + .5f) * dx }`).
@@ -32,52 +36,42 @@ __device__ __forceinline__ void position(int x, int y, int z, float h, float& px
     pz = LOC == FACE_Z ? float(z) * h : (float(z) + 0.5f) * h;
 }
 
-template <int LOC>
-__global__ void __launch_bounds__(kThreads) k_advect_forward(Grid g, float dt, const float* __restrict__ src,
-                                                             const float* __restrict__ u,
-                                                             const float* __restrict__ v,
-                                                             const float* __restrict__ w,
-                                                             float* __restrict__ out, float post_scale) {
-    int x, y, z;
-    bool valid;
-    decode<LOC>(g.n, x, y, z, valid);
-    if (!valid) return;
+// Base donor index of the limiter: int(pos/h) on the staggered axis, else
+// int(pos/h - .5), clamped to the location's index range.
+template <bool STAGGERED, bool POW2>
+__device__ __forceinline__ int donor(float coord, float h, float ih, int n) {
+    return STAGGERED ? clampi_ref(int(div_h<POW2>(coord, h, ih)), 0, n)
+                     : clampi_ref(int(div_h<POW2>(coord, h, ih) - 0.5f), 0, n - 1);
+}
+
+template <int LOC, bool POW2>
+__device__ __forceinline__ void forward_point(const Grid& g, float ih, float dt, int x, int y, int z,
+                                              const float* __restrict__ src, const float* __restrict__ u,
+                                              const float* __restrict__ v, const float* __restrict__ w,
+                                              float* __restrict__ out, float post_scale) {
     float px, py, pz;
     position<LOC>(x, y, z, g.h, px, py, pz);
-    const Vel vel = velocity_at(u, v, w, g.n, g.h, px, py, pz);
+    const Vel vel = velocity_at<POW2>(u, v, w, g.n, g.h, px, py, pz, ih);
     const float qx = px - vel.x * dt, qy = py - vel.y * dt, qz = pz - vel.z * dt;
-    const float value = sample<LOC>(src, g.n, g.h, qx, qy, qz);
+    const float value = sample<LOC, POW2>(src, g.n, g.h, qx, qy, qz, ih);
     out[index_of(g.n, LOC, x, y, z)] = value * post_scale;
 }
 
-// Base donor index of the limiter: int(pos/h) on the staggered axis, else
-// int(pos/h - .5), clamped to the location's index range.
-template <bool STAGGERED>
-__device__ __forceinline__ int donor(float coord, float h, int n) {
-    return STAGGERED ? clampi_ref(int(coord / h), 0, n) : clampi_ref(int(coord / h - 0.5f), 0, n - 1);
-}
-
-template <int LOC>
-__global__ void __launch_bounds__(kThreads) k_advect_maccormack(Grid g, float dt, float cfl_limit,
-                                                                const float* __restrict__ src,
-                                                                const float* __restrict__ fwd,
-                                                                const float* __restrict__ u,
-                                                                const float* __restrict__ v,
-                                                                const float* __restrict__ w,
-                                                                float* __restrict__ out, float post_scale) {
-    int x, y, z;
-    bool valid;
-    decode<LOC>(g.n, x, y, z, valid);
-    if (!valid) return;
+template <int LOC, bool POW2>
+__device__ __forceinline__ void maccormack_point(const Grid& g, float ih, float dt, float cfl_limit, int x, int y,
+                                                 int z, const float* __restrict__ src,
+                                                 const float* __restrict__ fwd, const float* __restrict__ u,
+                                                 const float* __restrict__ v, const float* __restrict__ w,
+                                                 float* __restrict__ out, float post_scale) {
     const int n = g.n;
     const float h = g.h, box = g.box;
     const size_t i = index_of(n, LOC, x, y, z);
     float px, py, pz;
     position<LOC>(x, y, z, h, px, py, pz);
-    const Vel vel = velocity_at(u, v, w, n, h, px, py, pz);
+    const Vel vel = velocity_at<POW2>(u, v, w, n, h, px, py, pz, ih);
     const float fx = px - vel.x * dt, fy = py - vel.y * dt, fz = pz - vel.z * dt;
     const float bx = px + vel.x * dt, by = py + vel.y * dt, bz = pz + vel.z * dt;
-    const float cfl = sqrtf(vel.x * vel.x + vel.y * vel.y + vel.z * vel.z) * dt / h;
+    const float cfl = div_h<POW2>(sqrtf(vel.x * vel.x + vel.y * vel.y + vel.z * vel.z) * dt, h, ih);
     const float f0 = fwd[i];
     const bool leaves = fx < 0.f || fx > box || fy < 0.f || fy > box || fz < 0.f || fz > box || bx < 0.f ||
                         bx > box || by < 0.f || by > box || bz < 0.f || bz > box;
@@ -85,12 +79,12 @@ __global__ void __launch_bounds__(kThreads) k_advect_maccormack(Grid g, float dt
     if (leaves || cfl > cfl_limit) {
         result = f0;
     } else {
-        const float back = sample<LOC>(fwd, n, h, bx, by, bz);
+        const float back = sample<LOC, POW2>(fwd, n, h, bx, by, bz, ih);
         const float corrected = f0 + 0.5f * (__ldg(src + i) - back);
         const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y), ez = n + (LOC == FACE_Z);
-        const int gx = donor<LOC == FACE_X>(fx, h, n);
-        const int gy = donor<LOC == FACE_Y>(fy, h, n);
-        const int gz = donor<LOC == FACE_Z>(fz, h, n);
+        const int gx = donor<LOC == FACE_X, POW2>(fx, h, ih, n);
+        const int gy = donor<LOC == FACE_Y, POW2>(fy, h, ih, n);
+        const int gz = donor<LOC == FACE_Z, POW2>(fz, h, ih, n);
         const int x1 = min(gx + 1, ex - 1), y1 = min(gy + 1, ey - 1), z1 = min(gz + 1, ez - 1);
         const float s000 = __ldg(src + index_of(n, LOC, gx, gy, gz));
         float lo = s000, hi = s000;
@@ -108,20 +102,105 @@ __global__ void __launch_bounds__(kThreads) k_advect_maccormack(Grid g, float dt
     out[i] = result * post_scale;
 }
 
-template <int LOC>
+// Grid row blockIdx.y -> (field of the set, z plane); blockIdx.x * blockDim.x
+// + threadIdx.x -> (x, y) within that field's plane. FACES: the set is u, v,
+// w (planes n, n and n + 1); otherwise the smoke (n planes).
+template <bool FACES, bool MC, bool POW2>
+__global__ void __launch_bounds__(kThreads) k_advect_set(Grid g, float dt, float cfl_limit, FieldSet f,
+                                                         const float* __restrict__ u, const float* __restrict__ v,
+                                                         const float* __restrict__ w, float post_scale) {
+    const int n = g.n;
+    const float ih = POW2 ? 1.f / g.h : 0.f;
+    int field = 0, z = int(blockIdx.y);
+    if (FACES) {
+        field = z < n ? 0 : (z < 2 * n ? 1 : 2);
+        z -= field * n;
+    }
+    const int xy = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int ex = n + (FACES && field == 0), ey = n + (FACES && field == 1);
+    if (xy >= ex * ey) return;
+    const int y = xy / ex, x = xy - y * ex;
+    const float* src = f.src[field];
+    float* out = MC ? f.out[field] : f.fwd[field];
+    if (!FACES) {
+        if (MC) maccormack_point<CELL, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, post_scale);
+        else forward_point<CELL, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, post_scale);
+    } else if (field == 0) {
+        if (MC) maccormack_point<FACE_X, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, 1.f);
+        else forward_point<FACE_X, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+    } else if (field == 1) {
+        if (MC) maccormack_point<FACE_Y, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[1], u, v, w, out, 1.f);
+        else forward_point<FACE_Y, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+    } else {
+        if (MC) maccormack_point<FACE_Z, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[2], u, v, w, out, 1.f);
+        else forward_point<FACE_Z, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+    }
+}
+
+// One location at a time (staged calls): the same device code, one field.
+template <int LOC, bool MC, bool POW2>
+__global__ void __launch_bounds__(kThreads) k_advect_one(Grid g, float dt, float cfl_limit,
+                                                         const float* __restrict__ src,
+                                                         const float* __restrict__ fwd,
+                                                         const float* __restrict__ u, const float* __restrict__ v,
+                                                         const float* __restrict__ w, float* __restrict__ out,
+                                                         float post_scale) {
+    const int n = g.n;
+    const float ih = POW2 ? 1.f / g.h : 0.f;
+    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
+    const int xy = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (xy >= ex * ey) return;
+    const int z = int(blockIdx.y), y = xy / ex, x = xy - y * ex;
+    if (MC) maccormack_point<LOC, POW2>(g, ih, dt, cfl_limit, x, y, z, src, fwd, u, v, w, out, post_scale);
+    else forward_point<LOC, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, post_scale);
+}
+
+bool power_of_two(float h) {
+    int e = 0;
+    return std::isfinite(h) && h > 0.f && std::frexp(h, &e) == 0.5f;
+}
+
+template <bool FACES, bool POW2>
+void advect_set(const Grid& g, float dt, float cfl_limit, bool maccormack, const FieldSet& f, const float* u,
+                const float* v, const float* w, float post_scale, cudaStream_t s) {
+    const int n = g.n;
+    const int plane = FACES ? (n + 1) * n : n * n;
+    const dim3 grid((plane + kThreads - 1) / kThreads, FACES ? 3 * n + 1 : n);
+    count_launch();
+    k_advect_set<FACES, false, POW2><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, f, u, v, w,
+                                                               maccormack ? 1.f : post_scale);
+    if (!maccormack) return;
+    count_launch();
+    k_advect_set<FACES, true, POW2><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, f, u, v, w, post_scale);
+}
+
+template <int LOC, bool POW2>
 void advect_loc(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* src, const float* u,
                 const float* v, const float* w, float* fwd, float* out, float post_scale, cudaStream_t s) {
     const int ex = extent(g.n, LOC, 0), ey = extent(g.n, LOC, 1), ez = extent(g.n, LOC, 2);
     const dim3 grid((ex * ey + kThreads - 1) / kThreads, ez);
     if (!maccormack) {
         count_launch();
-        k_advect_forward<LOC><<<grid, kThreads, 0, s>>>(g, dt, src, u, v, w, out, post_scale);
+        k_advect_one<LOC, false, POW2><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, src, nullptr, u, v, w, out,
+                                                                 post_scale);
         return;
     }
     count_launch();
-    k_advect_forward<LOC><<<grid, kThreads, 0, s>>>(g, dt, src, u, v, w, fwd, 1.f);
+    k_advect_one<LOC, false, POW2><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, src, nullptr, u, v, w, fwd, 1.f);
     count_launch();
-    k_advect_maccormack<LOC><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, src, fwd, u, v, w, out, post_scale);
+    k_advect_one<LOC, true, POW2><<<grid, kThreads, 0, s>>>(g, dt, cfl_limit, src, fwd, u, v, w, out, post_scale);
+}
+
+template <bool POW2>
+void advect_any(const Grid& g, int loc, float dt, float cfl_limit, bool maccormack, const float* src,
+                const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
+                cudaStream_t s) {
+    switch (loc) {
+        case CELL: advect_loc<CELL, POW2>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
+        case FACE_X: advect_loc<FACE_X, POW2>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
+        case FACE_Y: advect_loc<FACE_Y, POW2>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
+        default: advect_loc<FACE_Z, POW2>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
+    }
 }
 
 }  // namespace
@@ -129,12 +208,22 @@ void advect_loc(const Grid& g, float dt, float cfl_limit, bool maccormack, const
 void launch_advect(const Grid& g, int loc, float dt, float cfl_limit, bool maccormack, const float* src,
                    const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
                    cudaStream_t s) {
-    switch (loc) {
-        case CELL: advect_loc<CELL>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
-        case FACE_X: advect_loc<FACE_X>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
-        case FACE_Y: advect_loc<FACE_Y>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
-        default: advect_loc<FACE_Z>(g, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s); break;
+    if (power_of_two(g.h)) advect_any<true>(g, loc, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s);
+    else advect_any<false>(g, loc, dt, cfl_limit, maccormack, src, u, v, w, fwd, out, post_scale, s);
+}
+
+void launch_advect_velocity(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* const src[3],
+                            const float* u, const float* v, const float* w, float* const fwd[3],
+                            float* const out[3], cudaStream_t s) {
+    FieldSet f;
+    for (int c = 0; c < 3; ++c) {
+        f.src[c] = src[c];
+        // without MacCormack the forward pass is the result
+        f.fwd[c] = maccormack ? fwd[c] : out[c];
+        f.out[c] = out[c];
     }
+    if (power_of_two(g.h)) advect_set<true, true>(g, dt, cfl_limit, maccormack, f, u, v, w, 1.f, s);
+    else advect_set<true, false>(g, dt, cfl_limit, maccormack, f, u, v, w, 1.f, s);
 }
 
 }  // namespace vb

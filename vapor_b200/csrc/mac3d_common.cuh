@@ -43,6 +43,15 @@ __device__ __forceinline__ int clampi_ref(int v, int lo, int hi) { return v < lo
 __device__ __forceinline__ float minf_ref(float a, float b) { return b < a ? b : a; }  // std::min
 __device__ __forceinline__ float maxf_ref(float a, float b) { return a < b ? b : a; }  // std::max
 
+// Division by the cell size as the reference writes it, coord / h, or, when h
+// is a power of two, coord * (1 / h): 1 / h is then exact, so both forms round
+// the same real quotient to the same float (also for subnormal results) and
+// the multiplication saves the IEEE division's instruction sequence.
+template <bool POW2>
+__device__ __forceinline__ float div_h(float coord, float h, float ih) {
+    return POW2 ? coord * ih : coord / h;
+}
+
 // One axis of the clamped trilinear lookup (MacGridSampler3D.cpp:6-11 and the
 // staggered variants :23-28, :42-47, :61-66).
 struct Bracket {
@@ -50,16 +59,16 @@ struct Bracket {
     float t;
 };
 
-template <bool STAGGERED>
-__device__ __forceinline__ Bracket bracket(float coord, float h, int n) {
+template <bool STAGGERED, bool POW2 = false>
+__device__ __forceinline__ Bracket bracket(float coord, float h, int n, float ih = 0.f) {
     Bracket b;
     if (STAGGERED) {
-        const float g = clampf_ref(coord / h, 0.f, float(n));
+        const float g = clampf_ref(div_h<POW2>(coord, h, ih), 0.f, float(n));
         b.i0 = min(int(g), n - 1);
         b.i1 = b.i0 + 1;
         b.t = g - float(b.i0);
     } else {
-        const float g = clampf_ref(coord / h - 0.5f, 0.f, float(n - 1));
+        const float g = clampf_ref(div_h<POW2>(coord, h, ih) - 0.5f, 0.f, float(n - 1));
         b.i0 = int(g);
         b.i1 = min(b.i0 + 1, n - 1);
         b.t = g - float(b.i0);
@@ -67,24 +76,9 @@ __device__ __forceinline__ Bracket bracket(float coord, float h, int n) {
     return b;
 }
 
-// Trilinear sample of a field at location LOC, world position (px,py,pz), with
-// the reference's fixed 8-term order and left-to-right products.
-template <int LOC>
-__device__ __forceinline__ float sample(const float* __restrict__ f, int n, float h, float px, float py,
-                                        float pz) {
-    const Bracket bx = bracket<LOC == FACE_X>(px, h, n);
-    const Bracket by = bracket<LOC == FACE_Y>(py, h, n);
-    const Bracket bz = bracket<LOC == FACE_Z>(pz, h, n);
-    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
-    const size_t r00 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i0));
-    const size_t r10 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i0));
-    const size_t r01 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i1));
-    const size_t r11 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i1));
-    const float f000 = __ldg(f + r00 + bx.i0), f100 = __ldg(f + r00 + bx.i1);
-    const float f010 = __ldg(f + r10 + bx.i0), f110 = __ldg(f + r10 + bx.i1);
-    const float f001 = __ldg(f + r01 + bx.i0), f101 = __ldg(f + r01 + bx.i1);
-    const float f011 = __ldg(f + r11 + bx.i0), f111 = __ldg(f + r11 + bx.i1);
-    const float tx = bx.t, ty = by.t, tz = bz.t;
+// The reference's fixed 8-term trilinear sum with left-to-right products.
+__device__ __forceinline__ float trilinear(float f000, float f100, float f010, float f110, float f001, float f101,
+                                           float f011, float f111, float tx, float ty, float tz) {
     const float ux = 1.f - tx, uy = 1.f - ty, uz = 1.f - tz;
     float s = f000 * ux * uy * uz;
     s = s + f100 * tx * uy * uz;
@@ -95,6 +89,24 @@ __device__ __forceinline__ float sample(const float* __restrict__ f, int n, floa
     s = s + f011 * ux * ty * tz;
     s = s + f111 * tx * ty * tz;
     return s;
+}
+
+// Trilinear sample of a field at location LOC, world position (px,py,pz), with
+// the reference's fixed 8-term order and left-to-right products.
+template <int LOC, bool POW2 = false>
+__device__ __forceinline__ float sample(const float* __restrict__ f, int n, float h, float px, float py,
+                                        float pz, float ih = 0.f) {
+    const Bracket bx = bracket<LOC == FACE_X, POW2>(px, h, n, ih);
+    const Bracket by = bracket<LOC == FACE_Y, POW2>(py, h, n, ih);
+    const Bracket bz = bracket<LOC == FACE_Z, POW2>(pz, h, n, ih);
+    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
+    const size_t r00 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i0));
+    const size_t r10 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i0));
+    const size_t r01 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i1));
+    const size_t r11 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i1));
+    return trilinear(__ldg(f + r00 + bx.i0), __ldg(f + r00 + bx.i1), __ldg(f + r10 + bx.i0),
+                     __ldg(f + r10 + bx.i1), __ldg(f + r01 + bx.i0), __ldg(f + r01 + bx.i1),
+                     __ldg(f + r11 + bx.i0), __ldg(f + r11 + bx.i1), bx.t, by.t, bz.t);
 }
 
 // Red-black split storage of the projection's cell arrays (b, p, e, r32,
@@ -123,13 +135,14 @@ struct Vel {
 };
 
 // MacGridSampler3D::velocity (MacGridSampler3D.cpp:73-75).
+template <bool POW2 = false>
 __device__ __forceinline__ Vel velocity_at(const float* __restrict__ u, const float* __restrict__ v,
                                            const float* __restrict__ w, int n, float h, float px, float py,
-                                           float pz) {
+                                           float pz, float ih = 0.f) {
     Vel r;
-    r.x = sample<FACE_X>(u, n, h, px, py, pz);
-    r.y = sample<FACE_Y>(v, n, h, px, py, pz);
-    r.z = sample<FACE_Z>(w, n, h, px, py, pz);
+    r.x = sample<FACE_X, POW2>(u, n, h, px, py, pz, ih);
+    r.y = sample<FACE_Y, POW2>(v, n, h, px, py, pz, ih);
+    r.z = sample<FACE_Z, POW2>(w, n, h, px, py, pz, ih);
     return r;
 }
 
