@@ -354,6 +354,11 @@ vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch);
 /* Tuning (extension): z chunks per blocked launch for grids of size n (0 =
  * automatic: one wave of resident CTAs). Results do not depend on it. */
 vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks);
+/* Tuning (extension): 1 (default) runs the learned network's 3x3x3
+ * convolutions that fit in shared memory on the warp-specialised tcgen05
+ * kernel (producer, MMA and epilogue warps on mbarriers), 0 on the
+ * block-synchronous z-marching kernel. Same results either way. */
+vapor_status vapor_tune_conv_kernel(int32_t warp_specialised);
 
 /* ---- Batched scenes (extension, no reference counterpart) ----
  * Steps many resident simulations (uneven grid sizes allowed, each with its

@@ -128,12 +128,42 @@ def test_forward_matches_torch_reference(n):
     assert err < 2e-2, err  # BF16 activations: a few rounding flips propagate
 
 
-def test_bounded_wait_that_runs_out_reports_an_error_and_recovers():
+@pytest.mark.parametrize("n", [16, 32, 64])
+def test_warp_specialised_convolutions_equal_block_synchronous(n):
+    """The warp-specialised convolution kernel (producer / MMA / epilogue
+    warps on mbarriers) against the block-synchronous z-marching kernel: the
+    same MMAs on the same operands, so the network's outputs and parameter
+    gradients are bit-identical."""
+    import torch
+    net = Net(seed=13)
+    x = features(n, 21)
+    xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+    g = torch.tensor(np.random.default_rng(2).standard_normal(n ** 3).astype(np.float32)).cuda()
+    outs, grads = [], []
+    try:
+        for ws in (0, 1):
+            vb.tune_conv_kernel(ws)
+            out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+            vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+            gp = np.zeros(net.P, np.float32)
+            vb.check(net.lib.vapor_unet_backward(net.h, n, g.data_ptr(), gp.ctypes.data))
+            outs.append(out.cpu().numpy())
+            grads.append(gp)
+    finally:
+        vb.tune_conv_kernel(1)
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(grads[0].view(np.uint32), grads[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("ws", [0, 1])
+def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     """The convolutions' completion waits poll an mbarrier with an iteration
     limit. With the test hook they poll one that nothing completes, run out,
     drain their MMAs and free TMEM: the call reports VAPOR_RUNTIME_ERROR and
-    the next normal call gives the same output as before."""
+    the next normal call gives the same output as before (both convolution
+    kernels)."""
     import torch
+    vb.tune_conv_kernel(ws)
     net = Net(seed=5)
     n = 8
     xin = torch.tensor(features(n, 9)).to(torch.bfloat16).cuda().contiguous()
@@ -148,6 +178,7 @@ def test_bounded_wait_that_runs_out_reports_an_error_and_recovers():
     vb.check(net.lib.vapor_unet_set_wait_probe(net.h, 0))
     after = torch.zeros_like(before)
     vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), after.data_ptr()))
+    vb.tune_conv_kernel(1)
     assert torch.equal(after, before)
 
 

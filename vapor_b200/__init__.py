@@ -112,6 +112,7 @@ def _declare(lib):
     f("vapor_tune_sor_planes", C.c_int32, C.c_int32)
     f("vapor_tune_sor_blocking", C.c_int32)
     f("vapor_tune_sor_blocked_chunks", C.c_int32, C.c_int32)
+    f("vapor_tune_conv_kernel", C.c_int32)
     f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_batch_destroy", _vp)
     f("vapor_batch_advance", _vp, C.c_float)
@@ -349,6 +350,12 @@ def tune_sor_blocking(iterations_per_launch):
     """Red+black iterations per temporally blocked sweep launch (1 or 2; 0:
     one launch per colour). Same results either way."""
     check(library().vapor_tune_sor_blocking(int(iterations_per_launch)))
+
+
+def tune_conv_kernel(warp_specialised):
+    """1: warp-specialised tcgen05 convolutions (default); 0: block-synchronous
+    z-marching ones. Same results either way."""
+    check(library().vapor_tune_conv_kernel(int(warp_specialised)))
 
 
 def tune_sor_blocked_chunks(n, chunks):

@@ -55,6 +55,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int lim
     return false;
 }
 
+// Bounded wait that also gives up when another role of the CTA has set
+// *abort (a timeout elsewhere): false on timeout or abort.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, int limit,
+                                                   const volatile int* abort) {
+    for (int i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(bar) : "memory");
+}
+// Arrives on the mbarrier once all of this thread's earlier cp.async copies
+// have landed (the barrier's expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(dst_smem), "r"(ncols)
                  : "memory");

@@ -51,6 +51,9 @@ struct WGradArgs {
 
 // Sets the kernels' shared-memory limits (once per device, before use).
 void configure_conv_kernels();
+// Selects the warp-specialised convolution kernel (default) or the
+// block-synchronous one for every later launch (same results).
+void set_conv_warp_specialised(bool on);
 void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
 void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,

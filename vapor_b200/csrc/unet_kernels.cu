@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "kernels.hpp"
 #include "tc_conv.cuh"
@@ -23,6 +24,10 @@ namespace unet {
 namespace {
 
 constexpr int kWaitLimit = 1 << 22;
+
+// Convolutions that fit take the warp-specialised kernel (else the
+// block-synchronous z-marching one); both give the same results.
+std::atomic<bool> g_conv_ws{true};
 
 __device__ __forceinline__ void decode(long v, int H, int W, int& x, int& y, int& z) {
     x = int(v % W);
@@ -378,6 +383,220 @@ __global__ void __launch_bounds__(256) k_conv3_zm(ConvArgs a, int zt, int ring) 
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, Z::kCols);
+}
+
+// Warp-specialised form of the z-marching convolution. The CTA's roles run
+// as a pipeline on mbarriers, with no block-wide barrier inside the march:
+//   warp 0 (producer): loads halo plane q (all chunks, cp.async with zero
+//     fill) into ring slot q % ring once the MMAs that read the slot's previous
+//     plane are complete (`empty`), and signals `full` when its copies land;
+//   warp 1 (MMA, one lane): for plane z waits for planes z - 1 .. z + 1 and
+//     for accumulator k = plane & 1 to be drained (`acc_empty`), issues the
+//     27 x chunks MMAs into it, then commits to `acc_full[k]` and to the
+//     `empty` barrier of plane z - 1's slot (its last reader);
+//   warps 2-5 (epilogue): wait for `acc_full[k]`, read their 32 TMEM lanes
+//     (all N columns), add bias, ReLU, store, and arrive on `acc_empty[k]`.
+// The weights stay resident as in k_conv3_zm; the A and B operands and the
+// accumulator layout are the same, so results equal k_conv3_zm's. Every wait
+// is bounded; a role that runs out sets the error flag and an abort flag that
+// ends the other roles' waits, after which the MMA lane drains its in-flight
+// MMAs (commit + bounded wait) before TMEM is freed.
+template <int N>
+struct ConvWS {
+    static constexpr int kThreads = 192;
+    static constexpr int kMaxRing = 6;
+    static constexpr int kPlane = 18 * 320;
+    static constexpr uint32_t kCols = TmemColumns<2 * N>::value;
+    static constexpr uint32_t kAcc1 = kCols / 2;
+    static int smem(int cin, int ring) { return 27 * N * cin * 2 + ring * (cin / 16) * kPlane + 1024; }
+    static bool fits(int cin, int ring) { return smem(cin, ring) <= 200 * 1024; }
+};
+
+// Epilogue of one plane for one warp: TMEM lanes 32 quarter .. + 31 (voxel
+// m = lane index within the 8 x 16 tile), all N accumulator columns.
+template <int N>
+__device__ __forceinline__ void ws_epilogue(const ConvArgs& a, uint32_t acc, const float* s_bias, int x0, int y0,
+                                            int z, int quarter, int lane) {
+    const int m = quarter * 32 + lane;
+    const int x = x0 + (m & 7), y = y0 + (m >> 3);
+    const bool vin = x < a.W && y < a.H;
+    const long v = (long(z) * a.H + y) * a.W + x;
+    const uint32_t lane_base = uint32_t(quarter * 32) << 16;
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 8) {
+        float val[8];
+        tc::tmem_ld8(acc + lane_base + uint32_t(c0), val);
+        if (vin) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                val[i] += s_bias[c0 + i];
+                if (a.relu) val[i] = fmaxf(val[i], 0.f);
+            }
+            const long o = v * a.out_stride + a.out_offset + c0;
+            if (a.out_fp32) {
+                float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.out) + o);
+                dst[0] = make_float4(val[0], val[1], val[2], val[3]);
+                dst[1] = make_float4(val[4], val[5], val[6], val[7]);
+            } else {
+                __align__(16) __nv_bfloat16 hv[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) hv[i] = __float2bfloat16_rn(val[i]);
+                *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.out) + o) =
+                    *reinterpret_cast<const uint4*>(hv);
+            }
+        }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(ConvWS<N>::kThreads) k_conv3_ws(ConvArgs a, int zt, int ring) {
+    using W = ConvWS<N>;
+    extern __shared__ uint8_t smem_raw[];
+    // full[6], empty[6], acc_full[2], acc_empty[2], drain, probe
+    __shared__ __align__(8) uint64_t bars[2 * W::kMaxRing + 6];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    __shared__ float s_bias[N];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16;
+    const int z0 = blockIdx.z * zt, z1 = min(a.D, z0 + zt);
+    const int planes = z1 - z0;    // MMA / epilogue steps
+    const int loads = planes + 2;  // halo planes z0 - 1 .. z1
+    const int chunks = a.cin / 16;
+    const uint32_t sbase = tc::smem_addr(smem);
+    const uint32_t wbase = sbase;
+    const uint32_t rbase = sbase + uint32_t(27 * N * a.cin * 2);
+    const uint32_t plane_bytes = uint32_t(chunks * W::kPlane);
+    const uint32_t b0 = tc::smem_addr(&bars[0]);
+    auto full = [&](int s) { return b0 + uint32_t(8 * s); };
+    auto empty = [&](int s) { return b0 + uint32_t(8 * (W::kMaxRing + s)); };
+    auto acc_full = [&](int k) { return b0 + uint32_t(8 * (2 * W::kMaxRing + k)); };
+    auto acc_empty = [&](int k) { return b0 + uint32_t(8 * (2 * W::kMaxRing + 2 + k)); };
+    const uint32_t drain = b0 + uint32_t(8 * (2 * W::kMaxRing + 4));
+    const uint32_t probe = b0 + uint32_t(8 * (2 * W::kMaxRing + 5));
+    volatile int* abort_v = &abort_flag;
+
+    if (tid == 0) {
+        for (int s = 0; s < ring; ++s) {
+            tc::mbar_init(full(s), 32);  // one cp.async arrival per producer lane
+            tc::mbar_init(empty(s), 1);
+        }
+        tc::mbar_init(acc_full(0), 1);
+        tc::mbar_init(acc_full(1), 1);
+        tc::mbar_init(acc_empty(0), 4);  // one arrival per epilogue warp
+        tc::mbar_init(acc_empty(1), 4);
+        tc::mbar_init(drain, 1);
+        tc::mbar_init(probe, 1);
+        tc::fence_mbarrier_init();
+        abort_flag = 0;
+    }
+    if (warp == 1) tc::tmem_alloc(tc::smem_addr(&tmem_slot), W::kCols);
+    for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
+    // all weights: (chunk, tap, co, half) segments of 16 bytes
+    for (int i = tid; i < chunks * 27 * N * 2; i += blockDim.x) {
+        const int half = i & 1, co = (i >> 1) % N, ct = (i >> 1) / N;  // ct = chunk * 27 + tap
+        const int t = ct % 27, cc = ct / 27;
+        const __nv_bfloat16* wsrc = a.w + (long(t) * N + co) * a.cin + cc * 16 + half * 8;
+        tc::cp_async16(wbase + uint32_t(ct * N * 32 + (co >> 3) * 256 + half * 128 + (co & 7) * 16), wsrc, true);
+    }
+    tc::cp_async_commit();
+    tc::cp_async_wait_all();
+    tc::fence_proxy_async();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    bool ok = true;
+
+    if (warp == 0) {
+        // producer: halo plane zz = z0 - 1 + q into slot q % ring
+        for (int q = 0; q < loads; ++q) {
+            const int slot = q % ring;
+            if (q >= ring) {  // the slot's previous plane q - ring is last read by the MMAs of step q - ring
+                const bool got =
+                    tc::mbar_wait_or_abort(empty(slot), uint32_t((q / ring - 1) & 1), kWaitLimit, abort_v);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
+            }
+            const int zz = z0 - 1 + q;
+            const uint32_t dst = rbase + uint32_t(slot) * plane_bytes;
+            for (int i = lane; i < chunks * 18 * 20; i += 32) {
+                const int half = i & 1, v = (i >> 1) % 10, rc = (i >> 1) / 10;  // rc = chunk * 18 + ry
+                const int ry = rc % 18, cc = rc / 18;
+                const int x = x0 - 1 + v, y = y0 + ry - 1;
+                const bool valid = x >= 0 && x < a.W && y >= 0 && y < a.H && zz >= 0 && zz < a.D;
+                const __nv_bfloat16* src =
+                    valid ? a.in + ((long(zz) * a.H + y) * a.W + x) * a.in_stride + cc * 16 + half * 8 : a.in;
+                tc::cp_async16(dst + uint32_t(rc * 320 + half * 160 + v * 16), src, valid);
+            }
+            tc::cp_async_arrive(full(slot));
+        }
+        tc::cp_async_wait_all();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = tc::instr_desc_bf16(128, N);
+            const uint64_t a_desc = tc::smem_desc(rbase, 160, 320);
+            const uint64_t b_desc = tc::smem_desc(wbase, 128, 256);
+            for (int j = 0; j < planes && ok; ++j) {
+                // planes j .. j + 2 (z - 1 .. z + 1) have landed; the first
+                // two were waited for in earlier steps
+                for (int q = (j == 0 ? 0 : j + 2); q <= j + 2 && ok; ++q) {
+                    ok = a.wait_probe ? tc::mbar_wait_or_abort(probe, 0u, a.wait_probe, abort_v)
+                                      : tc::mbar_wait_or_abort(full(q % ring), uint32_t((q / ring) & 1), kWaitLimit,
+                                                               abort_v);
+                }
+                const int k = j & 1;
+                if (ok && j >= 2)
+                    ok = tc::mbar_wait_or_abort(acc_empty(k), uint32_t(((j - 2) >> 1) & 1), kWaitLimit, abort_v);
+                if (!ok) break;
+                tc::fence_proxy_async();  // cp.async data -> tensor core (async proxy)
+                tc::tc_fence_after();
+                const uint32_t dz_bytes[3] = {uint32_t(j % ring) * plane_bytes, uint32_t((j + 1) % ring) * plane_bytes,
+                                              uint32_t((j + 2) % ring) * plane_bytes};
+#pragma unroll 1
+                for (int cc = 0; cc < chunks; ++cc)
+                    issue_taps<N>(tmem + uint32_t(k) * W::kAcc1, a_desc + uint32_t(cc * (W::kPlane >> 4)), dz_bytes,
+                                  b_desc + uint32_t(cc * 27 * N * 2), idesc, cc > 0);
+                tc::mma_commit(acc_full(k));
+                tc::mma_commit(empty(j % ring));  // plane j (z - 1) has no later reader
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+    } else {
+        // epilogue warps 2..5 -> TMEM lane quarters 2, 3, 0, 1
+        const int quarter = warp & 3;
+        for (int j = 0; j < planes; ++j) {
+            const int k = j & 1;
+            const bool got = tc::mbar_wait_or_abort(acc_full(k), uint32_t((j >> 1) & 1), kWaitLimit, abort_v);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            tc::tc_fence_after();
+            ws_epilogue<N>(a, tmem + uint32_t(k) * W::kAcc1, s_bias, x0, y0, z0 + j, quarter, lane);
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(acc_empty(k));
+        }
+    }
+    if (!ok) {
+        *abort_v = 1;
+        if (lane == 0) atomicOr(a.error, 1u);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (tid == 32) {
+        // every MMA this thread issued is complete before TMEM is freed
+        tc::mma_commit(drain);
+        if (!tc::mbar_wait(drain, 0u, kWaitLimit)) atomicOr(a.error, 2u);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    if (warp == 1) tc::tmem_dealloc(tmem, W::kCols);
 }
 
 // ---- CUDA-core kernels -------------------------------------------------------
@@ -851,6 +1070,16 @@ void configure_n() {
     VB_CUDA(cudaFuncSetAttribute(k_conv3_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  ConvTile<N>::kSmemMax));
     VB_CUDA(cudaFuncSetAttribute(k_conv3_zm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_ws<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+}
+
+// Resident CTAs per SM of the warp-specialised convolution: shared memory,
+// threads, and the 512 TMEM columns (two accumulators per CTA).
+template <int N>
+int resident_ws(int smem) {
+    constexpr int kSmemPerSm = 228 * 1024, kPerCta = 1024 + 512;
+    return std::max(1, std::min({2048 / ConvWS<N>::kThreads, 512 / int(ConvWS<N>::kCols),
+                                 kSmemPerSm / (smem + kPerCta)}));
 }
 
 template <int N>
@@ -859,7 +1088,19 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
         fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
     const unsigned gx = unsigned((a.W + 7) / 8), gy = unsigned((a.H + 15) / 16);
     count_launch();
-    if (ConvMarch<N>::fits(a.cin, 4)) {
+    if (g_conv_ws.load() && ConvWS<N>::fits(a.cin, 4)) {
+        // planes per CTA: the smallest power of two (at least 2, up to 16)
+        // whose grid runs in one wave of resident CTAs; the 6-plane ring when
+        // it fits without lowering the resident count
+        const int ring = (ConvWS<N>::fits(a.cin, 6) &&
+                          resident_ws<N>(ConvWS<N>::smem(a.cin, 6)) == resident_ws<N>(ConvWS<N>::smem(a.cin, 4)))
+                             ? 6 : 4;
+        const long slots = long(resident_ws<N>(ConvWS<N>::smem(a.cin, ring))) * device_sm_count();
+        int zt = 2;
+        while (zt < 16 && long(gx) * gy * ((a.D + zt - 1) / zt) > slots) zt <<= 1;
+        const dim3 grid(gx, gy, unsigned((a.D + zt - 1) / zt));
+        k_conv3_ws<N><<<grid, ConvWS<N>::kThreads, ConvWS<N>::smem(a.cin, ring), s>>>(a, zt, ring);
+    } else if (ConvMarch<N>::fits(a.cin, 4)) {
         // planes per CTA: the smallest power of two (up to 16) whose grid runs
         // in one wave of resident CTAs; the 6-plane ring when it fits, keeps
         // that plane count and the CTAs march at least 4 planes
@@ -880,6 +1121,8 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
 }
 
 }  // namespace
+
+void set_conv_warp_specialised(bool on) { g_conv_ws.store(on); }
 
 void configure_conv_kernels() {
     configure_n<16>();
