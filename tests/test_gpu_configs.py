@@ -118,3 +118,71 @@ def test_reflection_plume_scene_matches_oracle_mixed_solve():
         assert got.final_residual <= 1e-6 * got.initial_residual
     for x, y in zip(sim.download(), ref.fields()):
         assert bits_equal(x, y)
+
+
+def test_reflection_plume_128_matches_oracle_and_fp64_error():
+    """The Reflection-MacCormack plume configuration at its own size, 128^3:
+    three steps with the mixed-precision solve to relative divergence 1e-6,
+    bit for bit against the FP32 oracle with equal iteration counts; then one
+    step from the GPU's state against the FP64 oracle (the same step in
+    double), with the max relative error of every field stated and bounded
+    by 1e-5, the per-step FP32 bar."""
+    n = 128
+    p = scene_params(vb.default_params(), n, rel=1e-6, max_iterations=20000)
+    fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=5)]
+    sim = vb.MacSimulation3D(n, 1.0, p)
+    sim.upload(*fields)
+    ref = OracleSim(n, 1.0)
+    ref.params = p
+    ref.set_fields(*fields)
+    for _ in range(3):
+        assert ref.advance(DT) == 0
+        sim.advance(DT)
+        got, want = sim.last_projection().linear_solve, ref.last_projection().linear_solve
+        assert got.iterations == want.iterations and got.converged
+        assert got.final_residual <= 1e-6 * got.initial_residual
+    state = sim.download()
+    for x, y in zip(state, ref.fields()):
+        assert bits_equal(x, y)
+    f64 = OracleSim(n, 1.0, dtype=np.float64)
+    f64.params = p
+    f64.set_fields(*[x.astype(np.float64) for x in state])
+    sim.advance(DT)
+    assert f64.advance(DT) == 0
+    errs = {}
+    for name, x, y in zip(("density", "u", "v", "w"), sim.download(), f64.fields()):
+        errs[name] = float(np.abs(x.astype(np.float64) - y).max() / max(1e-30, float(np.abs(y).max())))
+    print("128^3 plume step vs FP64 oracle, max relative error:", errs)
+    assert max(errs.values()) <= 1e-5, errs
+
+
+def test_plume_256_learned_arm_matches_plain_arm():
+    """The benchmark's two arms at 256^3 from the same state: the learned
+    solver (flexible PCG with the coarse network) and the plain red-black SOR,
+    both to relative divergence 1e-6 (FP64-verified). After two steps the
+    fields differ only by what two 1e-6 solves allow: the max difference of
+    every field relative to its max is stated and bounded by 1e-4."""
+    from vapor_b200.abi import SOLVER_FPCG
+    from vapor_b200.learned import COARSE_WEIGHTS, WarmStartNet
+    n = 256
+    fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=2024)]
+    net = WarmStartNet.load(COARSE_WEIGHTS)
+    outs = {}
+    for kind in (SOLVER_MIXED_REFINEMENT, SOLVER_FPCG):
+        p = scene_params(vb.default_params(), n, rel=1e-6, max_iterations=20000)
+        p.solver_kind = kind
+        sim = vb.MacSimulation3D(n, 1.0, p)
+        sim.upload(*fields)
+        if kind == SOLVER_FPCG:
+            sim.set_preconditioner(net)
+        for _ in range(2):
+            sim.advance(DT)
+            ls = sim.last_projection().linear_solve
+            assert ls.converged and ls.final_residual <= 1e-6 * ls.initial_residual
+        outs[kind] = sim.download()
+        sim.close()
+    diffs = {}
+    for name, a, b in zip(("density", "u", "v", "w"), outs[SOLVER_MIXED_REFINEMENT], outs[SOLVER_FPCG]):
+        diffs[name] = float(np.abs(a.astype(np.float64) - b).max() / max(1e-30, float(np.abs(a).max())))
+    print("256^3 learned vs plain after 2 steps, max relative difference:", diffs)
+    assert max(diffs.values()) <= 1e-4, diffs
