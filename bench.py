@@ -399,7 +399,7 @@ def main():
 
     # Plain arm: the reference's red-black SOR (mixed precision to reach 1e-6).
     plain_sim, _, plain = run_arm(vb, torch, args, n, fields, SOLVER_MIXED_REFINEMENT, None, dist)
-    plain_phases, _, _ = eager_phases(vb, plain_sim, 1)
+    plain_phases, _, plain_eager_sweeps = eager_phases(vb, plain_sim, 1)
     plain_sim.close()
     # Learned arm (headline): flexible PCG with the U-Net coarse-grid correction.
     clocks = ClockSampler(local)
@@ -430,22 +430,32 @@ def main():
     peak, peak_kind = measured_peaks()
     cells = n ** 3
 
-    def sor_roofline(ph):
+    def sor_roofline(ph, sweeps):
+        """The red-black sweep phase of one eager step covering `sweeps`
+        red+black iterations: per-launch algorithmic bytes over the average
+        launch time. A one-colour launch moves 6 B/cell (its colour's x and b,
+        the other colour's x, its x written); a temporally blocked launch of
+        several iterations reads x and b and writes x once, 12 B/cell."""
         sor = ph["sor"]
-        launch_ms = sor["ms"] / max(1, sor["launches"])
-        # one colour launch reads its colour's p and b, the other colour's p,
-        # and writes its p: 6 B/cell compulsory (12 B/cell per iteration)
-        nbytes = 6.0 * cells
+        launches = max(1, sor["launches"])
+        launch_ms = sor["ms"] / launches
+        per_launch = sweeps / launches
+        blocked = per_launch >= 1.5
+        nbytes = (12.0 if blocked else 6.0) * cells
         achieved = nbytes / (launch_ms * 1e-3) / 1e9
-        return {"bound": "hbm", "kernel": "k_sor_rbz (red-black colour sweep)", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": SOR_TRAFFIC_256 * cells / 256 ** 3,
-                "traffic_note": "dram bytes read + written per launch from an ncu --set full capture at 256^3, "
-                                "scaled by cells for other sizes",
+        line = {"bound": "hbm", "kernel": (f"k_sor_blocked ({per_launch:.0f} red+black iterations per launch)"
+                                           if blocked else "k_sor_rbz (red-black colour sweep)"),
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": None if blocked else SOR_TRAFFIC_256 * cells / 256 ** 3,
+                "traffic_note": ("see profiles/ for the blocked sweep's ncu traffic" if blocked else
+                                 "dram bytes read + written per launch from an ncu --set full capture at 256^3, "
+                                 "scaled by cells for other sizes"),
                 "bytes_per_launch": nbytes, "avg_launch_us": launch_ms * 1e3,
-                "timing_note": "average colour-launch time from CUDA events around the sweep phase of an eager "
-                               "replay of the benchmarked step on the simulation's stream (the kernels inside the "
-                               "step's CUDA graph cannot be bracketed one by one); launch gaps included"}
+                "sweeps_per_s": sweeps / (sor["ms"] * 1e-3) if sor["ms"] > 0 else None,
+                "timing_note": "average launch time from CUDA events around the sweep phase of an eager replay of "
+                               "the benchmarked step on the simulation's stream (the kernels inside the step's "
+                               "CUDA graph cannot be bracketed one by one); launch gaps included"}
+        return line
 
     # Network (tensor cores): FLOPs of the coarse U-Net per application over
     # the coarse phase's time per application (restriction, normalization,
@@ -477,13 +487,13 @@ def main():
                   "value": aggregate_steps_per_second(world, args.steps, plain["ms"]), "unit": "steps/s",
                   "ms_per_step": plain["ms"] / args.steps, "sweeps_per_step": plain["iterations"],
                   "omega": omega_for(n, args.omega), "final_relative_residual": plain["final_relative_residual"],
-                  "converged": plain["converged"], "roofline": sor_roofline(plain_phases),
+                  "converged": plain["converged"], "roofline": sor_roofline(plain_phases, plain_eager_sweeps),
                   "phases_ms_per_step": {k: v["ms"] for k, v in plain_phases.items() if v["ms"] > 0}},
         "speedup_vs_plain": plain["ms"] / learned["ms"],
         "sweep_ratio_vs_plain": plain["iterations"] / max(1e-9, 4 * (learned["iterations"] + 2)),
         "gpu_launches": launches,
         "gpu_launches_note": "kernels per step counted on the eager replay of the same step, times steps",
-        "roofline": sor_roofline(phases),
+        "roofline": sor_roofline(phases, 4.0 * (eager_its + 2.0) * roof_steps),
         "roofline_tensor": {"bound": "tensor", "kernel": "coarse U-Net forward (k_conv3_zm and k_conv3_tc, 10 convolutions)",
                             "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
                             "peak_kind": "measured sustained", "flops_per_application": net_flops,

@@ -149,6 +149,7 @@ Workspace::Workspace(int n, float box, cudaStream_t stream)
     const size_t slots = rb_count(n);  // red-black split storage
     b_.allocate(slots);
     p_.allocate(slots);
+    if (sor_blocked_applies(n)) x_alt_.allocate(slots);  // out-of-place blocked sweeps
     fwd_.allocate(faces);
     partial_capacity_ = reduction_blocks(faces);
     partials_.allocate(size_t(partial_capacity_));
@@ -301,7 +302,7 @@ void Workspace::set_solid(const uint8_t* mask) {
 
 void Workspace::ensure_fpcg(bool coarse) {
     const size_t count = rb_count(n_);
-    for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_})
+    for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_, &cg_z2_})
         if (v->n != count) {
             v->allocate(count);
             v->zero(stream_);
@@ -335,6 +336,9 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     // the smoothing pairs run as one temporally blocked launch each when the
     // grid allows (same bits as the one-colour launches)
     const bool blocked = sor_block_iterations(n_) == 2 && kFpcgSmoothing == 2;
+    // z after pre-smoothing and the coarse correction: the twin buffer when
+    // blocked (the post-smoothing launch is out of place), else z itself
+    float* zpre = blocked ? cg_z2_.p : cg_z_.p;
     if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);
     else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
     t.begin(VAPOR_PHASE_RESIDUAL);
@@ -344,8 +348,10 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     auto precondition = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_SOR);
         if (blocked) {
-            // both sweeps in one launch, starting from z = 0 (z is not read)
-            launch_sor_blocked(smooth, kFpcgSmoothing, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false, true);
+            // both sweeps in one launch, starting from z = 0 (no iterate is
+            // read), into the pre-smoothed twin z2
+            launch_sor_blocked(smooth, kFpcgSmoothing, 0, zpre, zpre, r, ctrl_, false, 0, false, st, false, false,
+                               true);
             t.end(VAPOR_PHASE_SOR, 1);
         } else {
             // the first colour sweep starts from z = 0 (and clears the other colour)
@@ -360,18 +366,18 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         }
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
-            launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
+            launch_restrict_residual(n_, r, zpre, cg_rows_.p, cg_rc_.p, st);
             if (coarse_log_)
                 launch_log_coarse(cg_rc_.p, cg_rc_.n, coarse_log_, coarse_log_capacity_, coarse_log_counter_, st);
             coarse->set_stream(st);
             const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
             coarse->set_stream(s);
-            launch_coarse_correction(n_, cg_z_.p, zc, cg_rc_.p, cg_partials_.p, cg_, st);
+            launch_coarse_correction(n_, zpre, zc, cg_rc_.p, cg_partials_.p, cg_, st);
             t.end(VAPOR_PHASE_COARSE, 0);
         }
         t.begin(VAPOR_PHASE_SOR);
         if (blocked) {
-            launch_sor_blocked(smooth, kFpcgSmoothing, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            launch_sor_blocked(smooth, kFpcgSmoothing, 1, zpre, cg_z_.p, r, ctrl_, false, 0, false, st, false);
             t.end(VAPOR_PHASE_SOR, 1);
         } else {
             for (int j = 0; j < kFpcgSmoothing; ++j) {
@@ -469,13 +475,27 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     auto sweeps = [&](cudaStream_t st, int k, int first_index, float* x, const float* rhs, bool subtract_mean,
                       bool measure = false) {
         t.begin(VAPOR_PHASE_SOR);
+        // Temporal blocking: launches of two (or one) red+black iterations,
+        // out of place between x and its twin, an even number of them so
+        // that the result ends in x; else one launch per colour, in place.
         const int per = sor_block_iterations(n_);
+        int n2 = per == 2 ? k / 2 : 0, n1 = per == 2 ? k % 2 : k;
+        if ((n2 + n1) % 2 == 1 && n2 > 0) {
+            --n2;
+            n1 += 2;
+        }
         long long launches = 0;
-        if (per > 0) {  // several red+black iterations per launch (temporal blocking)
-            for (int j = 0; j < k; j += per) {
-                const int it = std::min(per, k - j);
-                launch_sor_blocked(a, it, 0, x, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
+        if (per > 0 && (n2 + n1) % 2 == 0 && x_alt_.p) {
+            const float* src = x;
+            float* dst = x_alt_.p;
+            int j = 0;
+            for (int l = 0; l < n2 + n1; ++l) {
+                const int it = l < n2 ? 2 : 1;
+                launch_sor_blocked(a, it, 0, src, dst, rhs, ctrl_, true, first_index + j, subtract_mean, st, !mixed,
                                    measure && j + it == k);
+                j += it;
+                src = dst;
+                dst = dst == x ? x_alt_.p : x;
                 ++launches;
             }
         } else {

@@ -148,14 +148,17 @@ bool sor_fuses_measure(int n);
 // Temporally blocked form of the same sweeps (kernels_sor_blocked.cu):
 // `iterations` (1 or 2) red+black iterations in one launch, starting with
 // colour `first_colour`, bit-identical to 2 * iterations one-colour launches
-// with the same flags (for first_colour 1: the plain relaxation only). A
-// guarded launch covers sweep indices sweep_index .. + iterations - 1 and
-// stops at the iteration budget; `measure` records the residual of its last
-// half-sweep (colour 1) when it ran all iterations. Needs sor_blocked_applies(n).
+// with the same flags (for first_colour 1: the plain relaxation only). The
+// update is out of place, xin -> xout (they may coincide only with
+// `from_zero`, which reads no iterate). A guarded launch covers sweep indices
+// sweep_index .. + iterations - 1 and stops at the iteration budget (copying
+// xin to xout when no sweep is left); `measure` records the residual of its
+// last half-sweep (colour 1) when it ran all iterations. Needs
+// sor_blocked_applies(n).
 bool sor_blocked_applies(int n);
-void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colour, float* x, const float* b,
-                        ProjControl* ctrl, bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s,
-                        bool exact, bool measure = false, bool from_zero = false);
+void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colour, const float* xin, float* xout,
+                        const float* b, ProjControl* ctrl, bool guarded, int sweep_index, bool subtract_mean,
+                        cudaStream_t s, bool exact, bool measure = false, bool from_zero = false);
 // Autotuner hook: z chunks per blocked launch for grid size n (<= 0: one
 // wave of CTAs).
 void set_sor_blocked_chunks(int n, int chunks);

@@ -11,15 +11,18 @@
 // x-neighbour slot) come from shared memory, where they were written in the
 // previous step. One barrier per plane therefore orders everything.
 //
-// Shared memory holds a ring of 2K + 2 planes (both colours) of the tile and
-// its halo: one float4 group on each side in x and 2K rows on each side in y
-// (every half-sweep invalidates one more ring of cells at the tile edge). The
-// z-chunk loads 2K extra planes on each side for the same reason. Planes are
-// loaded one step ahead with cp.async (16 bytes per thread and colour; zero
-// fill outside the grid, where missing neighbours read as zero exactly as in
-// the one-colour sweep). Right-hand sides (and the solid-mask diagonal) are
-// read from global memory through the read-only path: each is needed once per
-// half-sweep of its colour.
+// Shared memory holds rings of 2K + 3 planes (both colours) of the iterate
+// and of the right-hand side over the tile and its halo: one float4 group on
+// each side in x and 2K rows on each side in y (every half-sweep invalidates
+// one more ring of cells at the tile edge). The z-chunk loads 2K extra planes
+// on each side for the same reason. Planes are loaded two steps ahead with
+// cp.async (16 bytes per thread, colour and field; zero fill outside the
+// grid, where missing neighbours read as zero exactly as in the one-colour
+// sweep), so no global load sits on a step's critical path.
+//
+// The update is out of place: the launch reads x_in and writes x_out, because
+// neighbouring CTAs read each other's cells as halo while they run. A guarded
+// launch past the iteration budget copies x_in to x_out.
 //
 // DRAM traffic per launch is the tile's halo-inflated read of x and b plus one
 // write of x: at 256^3 with TY = 16 about 2x (4 + 4) + 4 B per cell for K = 2
@@ -43,11 +46,11 @@ struct Blocked {
     static constexpr int S = 2 * K;        // colour half-sweeps per launch
     static constexpr int HY = S;           // halo rows on each side
     static constexpr int R = TY + 2 * HY;  // rows held
-    static constexpr int RING = S + 2;     // planes held
+    static constexpr int RING = S + 3;     // planes held (two loading ahead)
     static constexpr int POS = R * kGX;    // (row, group) positions, one per thread
     static constexpr int THREADS = (POS + 31) / 32 * 32;
     static constexpr int PLANE = R * kGX;  // float4 per plane and colour
-    static constexpr int SMEM = RING * 2 * PLANE * 16;
+    static constexpr int SMEM = 2 * RING * 2 * PLANE * 16;  // iterate and right-hand side
 };
 
 struct RelaxW {
@@ -61,6 +64,7 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ float comp(const float4& v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
@@ -125,7 +129,7 @@ __device__ __forceinline__ float4 relax4(const float4 xo, const float (&xl)[5], 
 
 // FIRST: colour of the first half-sweep (the reference order is 0 then 1;
 // the FPCG post-smoother runs 1 then 0). FROM_ZERO: the sweep starts from
-// x = 0 (x is not read; both colours are written). RESID: the last
+// x = 0 (x_in is not read; both colours are written). RESID: the last
 // half-sweep also records max |b' - off - diag x| over its updated cells into
 // ctrl->res32_bits, as the one-colour sweep's measuring form does.
 // A guarded launch covers sweeps sweep_index .. sweep_index + K - 1 of the
@@ -133,23 +137,14 @@ __device__ __forceinline__ float4 relax4(const float4 xo, const float (&xl)[5], 
 // remaining half-sweeps pass values through unchanged); it measures only when
 // it ran all K.
 template <int K, int TY, int FIRST, bool EXACT, bool RESID, bool FROM_ZERO, bool MASK>
-__global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
-    Grid g, float omega, float floor_diag, RelaxW wr, float* __restrict__ xs, const float* __restrict__ bs,
-    ProjControl* ctrl, int guarded, int sweep_index, int subtract_mean, int zc, const uint8_t* __restrict__ dg) {
+__global__ void __launch_bounds__(Blocked<K, TY>::THREADS, 2) k_sor_blocked(
+    Grid g, float omega, float floor_diag, RelaxW wr, const float* __restrict__ xin, float* __restrict__ xout,
+    const float* __restrict__ bs, ProjControl* ctrl, int guarded, int sweep_index, int subtract_mean, int zc,
+    const uint8_t* __restrict__ dg) {
     using B = Blocked<K, TY>;
     constexpr int S = B::S, RING = B::RING, R = B::R, PL = B::PLANE;
-    extern __shared__ float4 ring[];  // [RING][2][R][kGX]
+    extern __shared__ float4 ring[];  // x: [RING][2][R][kGX], then b: the same
     __shared__ float s_max[32];
-
-    int live = S;  // half-sweeps that update (the rest pass through)
-    if (guarded) {
-        if (ctrl->done) return;
-        const int left = ctrl->max_iterations - ctrl->iterations - sweep_index;
-        if (left <= 0) return;
-        live = 2 * min(K, left);
-    }
-    const bool measure = RESID && live == S;
-    const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
 
     const int n = g.n, hw = n >> 1, hg = hw >> 2;
     const int plane = n * hw, cstride = n * plane;
@@ -161,29 +156,48 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
     const bool in_dom = thread_live && y >= 0 && y < n && gg >= 0 && gg < hg;
     const bool interior = in_dom && r >= B::HY && r < B::HY + TY && gl >= 1 && gl <= kGroups;
     const int z0 = int(blockIdx.z) * zc, z1 = min(n, z0 + zc);
-    const int tau0 = max(0, z0 - (S - 1)), tau_end = z1 + S - 1;
     const int col = y * hw + gg * 4;  // offset of the thread's group in a plane of one colour
+
+    int live = S;  // half-sweeps that update (the rest pass through)
+    if (guarded) {
+        const int left = ctrl->max_iterations - ctrl->iterations - sweep_index;
+        live = ctrl->done ? 0 : 2 * max(0, min(K, left));
+    }
+    if (live == 0) {  // nothing to do: x_out = x_in over the CTA's own cells
+        if (interior)
+            for (int zz = z0; zz < z1; ++zz)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int o = c * cstride + zz * plane + col;
+                    *reinterpret_cast<float4*>(xout + o) = *reinterpret_cast<const float4*>(xin + o);
+                }
+        return;
+    }
+    const bool measure = RESID && live == S;
+    const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
+    const int tau0 = max(0, z0 - (S - 1)), tau_end = z1 + S - 1;
     const int me = r * kGX + gl;
     const int ny_yz = int(y > 0) + int(y + 1 < n);
     const bool left_group = gg == 0, right_group = gg == hg - 1;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4* bring = ring + RING * 2 * PL;
     float rmax = 0.f;
 
     auto slot_of = [&](int p) { return (p - tau0 + 1 + RING) % RING; };
     auto at = [&](int slot, int c) { return ring + (slot * 2 + c) * PL; };
-    // plane p (both colours) of the thread's position into its ring slot
+    auto bat = [&](int slot, int c) { return bring + (slot * 2 + c) * PL; };
+    // plane p (both colours, iterate and right-hand side) of the thread's
+    // position into its ring slot
     auto load_plane = [&](int p) {
         if (!thread_live) return;
         const int slot = slot_of(p);
+        const bool ok = in_dom && p >= 0 && p < n;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            if (FROM_ZERO) {
-                at(slot, c)[me] = zero4;
-            } else {
-                const bool ok = in_dom && p >= 0 && p < n;
-                const float* src = ok ? xs + c * cstride + p * plane + col : xs;
-                cp_async16(at(slot, c) + me, src, ok);
-            }
+            const int o = c * cstride + p * plane + col;
+            if (FROM_ZERO) at(slot, c)[me] = zero4;
+            else cp_async16(at(slot, c) + me, ok ? xin + o : xin, ok);
+            cp_async16(bat(slot, c) + me, ok ? bs + o : bs, ok);
         }
     };
 
@@ -198,7 +212,9 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
     load_plane(tau0);
     load_plane(tau0 + 1);
     cp_async_commit();
-    cp_async_wait_all();
+    load_plane(tau0 + 2);
+    cp_async_commit();
+    cp_async_wait_one();
     __syncthreads();
     if (thread_live) {
 #pragma unroll
@@ -214,7 +230,7 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
 #pragma unroll
             for (int c = 0; c < 2; ++c) V[c][0] = at(s1, c)[me];
         }
-        load_plane(tau + 2);  // into the slot of plane tau - S, read last in the previous step
+        load_plane(tau + 3);  // into the slot of plane tau - S, last read in the previous step
         cp_async_commit();
 #pragma unroll
         for (int t = 1; t <= S; ++t) {
@@ -236,10 +252,9 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
                     xl[0] = xc.x; xl[1] = xc.y; xl[2] = xc.z; xl[3] = xc.w;
                     xl[4] = gl < kGX - 1 ? reinterpret_cast<const float*>(oth + me + 1)[0] : 0.f;
                 }
-                const int goff = C * cstride + zt * plane + col;
-                const float4 b4 = __ldg(reinterpret_cast<const float4*>(bs + goff));
+                const float4 b4 = bat(st, C)[me];
                 uchar4 dm = make_uchar4(0, 0, 0, 0);
-                if (MASK) dm = __ldg(reinterpret_cast<const uchar4*>(dg + goff));
+                if (MASK) dm = __ldg(reinterpret_cast<const uchar4*>(dg + C * cstride + zt * plane + col));
                 const int ny = ny_yz + int(zt > 0) + int(zt + 1 < n);
                 const bool resid = measure && t == S && interior;
                 const float4 res = relax4<EXACT, MASK>(V[C][t], xl, ym, yp, V[OC][t + 1], V[OC][t - 1], b4, bm, ny,
@@ -253,16 +268,17 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS) k_sor_blocked(
         const int zf = tau - S + 1;
         if (interior && zf >= z0 && zf < z1) {
             constexpr int CL = (FIRST + S - 1) & 1;
-            *reinterpret_cast<float4*>(xs + CL * cstride + zf * plane + col) = V[CL][S];
-            *reinterpret_cast<float4*>(xs + (1 - CL) * cstride + zf * plane + col) = V[1 - CL][S];
+            *reinterpret_cast<float4*>(xout + CL * cstride + zf * plane + col) = V[CL][S];
+            *reinterpret_cast<float4*>(xout + (1 - CL) * cstride + zf * plane + col) = V[1 - CL][S];
         }
 #pragma unroll
         for (int c = 0; c < 2; ++c)
 #pragma unroll
             for (int k = S + 1; k > 0; --k) V[c][k] = V[c][k - 1];
-        cp_async_wait_all();
+        cp_async_wait_one();  // plane tau + 2 has landed (tau + 3 may still be in flight)
         __syncthreads();
     }
+    cp_async_wait_all();
     if (RESID) {
         const float br = block_max(rmax, s_max);
         if (threadIdx.x == 0 && measure && br > 0.f) atomicMax(&ctrl->res32_bits, __float_as_uint(br));
@@ -274,8 +290,8 @@ std::map<int, int> g_blocked_chunks;  // grid size -> z chunks per launch (tunin
 std::atomic<int> g_block_iterations{2};
 
 template <int K, int TY, int FIRST, bool EXACT, bool RESID, bool FROM_ZERO, bool MASK>
-void launch_blocked(const ProjectionArgs& a, float* x, const float* b, ProjControl* ctrl, bool guarded,
-                    int sweep_index, bool subtract_mean, cudaStream_t s) {
+void launch_blocked(const ProjectionArgs& a, const float* xin, float* xout, const float* b, ProjControl* ctrl,
+                    bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s) {
     using B = Blocked<K, TY>;
     auto kern = k_sor_blocked<K, TY, FIRST, EXACT, RESID, FROM_ZERO, MASK>;
     static const int resident = [&] {
@@ -304,7 +320,7 @@ void launch_blocked(const ProjectionArgs& a, float* x, const float* b, ProjContr
     RelaxW wr;
     for (int d = 0; d < 7; ++d) wr.w[d] = a.omega / std::max(float(d), a.diagonal_floor);
     count_launch();
-    kern<<<grid, B::THREADS, B::SMEM, s>>>(a.g, a.omega, a.diagonal_floor, wr, x, b, ctrl, guarded ? 1 : 0,
+    kern<<<grid, B::THREADS, B::SMEM, s>>>(a.g, a.omega, a.diagonal_floor, wr, xin, xout, b, ctrl, guarded ? 1 : 0,
                                           sweep_index, subtract_mean ? 1 : 0, zc, a.diag);
 }
 
@@ -328,9 +344,10 @@ void set_sor_blocked_chunks(int n, int chunks) {
     else g_blocked_chunks[n] = chunks;
 }
 
-void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colour, float* x, const float* b,
-                        ProjControl* ctrl, bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s,
-                        bool exact, bool measure, bool from_zero) {
+void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colour, const float* xin, float* xout,
+                        const float* b, ProjControl* ctrl, bool guarded, int sweep_index, bool subtract_mean,
+                        cudaStream_t s, bool exact, bool measure, bool from_zero) {
+    if (xin == xout && !from_zero) fail(VAPOR_RUNTIME_ERROR, "blocked sweep: the update is out of place");
     const bool mask = a.diag != nullptr;
     if (iterations != 1 && iterations != 2) fail(VAPOR_RUNTIME_ERROR, "blocked sweep: 1 or 2 iterations per launch");
     if (first_colour == 1 && (exact || measure || from_zero || mask))
@@ -340,7 +357,7 @@ void launch_sor_blocked(const ProjectionArgs& a, int iterations, int first_colou
     if (exact && measure) fail(VAPOR_RUNTIME_ERROR, "blocked sweep: the exact form does not measure");
     constexpr int TY = 16;
 #define VB_BLK(KK, F, E, R, Z, M) \
-    launch_blocked<KK, TY, F, E, R, Z, M>(a, x, b, ctrl, guarded, sweep_index, subtract_mean, s)
+    launch_blocked<KK, TY, F, E, R, Z, M>(a, xin, xout, b, ctrl, guarded, sweep_index, subtract_mean, s)
 #define VB_BLK_K(F, E, R, Z, M)                    \
     if (iterations == 2) VB_BLK(2, F, E, R, Z, M); \
     else VB_BLK(1, F, E, R, Z, M)
