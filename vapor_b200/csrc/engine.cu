@@ -202,7 +202,8 @@ void Workspace::advect_velocity(float dt, float cfl, bool maccormack, const floa
     }
     float* fwd[3] = {fwd3_.p, fwd3_.p + faces, fwd3_.p + 2 * faces};
     timer_.begin(VAPOR_PHASE_ADVECT);
-    launch_advect_velocity(grid(), dt, cfl, maccormack, src, u, v, w, fwd, out, stream_);
+    launch_advect_velocity(grid(), dt, cfl, maccormack, src, u, v, w, fwd, out, maccormack ? vel_cache_.p : nullptr,
+                           stream_);
     timer_.end(VAPOR_PHASE_ADVECT, maccormack ? 2 : 1);
     VB_CUDA(cudaGetLastError());
 }
@@ -210,6 +211,18 @@ void Workspace::advect_velocity(float dt, float cfl, bool maccormack, const floa
 void Workspace::ensure_velocity_scratch() {
     const size_t faces = size_t(n_) * n_ * (n_ + 1);
     if (fwd3_.n != 3 * faces) fwd3_.allocate(3 * faces);
+    if (vel_cache_.n != 9 * faces) vel_cache_.allocate(9 * faces);
+}
+
+void Workspace::advect_smoke(float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
+                             const float* w, float* out, float post_scale) {
+    // the velocity cache is free once the velocity has been advected; it
+    // holds 9 face arrays, more than the smoke's 3 cell arrays
+    float* cache = (maccormack && vel_cache_.p) ? vel_cache_.p : nullptr;
+    timer_.begin(VAPOR_PHASE_ADVECT);
+    launch_advect_smoke(grid(), dt, cfl, maccormack, src, u, v, w, fwd_.p, out, post_scale, cache, stream_);
+    timer_.end(VAPOR_PHASE_ADVECT, maccormack ? 2 : 1);
+    VB_CUDA(cudaGetLastError());
 }
 
 void Workspace::ensure_mixed() {
@@ -808,8 +821,8 @@ void Simulation::record_step(float dt) {
     // Smoke transport through the projected velocity, then dissipation
     // (MacGridFluidSolver3D.cpp:183-190) fused as a post-scale.
     const float factor = std::clamp(1.0f - p.smoke_decay * dt, 0.0f, 1.0f);
-    ws_.advect(CELL, dt, p.cfl_mc, p.mac_cormack_smoke != 0, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
-               vel_[S_][2].p, dens_[1 - cur_].p, factor);
+    ws_.advect_smoke(dt, p.cfl_mc, p.mac_cormack_smoke != 0, dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p,
+                     vel_[S_][2].p, dens_[1 - cur_].p, factor);
 }
 
 void Simulation::set_warm_start(unet::UNet* net) {
@@ -863,7 +876,7 @@ void Simulation::prepare_step(float dt) {
             noise_.allocate(need);
         }
         if (params.solver_kind != VAPOR_SOLVER_RED_BLACK_SOR) ws_.ensure_mixed();
-        if (params.mac_cormack_vel) ws_.ensure_velocity_scratch();
+        if (params.mac_cormack_vel || params.mac_cormack_smoke) ws_.ensure_velocity_scratch();
         if (warm_) {
             warm_->set_stream(ws_.stream());
             warm_->prepare(ws_.n());

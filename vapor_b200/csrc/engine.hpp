@@ -125,6 +125,10 @@ public:
     // (their forward passes kept in a 3-face-array scratch).
     void advect_velocity(float dt, float cfl, bool maccormack, const float* const src[3], const float* u,
                          const float* v, const float* w, float* const out[3]);
+    // The smoke through the flow, its forward pass's traced velocities cached
+    // for the MacCormack pass when the velocity scratch exists.
+    void advect_smoke(float dt, float cfl, bool maccormack, const float* src, const float* u, const float* v,
+                      const float* w, float* out, float post_scale);
     // Waits for the stream and returns the last projection result; raises
     // VAPOR_NON_FINITE if a non-finite divergence or residual was seen since
     // the last clear_errors().
@@ -158,6 +162,7 @@ private:
     cudaStream_t stream_;
     DevArray<float> b_, p_, fwd_;
     DevArray<float> fwd3_;  // forward passes of the three velocity components (allocated before capture)
+    DevArray<float> vel_cache_;  // traced velocities of the forward passes (9 face arrays)
     DevArray<double> partials_;
     DevArray<double> x64_[2];           // mixed-precision pressure (ping-pong)
     DevArray<float> r32_;               // mixed-precision inner right-hand side (FPCG: the residual)

@@ -97,10 +97,16 @@ void launch_advect(const Grid& g, int loc, float dt, float cfl_limit, bool macco
                    cudaStream_t s);
 // The three velocity components src[c] (faces of axis c) through the flow
 // (u, v, w) into out[c], in one forward launch (into fwd[c]) and one
-// MacCormack launch; same results as three launch_advect calls.
+// MacCormack launch; same results as three launch_advect calls. With
+// `vel_cache` (9 face arrays) the forward pass stores each point's traced
+// velocity and the MacCormack pass reads it back instead of sampling again.
 void launch_advect_velocity(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* const src[3],
                             const float* u, const float* v, const float* w, float* const fwd[3],
-                            float* const out[3], cudaStream_t s);
+                            float* const out[3], float* vel_cache, cudaStream_t s);
+// The smoke (cell centres) the same way, with `vel_cache` of 3 cell arrays.
+void launch_advect_smoke(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* src,
+                         const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
+                         float* vel_cache, cudaStream_t s);
 
 // ---- projection ----
 struct ProjectionArgs {

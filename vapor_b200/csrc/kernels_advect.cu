@@ -25,6 +25,10 @@ struct FieldSet {
     const float* src[3];
     float* fwd[3];
     float* out[3];
+    // Traced velocity of every sample point, written by the forward pass and
+    // read back by the MacCormack pass instead of sampling the flow again
+    // (null: the MacCormack pass samples it itself). [field][component].
+    float* vel[3][3];
 };
 
 // Sample point of location LOC: staggered axis at i*h, the others at (i+.5)h
@@ -48,10 +52,17 @@ template <int LOC, bool POW2>
 __device__ __forceinline__ void forward_point(const Grid& g, float ih, float dt, int x, int y, int z,
                                               const float* __restrict__ src, const float* __restrict__ u,
                                               const float* __restrict__ v, const float* __restrict__ w,
-                                              float* __restrict__ out, float post_scale) {
+                                              float* __restrict__ out, float post_scale,
+                                              float* const* vel_out = nullptr) {
     float px, py, pz;
     position<LOC>(x, y, z, g.h, px, py, pz);
     const Vel vel = velocity_at<POW2>(u, v, w, g.n, g.h, px, py, pz, ih);
+    if (vel_out) {
+        const size_t i = index_of(g.n, LOC, x, y, z);
+        vel_out[0][i] = vel.x;
+        vel_out[1][i] = vel.y;
+        vel_out[2][i] = vel.z;
+    }
     const float qx = px - vel.x * dt, qy = py - vel.y * dt, qz = pz - vel.z * dt;
     const float value = sample<LOC, POW2>(src, g.n, g.h, qx, qy, qz, ih);
     out[index_of(g.n, LOC, x, y, z)] = value * post_scale;
@@ -62,13 +73,21 @@ __device__ __forceinline__ void maccormack_point(const Grid& g, float ih, float 
                                                  int z, const float* __restrict__ src,
                                                  const float* __restrict__ fwd, const float* __restrict__ u,
                                                  const float* __restrict__ v, const float* __restrict__ w,
-                                                 float* __restrict__ out, float post_scale) {
+                                                 float* __restrict__ out, float post_scale,
+                                                 float* const* vel_in = nullptr) {
     const int n = g.n;
     const float h = g.h, box = g.box;
     const size_t i = index_of(n, LOC, x, y, z);
     float px, py, pz;
     position<LOC>(x, y, z, h, px, py, pz);
-    const Vel vel = velocity_at<POW2>(u, v, w, n, h, px, py, pz, ih);
+    Vel vel;
+    if (vel_in) {  // the forward pass's values for this point (the same bits)
+        vel.x = __ldg(vel_in[0] + i);
+        vel.y = __ldg(vel_in[1] + i);
+        vel.z = __ldg(vel_in[2] + i);
+    } else {
+        vel = velocity_at<POW2>(u, v, w, n, h, px, py, pz, ih);
+    }
     const float fx = px - vel.x * dt, fy = py - vel.y * dt, fz = pz - vel.z * dt;
     const float bx = px + vel.x * dt, by = py + vel.y * dt, bz = pz + vel.z * dt;
     const float cfl = div_h<POW2>(sqrtf(vel.x * vel.x + vel.y * vel.y + vel.z * vel.z) * dt, h, ih);
@@ -122,18 +141,19 @@ __global__ void __launch_bounds__(kThreads) k_advect_set(Grid g, float dt, float
     const int y = xy / ex, x = xy - y * ex;
     const float* src = f.src[field];
     float* out = MC ? f.out[field] : f.fwd[field];
+    float* const* vc = f.vel[field][0] ? f.vel[field] : nullptr;
     if (!FACES) {
-        if (MC) maccormack_point<CELL, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, post_scale);
-        else forward_point<CELL, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, post_scale);
+        if (MC) maccormack_point<CELL, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, post_scale, vc);
+        else forward_point<CELL, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, post_scale, vc);
     } else if (field == 0) {
-        if (MC) maccormack_point<FACE_X, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, 1.f);
-        else forward_point<FACE_X, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+        if (MC) maccormack_point<FACE_X, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[0], u, v, w, out, 1.f, vc);
+        else forward_point<FACE_X, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f, vc);
     } else if (field == 1) {
-        if (MC) maccormack_point<FACE_Y, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[1], u, v, w, out, 1.f);
-        else forward_point<FACE_Y, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+        if (MC) maccormack_point<FACE_Y, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[1], u, v, w, out, 1.f, vc);
+        else forward_point<FACE_Y, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f, vc);
     } else {
-        if (MC) maccormack_point<FACE_Z, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[2], u, v, w, out, 1.f);
-        else forward_point<FACE_Z, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f);
+        if (MC) maccormack_point<FACE_Z, POW2>(g, ih, dt, cfl_limit, x, y, z, src, f.fwd[2], u, v, w, out, 1.f, vc);
+        else forward_point<FACE_Z, POW2>(g, ih, dt, x, y, z, src, u, v, w, out, 1.f, vc);
     }
 }
 
@@ -214,16 +234,31 @@ void launch_advect(const Grid& g, int loc, float dt, float cfl_limit, bool macco
 
 void launch_advect_velocity(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* const src[3],
                             const float* u, const float* v, const float* w, float* const fwd[3],
-                            float* const out[3], cudaStream_t s) {
-    FieldSet f;
+                            float* const out[3], float* vel_cache, cudaStream_t s) {
+    FieldSet f{};
+    const size_t faces = size_t(g.n) * g.n * (g.n + 1);
     for (int c = 0; c < 3; ++c) {
         f.src[c] = src[c];
         // without MacCormack the forward pass is the result
         f.fwd[c] = maccormack ? fwd[c] : out[c];
         f.out[c] = out[c];
+        for (int k = 0; k < 3; ++k) f.vel[c][k] = (maccormack && vel_cache) ? vel_cache + (3 * c + k) * faces : nullptr;
     }
     if (power_of_two(g.h)) advect_set<true, true>(g, dt, cfl_limit, maccormack, f, u, v, w, 1.f, s);
     else advect_set<true, false>(g, dt, cfl_limit, maccormack, f, u, v, w, 1.f, s);
+}
+
+void launch_advect_smoke(const Grid& g, float dt, float cfl_limit, bool maccormack, const float* src,
+                         const float* u, const float* v, const float* w, float* fwd, float* out, float post_scale,
+                         float* vel_cache, cudaStream_t s) {
+    FieldSet f{};
+    const size_t cells = size_t(g.n) * g.n * g.n;
+    f.src[0] = src;
+    f.fwd[0] = maccormack ? fwd : out;
+    f.out[0] = out;
+    for (int k = 0; k < 3; ++k) f.vel[0][k] = (maccormack && vel_cache) ? vel_cache + k * cells : nullptr;
+    if (power_of_two(g.h)) advect_set<false, true>(g, dt, cfl_limit, maccormack, f, u, v, w, post_scale, s);
+    else advect_set<false, false>(g, dt, cfl_limit, maccormack, f, u, v, w, post_scale, s);
 }
 
 }  // namespace vb
