@@ -132,8 +132,9 @@ def test_forward_matches_torch_reference(n):
 def test_warp_specialised_convolutions_equal_block_synchronous(n):
     """The warp-specialised convolution kernel (producer / MMA / epilogue
     warps on mbarriers) against the block-synchronous z-marching kernel: the
-    same MMAs on the same operands, so the network's outputs and parameter
-    gradients are bit-identical."""
+    same MMAs on the same operands, so the network's outputs are
+    bit-identical; the parameter gradients agree to FP32 rounding (the weight
+    gradients accumulate with atomics in no fixed order)."""
     import torch
     net = Net(seed=13)
     x = features(n, 21)
@@ -152,7 +153,7 @@ def test_warp_specialised_convolutions_equal_block_synchronous(n):
     finally:
         vb.tune_conv_kernel(1)
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
-    assert np.array_equal(grads[0].view(np.uint32), grads[1].view(np.uint32))
+    assert np.abs(grads[0] - grads[1]).max() <= 1e-5 * np.abs(grads[0]).max()
 
 
 @pytest.mark.parametrize("ws", [0, 1])

@@ -296,6 +296,10 @@ void launch_blocked(const ProjectionArgs& a, const float* xin, float* xout, cons
     auto kern = k_sor_blocked<K, TY, FIRST, EXACT, RESID, FROM_ZERO, MASK>;
     static const int resident = [&] {
         VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, B::SMEM));
+        // all of the unified L1 / shared storage as shared memory, so that
+        // two CTAs fit on an SM
+        VB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     int(cudaSharedmemCarveoutMaxShared)));
         int blocks = 0;
         VB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, B::THREADS, B::SMEM));
         int dev = 0, sms = 0;
