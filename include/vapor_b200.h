@@ -237,6 +237,30 @@ vapor_status vapor_mac3d_last_projection(vapor_mac3d *sim, vapor_projection_resu
 vapor_status vapor_mac3d_total_iterations(vapor_mac3d *sim, int64_t *out);
 /* diagnostics(): kinetic energy, max |velocity|, max |divergence| (waits). */
 vapor_status vapor_mac3d_diagnostics(vapor_mac3d *sim, vapor_fluid_diagnostics *out);
+
+/* Comparison metrics of the current state (extension): the quantities the
+ * reference's diagnostic harness prints for its Reflection / MacCormack
+ * comparison (tests/ReflectionComparison.hpp:32-75), computed on the device.
+ * frames_per_second sets the frame time 1 / fps of the CFL and trace tests
+ * (the harness uses 60). Sums are FP64 (a fixed tree; the harness sums
+ * sequentially, so they agree to FP64 rounding); counts and maxima are exact.
+ * VAPOR_NON_FINITE when a divergence is not finite. */
+typedef struct vapor_comparison_metrics {
+    double mass_sum;          /* sum of density */
+    double mass;              /* mass_sum / n^3 */
+    double grad_per_mass;     /* sum of |d - d(+x)|, |d - d(+y)|, |d - d(+z)| over mass_sum */
+    double square_per_mass;   /* sum of d^2 over mass_sum */
+    double rms_div;           /* sqrt(mean divergence^2) */
+    double max_div;           /* max |divergence| */
+    long long smoke_cells;    /* cells with density > 0.001 */
+    long long cfl_fallback;   /* smoke cells with |v| / (h fps) > cfl_mc */
+    long long boundary_fallback; /* smoke cells whose trace -v/fps or +v/fps leaves the box */
+    double max_cfl;           /* max |v| / (h fps) over smoke cells */
+    int32_t nonfinite;
+    int32_t reserved;
+} vapor_comparison_metrics;
+vapor_status vapor_mac3d_comparison_metrics(vapor_mac3d *sim, float frames_per_second,
+                                            vapor_comparison_metrics *out);
 /* upload/download (GpuMacSimulation3D.cpp:110-141): host snapshot <-> device.
  * Array sizes are implied by n (see layout above). */
 vapor_status vapor_mac3d_upload(vapor_mac3d *sim, const float *density, const float *u,

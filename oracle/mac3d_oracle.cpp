@@ -898,6 +898,53 @@ VO_EXPORT vapor_status vapor_mac3d_default_params(vapor_mac3d_params* o) {
 VO_DEFINE(float, f32)
 VO_DEFINE(double, f64)
 
+// The comparison metrics of the reference's diagnostic harness
+// (tests/ReflectionComparison.hpp:32-75) on an FP32 state of box `box`
+// (positions (x + .5) / n scaled by the box, frame time 1 / fps), with the
+// harness's sequential FP64 sums. out: mass_sum, grad_sum, square_sum,
+// div_square_sum, max_div, smoke_cells, cfl_fallback, boundary_fallback,
+// max_cfl.
+VO_EXPORT void vo_comparison_metrics(int n, float box, float fps, float cflMc, const float* d, const float* u,
+                                     const float* v, const float* w, double* out) {
+    const Grid<float> g(n, box);
+    double mass = 0, grad = 0, square = 0, divSquare = 0, maxCfl = 0;
+    float maxDiv = 0.f;
+    long long smokeCells = 0, cflFallback = 0, boundaryFallback = 0;
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const float div = divergenceAt(g, u, v, w, x, y, z);
+                divSquare += double(div) * div;
+                maxDiv = maxT(maxDiv, std::fabs(div));
+            }
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const float dv = d[g.index(CELL, x, y, z)];
+                mass += dv;
+                square += double(dv) * dv;
+                if (x + 1 < n) grad += std::fabs(dv - d[g.index(CELL, x + 1, y, z)]);
+                if (y + 1 < n) grad += std::fabs(dv - d[g.index(CELL, x, y + 1, z)]);
+                if (z + 1 < n) grad += std::fabs(dv - d[g.index(CELL, x, y, z + 1)]);
+                if (dv <= .001f) continue;
+                ++smokeCells;
+                const V3<float> pos{(x + .5f) / n * box, (y + .5f) / n * box, (z + .5f) / n * box};
+                const V3<float> vel = velocityAt(g, u, v, w, pos);
+                const double cfl = std::sqrt(vel.x * vel.x + vel.y * vel.y + vel.z * vel.z) * n / (box * fps);
+                maxCfl = std::max(maxCfl, cfl);
+                if (cfl > cflMc) ++cflFallback;
+                const float step = 1.f / fps;
+                const V3<float> a{pos.x - vel.x * step, pos.y - vel.y * step, pos.z - vel.z * step};
+                const V3<float> b{pos.x + vel.x * step, pos.y + vel.y * step, pos.z + vel.z * step};
+                if (a.x < 0 || a.x > box || a.y < 0 || a.y > box || a.z < 0 || a.z > box || b.x < 0 ||
+                    b.x > box || b.y < 0 || b.y > box || b.z < 0 || b.z > box)
+                    ++boundaryFallback;
+            }
+    const double r[9] = {mass, grad, square, divSquare, double(maxDiv), double(smokeCells), double(cflFallback),
+                         double(boundaryFallback), maxCfl};
+    std::copy(r, r + 9, out);
+}
+
 // MacGridParameters3D(MacAlgorithm) presets (MacGridFluidSolver3D.cpp:11-26).
 VO_EXPORT vapor_status vapor_mac3d_algorithm_params(int32_t algorithm, vapor_mac3d_params* o) {
     if (algorithm < 0 || algorithm > 3) return VAPOR_INVALID_ARGUMENT;

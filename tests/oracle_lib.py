@@ -58,6 +58,9 @@ def _setup_oracle(lib):
         f("vo_sim_total_iterations", C.c_longlong, _vp)
     lib.vapor_mac3d_default_params.argtypes = [C.POINTER(MacParams)]
     lib.vapor_mac3d_algorithm_params.argtypes = [C.c_int32, C.POINTER(MacParams)]
+    lib.vo_comparison_metrics.restype = None
+    lib.vo_comparison_metrics.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, _f32p, _f32p, _f32p, _f32p,
+                                          _f64p]
     return lib
 
 
@@ -315,3 +318,17 @@ def random_fields(n, seed, scale=1.0, density=True):
     sd, su, sv, sw = field_shapes(n)
     d = rng.random(sd, dtype=np.float32) if density else np.zeros(sd, np.float32)
     return [d] + [(rng.standard_normal(s) * scale).astype(np.float32) for s in (su, sv, sw)]
+
+
+def comparison_metrics(n, box, d, u, v, w, fps=60.0, cfl_mc=3.0):
+    """The reference harness's comparison metrics on the CPU (the oracle's
+    restatement of tests/ReflectionComparison.hpp:32-75), as the device
+    entry point reports them."""
+    out = np.zeros(9, np.float64)
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (d, u, v, w)]
+    oracle().vo_comparison_metrics(n, box, fps, cfl_mc, *arrs, out)
+    mass_sum, grad, square, divsq, max_div, smoke, cfl_fb, bnd_fb, max_cfl = out
+    return {"mass_sum": mass_sum, "mass": mass_sum / n ** 3, "grad_per_mass": grad / mass_sum,
+            "square_per_mass": square / mass_sum, "rms_div": float(np.sqrt(divsq / n ** 3)), "max_div": max_div,
+            "smoke_cells": int(smoke), "cfl_fallback": int(cfl_fb), "boundary_fallback": int(bnd_fb),
+            "max_cfl": max_cfl}

@@ -444,3 +444,29 @@ def test_plume_step_error_against_fp64_oracle():
         for x, y in zip(a.fields(), b.fields()):
             err = np.abs(x.astype(np.float64) - y).max() / max(1e-30, float(np.abs(y).max()))
             assert err <= 1e-5, err
+
+
+def test_comparison_metrics_known_answers():
+    """The harness metrics (tests/ReflectionComparison.hpp:32-75) on states
+    whose values are known: one smoke cell at rest (grad counts its six
+    faces, no fallbacks), then a uniform x-velocity of 6 cells per frame
+    (CFL 6 > 3) whose traces leave the box from cells near the walls."""
+    from oracle_lib import comparison_metrics
+    n = 8
+    d = np.zeros((n, n, n), np.float32)
+    u = np.zeros((n, n, n + 1), np.float32)
+    v = np.zeros((n, n + 1, n), np.float32)
+    w = np.zeros((n + 1, n, n), np.float32)
+    d[3, 3, 3] = 1.0
+    m = comparison_metrics(n, 1.0, d, u, v, w)
+    assert m["mass_sum"] == 1.0 and m["grad_per_mass"] == 6.0 and m["square_per_mass"] == 1.0
+    assert m["smoke_cells"] == 1 and m["cfl_fallback"] == 0 and m["boundary_fallback"] == 0
+    assert m["max_cfl"] == 0.0 and m["rms_div"] == 0.0 and m["max_div"] == 0.0
+    d[...] = 0.5
+    u[...] = 6.0 * 60.0 / n  # 6 cells per frame at 60 frames per second
+    m = comparison_metrics(n, 1.0, d, u, v, w)
+    assert m["smoke_cells"] == n ** 3 and m["cfl_fallback"] == n ** 3
+    assert abs(m["max_cfl"] - 6.0) < 1e-6
+    # traces of +-6 cells stay inside only for no cell of an 8-wide box
+    assert m["boundary_fallback"] == n ** 3
+    assert m["grad_per_mass"] == 0.0 and m["max_div"] == 0.0

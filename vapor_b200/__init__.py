@@ -85,6 +85,7 @@ def _declare(lib):
     f("vapor_mac3d_last_projection", _vp, C.POINTER(ProjectionResult))
     f("vapor_mac3d_total_iterations", _vp, C.POINTER(C.c_int64))
     f("vapor_mac3d_diagnostics", _vp, C.POINTER(FluidDiagnostics))
+    f("vapor_mac3d_comparison_metrics", _vp, C.c_float, C.POINTER(abi.ComparisonMetrics))
     f("vapor_mac3d_upload", _vp, _vp, _vp, _vp, _vp)
     f("vapor_mac3d_download", _vp, _vp, _vp, _vp, _vp)
     f("vapor_mac3d_byte_counters", _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
@@ -276,6 +277,14 @@ class MacSimulation3D:
         d = FluidDiagnostics()
         check(library().vapor_mac3d_diagnostics(self._h, C.byref(d)))
         return d
+
+    def comparison_metrics(self, frames_per_second=60.0):
+        """The reference harness's comparison metrics of the current state
+        (mass, gradient and square per mass, rms and max divergence, smoke
+        cells and their CFL / boundary fallbacks, max CFL), on the device."""
+        m = abi.ComparisonMetrics()
+        check(library().vapor_mac3d_comparison_metrics(self._h, float(frames_per_second), C.byref(m)))
+        return m.as_dict()
 
     def upload(self, density, u, v, w):
         sizes = field_sizes(self.n)

@@ -83,6 +83,18 @@ class FluidDiagnostics(C.Structure):
     _fields_ = [("kinetic_energy", C.c_float), ("max_velocity", C.c_float), ("max_divergence", C.c_float)]
 
 
+class ComparisonMetrics(C.Structure):
+    """vapor_comparison_metrics: the reference harness's comparison metrics."""
+    _fields_ = [("mass_sum", C.c_double), ("mass", C.c_double), ("grad_per_mass", C.c_double),
+                ("square_per_mass", C.c_double), ("rms_div", C.c_double), ("max_div", C.c_double),
+                ("smoke_cells", C.c_longlong), ("cfl_fallback", C.c_longlong),
+                ("boundary_fallback", C.c_longlong), ("max_cfl", C.c_double), ("nonfinite", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name not in ("nonfinite", "reserved")}
+
+
 class MacParams(C.Structure):
     _fields_ = [
         ("emitter_radius", C.c_float),

@@ -195,6 +195,12 @@ VB_API vapor_status vapor_mac3d_total_iterations(vapor_mac3d* sim, int64_t* out)
 VB_API vapor_status vapor_mac3d_diagnostics(vapor_mac3d* sim, vapor_fluid_diagnostics* out) {
     SIM_GUARD(require(out != nullptr, "null output"); sim->sim.diagnostics(out));
 }
+VB_API vapor_status vapor_mac3d_comparison_metrics(vapor_mac3d* sim, float frames_per_second,
+                                                   vapor_comparison_metrics* out) {
+    SIM_GUARD(require(out != nullptr, "null output");
+              require(std::isfinite(frames_per_second) && frames_per_second > 0.f, "Invalid frame rate");
+              sim->sim.comparison_metrics(frames_per_second, out));
+}
 VB_API vapor_status vapor_mac3d_upload(vapor_mac3d* sim, const float* d, const float* u, const float* v,
                                        const float* w) {
     SIM_GUARD(require(d && u && v && w, "null field"); sim->sim.upload(d, u, v, w));

@@ -1083,6 +1083,11 @@ void Simulation::diagnostics(vapor_fluid_diagnostics* out) {
     ws_.diagnostics(vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, out);
 }
 
+void Simulation::comparison_metrics(float frames_per_second, vapor_comparison_metrics* out) {
+    vb::comparison_metrics(ws_.grid(), frames_per_second, params.cfl_mc, dens_[cur_].p, vel_[S_][0].p,
+                           vel_[S_][1].p, vel_[S_][2].p, out, ws_.stream());
+}
+
 // ---------------------------------------------------------------------------
 // Staged stages
 // ---------------------------------------------------------------------------

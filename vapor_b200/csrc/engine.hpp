@@ -223,6 +223,8 @@ public:
     void synchronize();
     vapor_projection_result last_projection();
     void diagnostics(vapor_fluid_diagnostics* out);
+    // The harness comparison metrics of the current state (waits).
+    void comparison_metrics(float frames_per_second, vapor_comparison_metrics* out);
     long long total_iterations() { return ws_.total_iterations(); }
     PhaseTimer& timer() { return ws_.timer(); }
 

@@ -264,6 +264,10 @@ void launch_coarse_correction(int n, float* z, const float* zc, const float* rc,
                               cudaStream_t s);
 
 // ---- diagnostics ----
+// Comparison metrics of (d, u, v, w) (kernels_metrics.cu); waits for the
+// stream; VAPOR_NON_FINITE on a non-finite divergence.
+void comparison_metrics(const Grid& g, float fps, float cfl_limit, const float* d, const float* u, const float* v,
+                        const float* w, vapor_comparison_metrics* out, cudaStream_t s);
 void launch_diagnostics(const Grid& g, const float* u, const float* v, const float* w, double* partials,
                         int partial_capacity, DiagControl* diag, cudaStream_t s);
 
