@@ -261,6 +261,32 @@ typedef struct vapor_comparison_metrics {
 } vapor_comparison_metrics;
 vapor_status vapor_mac3d_comparison_metrics(vapor_mac3d *sim, float frames_per_second,
                                             vapor_comparison_metrics *out);
+
+/* Headless volume ray-march of the smoke density (extension): the reference's
+ * volume shader (src/renderer/shaders/volume.frag:13-55) seen from its orbit
+ * camera (src/renderer/OrbitCamera.cpp:5-28), one CUDA thread per pixel and
+ * no graphics API. The image is width x height RGB floats in [0, 1], pixel
+ * (i, j) at rgb[3 (j width + i)] with row j = 0 at the bottom (OpenGL's
+ * order); pixels without smoke hold the clear colour (.03, .04, .07). The
+ * harness's image: azimuth -1.2, elevation .3, distance 2.5, step_scale .5,
+ * alpha_mul 30, light (.3, .4, 1) / sqrt(1.25), shadow_strength .3,
+ * shadow_step .1. */
+typedef struct vapor_render_params {
+    int32_t width, height;
+    float azimuth, elevation, distance;  /* orbit camera around the box centre */
+    float step_scale;                    /* ray step = step_scale / n (world units for box 1) */
+    float alpha_mul;                     /* opacity per unit density and length */
+    float light[3];                      /* unit direction towards the light */
+    float shadow_strength;               /* 0: no shadow march */
+    float shadow_step;
+} vapor_render_params;
+/* density_device: n^3 FP32 on the current device; rgb_device: 3 * width *
+ * height floats on the device. Allocates nothing. */
+vapor_status vapor_render_volume(const float *density_device, int32_t n, float box,
+                                 const vapor_render_params *params, float *rgb_device, void *stream);
+/* The simulation's current density into host memory (3 * width * height
+ * floats); waits. */
+vapor_status vapor_mac3d_render(vapor_mac3d *sim, const vapor_render_params *params, float *rgb_host);
 /* upload/download (GpuMacSimulation3D.cpp:110-141): host snapshot <-> device.
  * Array sizes are implied by n (see layout above). */
 vapor_status vapor_mac3d_upload(vapor_mac3d *sim, const float *density, const float *u,

@@ -960,3 +960,99 @@ VO_EXPORT vapor_status vapor_mac3d_algorithm_params(int32_t algorithm, vapor_mac
     o->sor_omega = 1.9f;
     return VAPOR_OK;
 }
+
+
+// Headless restatement of the reference's volume shader
+// (src/renderer/shaders/volume.frag:13-55) with its orbit camera
+// (src/renderer/OrbitCamera.cpp:5-28): for each pixel centre, the ray from the
+// camera, the box slab test, front-to-back compositing of the FP32 trilinear
+// (linear filter, clamp to edge) density, and the shadow march towards the
+// light. rgb is width x height x 3, row 0 at the bottom; pixels without smoke
+// keep the clear colour.
+VO_EXPORT void vo_render_volume(int n, float box, const float* d, const vapor_render_params* p, float* rgb) {
+    const float cax = cosf(p->azimuth), sax = sinf(p->azimuth), cel = cosf(p->elevation), sel = sinf(p->elevation);
+    const float half = box * 0.5f;
+    const float ro[3] = {half + p->distance * cel * cax, half + p->distance * cel * sax, half + p->distance * sel};
+    const float up[3] = {-sel * cax, -sel * sax, cel};
+    float fw[3] = {half - ro[0], half - ro[1], half - ro[2]};
+    const float fl = sqrtf(fw[0] * fw[0] + fw[1] * fw[1] + fw[2] * fw[2]);
+    for (float& c : fw) c /= fl;
+    const float rt[3] = {fw[1] * up[2] - fw[2] * up[1], fw[2] * up[0] - fw[0] * up[2], fw[0] * up[1] - fw[1] * up[0]};
+    const float f = 1.0f / tanf(0.8f * 0.5f);
+    const float inv_p0 = 1.f / (f / (float(p->width) / float(p->height))), inv_p5 = 1.f / f;
+    const float nf = float(n);
+    auto tex = [&](float sx, float sy, float sz) {
+        auto axis = [&](float s, int& i0, int& i1, float& t) {
+            const float g = clampT(s * nf - 0.5f, 0.f, nf - 1.f);
+            i0 = int(g);
+            i1 = std::min(i0 + 1, n - 1);
+            t = g - float(i0);
+        };
+        int x0, x1, y0, y1, z0, z1;
+        float tx, ty, tz;
+        axis(sx, x0, x1, tx);
+        axis(sy, y0, y1, ty);
+        axis(sz, z0, z1, tz);
+        auto at = [&](int x, int y, int z) { return d[(size_t(z) * n + y) * n + x]; };
+        const float ux = 1.f - tx, uy = 1.f - ty, uz = 1.f - tz;
+        float s = at(x0, y0, z0) * ux * uy * uz;
+        s = s + at(x1, y0, z0) * tx * uy * uz;
+        s = s + at(x0, y1, z0) * ux * ty * uz;
+        s = s + at(x1, y1, z0) * tx * ty * uz;
+        s = s + at(x0, y0, z1) * ux * uy * tz;
+        s = s + at(x1, y0, z1) * tx * uy * tz;
+        s = s + at(x0, y1, z1) * ux * ty * tz;
+        s = s + at(x1, y1, z1) * tx * ty * tz;
+        return s;
+    };
+    const float bg[3] = {0.03f, 0.04f, 0.07f}, smoke[3] = {0.9f, 0.85f, 0.75f};
+    for (int j = 0; j < p->height; ++j)
+        for (int i = 0; i < p->width; ++i) {
+            float* out = rgb + 3 * (size_t(j) * p->width + i);
+            for (int k = 0; k < 3; ++k) out[k] = bg[k];
+            const float xn = (float(i) + 0.5f) / float(p->width) * 2.f - 1.f;
+            const float yn = (float(j) + 0.5f) / float(p->height) * 2.f - 1.f;
+            const float vx = xn * inv_p0, vy = yn * inv_p5;
+            float rd[3];
+            for (int k = 0; k < 3; ++k) rd[k] = rt[k] * vx + up[k] * vy + fw[k];
+            const float len = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+            for (float& c : rd) c = c / len;
+            float tnear = -std::numeric_limits<float>::infinity(), tfar = std::numeric_limits<float>::infinity();
+            for (int k = 0; k < 3; ++k) {
+                const float t0 = (0.f - ro[k]) / rd[k], t1 = (box - ro[k]) / rd[k];
+                tnear = std::fmax(tnear, std::fmin(t0, t1));
+                tfar = std::fmin(tfar, std::fmax(t0, t1));
+            }
+            if (tnear < 0.f) tnear = 0.f;
+            if (!(tnear < tfar)) continue;
+            const float step = p->step_scale / nf;
+            float col[4] = {0.f, 0.f, 0.f, 0.f};
+            bool hit = false;
+            for (float t = tnear; t < tfar; t += step) {
+                const float px = ro[0] + rd[0] * t, py = ro[1] + rd[1] * t, pz = ro[2] + rd[2] * t;
+                const float dv = tex(px / box, py / box, pz / box);
+                if (dv > 0.001f) {
+                    hit = true;
+                    float shadow = 1.f;
+                    if (p->shadow_strength > 0.f) {
+                        float sa = 0.f;
+                        for (float st = p->shadow_step; st < box * 2.f; st += p->shadow_step) {
+                            const float sx = px + p->light[0] * st, sy = py + p->light[1] * st,
+                                        sz = pz + p->light[2] * st;
+                            if (sx < 0.f || sx > box || sy < 0.f || sy > box || sz < 0.f || sz > box) break;
+                            sa += tex(sx / box, sy / box, sz / box) * p->shadow_step * p->alpha_mul *
+                                  p->shadow_strength;
+                            if (sa > 3.f) break;
+                        }
+                        shadow = std::exp(-sa);
+                    }
+                    const float alpha = clampT(dv * step * p->alpha_mul, 0.f, 1.f);
+                    for (int k = 0; k < 3; ++k) col[k] += (1.f - col[3]) * smoke[k] * alpha * shadow;
+                    col[3] += (1.f - col[3]) * alpha;
+                }
+                if (col[3] > 0.99f) break;
+            }
+            if (!hit) continue;
+            for (int k = 0; k < 3; ++k) out[k] = bg[k] * (1.f - col[3]) + col[k];
+        }
+}

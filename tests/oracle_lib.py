@@ -58,6 +58,8 @@ def _setup_oracle(lib):
         f("vo_sim_total_iterations", C.c_longlong, _vp)
     lib.vapor_mac3d_default_params.argtypes = [C.POINTER(MacParams)]
     lib.vapor_mac3d_algorithm_params.argtypes = [C.c_int32, C.POINTER(MacParams)]
+    lib.vo_render_volume.restype = None
+    lib.vo_render_volume.argtypes = [C.c_int, C.c_float, _f32p, C.c_void_p, _f32p]
     lib.vo_comparison_metrics.restype = None
     lib.vo_comparison_metrics.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, _f32p, _f32p, _f32p, _f32p,
                                           _f64p]
@@ -332,3 +334,10 @@ def comparison_metrics(n, box, d, u, v, w, fps=60.0, cfl_mc=3.0):
             "square_per_mass": square / mass_sum, "rms_div": float(np.sqrt(divsq / n ** 3)), "max_div": max_div,
             "smoke_cells": int(smoke), "cfl_fallback": int(cfl_fb), "boundary_fallback": int(bnd_fb),
             "max_cfl": max_cfl}
+
+
+def render_volume(n, box, density, params):
+    """The oracle's restatement of the volume shader: (height, width, 3)."""
+    rgb = np.zeros((params.height, params.width, 3), np.float32)
+    oracle().vo_render_volume(n, box, np.ascontiguousarray(density, np.float32), C.addressof(params), rgb)
+    return rgb

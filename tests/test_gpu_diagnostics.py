@@ -46,3 +46,27 @@ def test_density_dump_is_the_raw_fp32_field(tmp_path):
     assert os.path.getsize(path) == n ** 3 * 4
     assert np.array_equal(read_density(path, n).view(np.uint32), d.view(np.uint32))
     sim.close()
+
+
+def test_device_render_matches_the_shader_restatement():
+    """The CUDA ray-march of a plume's density against the oracle's FP32
+    restatement of the volume shader on the same density and camera: the
+    same operations except the exponential of the shadow (CUDA's expf against
+    the C library's), so channels agree to 1e-4 except where a compositing
+    cut-off (alpha > .99, shadow > 3) flips, which the bound on the fraction
+    of differing pixels covers."""
+    from oracle_lib import render_volume
+    from vapor_b200.abi import RenderParams
+    n = 32
+    sim = MacSimulation3D(n, 1.0, harness_params(3, 40))
+    for _ in range(40):
+        sim.advance(1.0 / 60.0)
+    params = RenderParams.harness(160, 120)
+    got = sim.render(params)
+    want = render_volume(n, 1.0, sim.download()[0], params)
+    bg = np.array([0.03, 0.04, 0.07], np.float32)
+    assert (np.abs(want - bg).max(axis=2) > 1e-3).sum() > 100  # the plume is visible
+    diff = np.abs(got - want)
+    assert (diff > 1e-4).mean() < 1e-3, float(diff.max())
+    assert float(diff.max()) < 0.05
+    sim.close()

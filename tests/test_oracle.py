@@ -470,3 +470,28 @@ def test_comparison_metrics_known_answers():
     # traces of +-6 cells stay inside only for no cell of an 8-wide box
     assert m["boundary_fallback"] == n ** 3
     assert m["grad_per_mass"] == 0.0 and m["max_div"] == 0.0
+
+
+def test_volume_render_restatement_known_answers(tmp_path):
+    """The oracle's restatement of the volume shader (volume.frag:13-55): an
+    empty volume leaves the clear colour everywhere; a box full of dense smoke
+    saturates the pixels whose rays meet it (alpha reaches 0.99 in a few
+    steps) and leaves the others at the clear colour; the PPM writer emits the
+    harness's header and top row first."""
+    from oracle_lib import render_volume
+    from vapor_b200.abi import RenderParams
+    from vapor_b200.diagnostics import write_ppm
+    n = 16
+    params = RenderParams.harness(48, 32)
+    bg = np.array([0.03, 0.04, 0.07], np.float32)
+    img = render_volume(n, 1.0, np.zeros((n, n, n), np.float32), params)
+    assert np.array_equal(img, np.broadcast_to(bg, img.shape))
+    full = render_volume(n, 1.0, np.full((n, n, n), 50.0, np.float32), params)
+    centre = full[16, 24]
+    assert not np.allclose(centre, bg) and 0.0 < centre.max() <= 1.0
+    corner = full[0, 0]
+    assert np.allclose(corner, bg)  # the box does not reach the image corner from this camera
+    path = tmp_path / "img.ppm"
+    write_ppm(path, full)
+    data = path.read_bytes()
+    assert data.startswith(b"P6\n48 32\n255\n") and len(data) == len(b"P6\n48 32\n255\n") + 48 * 32 * 3

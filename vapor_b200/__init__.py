@@ -86,6 +86,8 @@ def _declare(lib):
     f("vapor_mac3d_total_iterations", _vp, C.POINTER(C.c_int64))
     f("vapor_mac3d_diagnostics", _vp, C.POINTER(FluidDiagnostics))
     f("vapor_mac3d_comparison_metrics", _vp, C.c_float, C.POINTER(abi.ComparisonMetrics))
+    f("vapor_mac3d_render", _vp, C.POINTER(abi.RenderParams), _vp)
+    f("vapor_render_volume", _vp, C.c_int32, C.c_float, C.POINTER(abi.RenderParams), _vp, _vp)
     f("vapor_mac3d_upload", _vp, _vp, _vp, _vp, _vp)
     f("vapor_mac3d_download", _vp, _vp, _vp, _vp, _vp)
     f("vapor_mac3d_byte_counters", _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
@@ -277,6 +279,15 @@ class MacSimulation3D:
         d = FluidDiagnostics()
         check(library().vapor_mac3d_diagnostics(self._h, C.byref(d)))
         return d
+
+    def render(self, params=None):
+        """Headless ray-marched image of the current density (the reference's
+        volume shader): a (height, width, 3) float32 array, row 0 at the
+        bottom. params: abi.RenderParams (default: the harness's 960 x 960)."""
+        params = params or abi.RenderParams.harness()
+        rgb = np.empty((params.height, params.width, 3), np.float32)
+        check(library().vapor_mac3d_render(self._h, C.byref(params), rgb.ctypes.data))
+        return rgb
 
     def comparison_metrics(self, frames_per_second=60.0):
         """The reference harness's comparison metrics of the current state

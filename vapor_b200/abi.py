@@ -95,6 +95,20 @@ class ComparisonMetrics(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name not in ("nonfinite", "reserved")}
 
 
+class RenderParams(C.Structure):
+    """vapor_render_params: camera, ray step, opacity and shadow of the
+    headless ray-march. harness() gives the reference harness's image."""
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("azimuth", C.c_float), ("elevation", C.c_float),
+                ("distance", C.c_float), ("step_scale", C.c_float), ("alpha_mul", C.c_float),
+                ("light", C.c_float * 3), ("shadow_strength", C.c_float), ("shadow_step", C.c_float)]
+
+    @classmethod
+    def harness(cls, width=960, height=960):
+        norm = 1.25 ** 0.5
+        return cls(width, height, -1.2, 0.3, 2.5, 0.5, 30.0, (C.c_float * 3)(0.3 / norm, 0.4 / norm, 1.0 / norm),
+                   0.3, 0.1)
+
+
 class MacParams(C.Structure):
     _fields_ = [
         ("emitter_radius", C.c_float),

@@ -201,6 +201,27 @@ VB_API vapor_status vapor_mac3d_comparison_metrics(vapor_mac3d* sim, float frame
               require(std::isfinite(frames_per_second) && frames_per_second > 0.f, "Invalid frame rate");
               sim->sim.comparison_metrics(frames_per_second, out));
 }
+static void validate_render(const vapor_render_params* p) {
+    require(p != nullptr, "null parameters");
+    require(p->width > 0 && p->height > 0 && p->width <= 16384 && p->height <= 16384, "Invalid image size");
+    const float v[] = {p->azimuth, p->elevation, p->distance, p->step_scale, p->alpha_mul, p->light[0],
+                       p->light[1], p->light[2], p->shadow_strength, p->shadow_step};
+    for (float x : v) require(std::isfinite(x), "Non-finite render parameter");
+    require(p->step_scale > 0.f && p->distance > 0.f, "Invalid ray step or camera distance");
+    require(p->shadow_strength <= 0.f || p->shadow_step > 0.f, "Invalid shadow step");
+}
+VB_API vapor_status vapor_render_volume(const float* density_device, int32_t n, float box,
+                                        const vapor_render_params* params, float* rgb_device, void* stream) {
+    return guarded([&] {
+        vb::validate_grid(n, box);
+        validate_render(params);
+        require(density_device && rgb_device, "null buffer");
+        vb::render_volume(density_device, n, box, *params, rgb_device, static_cast<cudaStream_t>(stream));
+    });
+}
+VB_API vapor_status vapor_mac3d_render(vapor_mac3d* sim, const vapor_render_params* params, float* rgb_host) {
+    SIM_GUARD(validate_render(params); require(rgb_host != nullptr, "null output"); sim->sim.render(*params, rgb_host));
+}
 VB_API vapor_status vapor_mac3d_upload(vapor_mac3d* sim, const float* d, const float* u, const float* v,
                                        const float* w) {
     SIM_GUARD(require(d && u && v && w, "null field"); sim->sim.upload(d, u, v, w));

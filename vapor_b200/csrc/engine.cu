@@ -1083,6 +1083,15 @@ void Simulation::diagnostics(vapor_fluid_diagnostics* out) {
     ws_.diagnostics(vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p, out);
 }
 
+void Simulation::render(const vapor_render_params& p, float* rgb_host) {
+    const size_t count = size_t(3) * p.width * p.height;
+    DevArray<float> rgb;
+    rgb.allocate(count);
+    render_volume(dens_[cur_].p, ws_.n(), ws_.box(), p, rgb.p, ws_.stream());
+    VB_CUDA(cudaMemcpyAsync(rgb_host, rgb.p, count * sizeof(float), cudaMemcpyDeviceToHost, ws_.stream()));
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+}
+
 void Simulation::comparison_metrics(float frames_per_second, vapor_comparison_metrics* out) {
     vb::comparison_metrics(ws_.grid(), frames_per_second, params.cfl_mc, dens_[cur_].p, vel_[S_][0].p,
                            vel_[S_][1].p, vel_[S_][2].p, out, ws_.stream());

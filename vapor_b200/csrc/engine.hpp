@@ -225,6 +225,8 @@ public:
     void diagnostics(vapor_fluid_diagnostics* out);
     // The harness comparison metrics of the current state (waits).
     void comparison_metrics(float frames_per_second, vapor_comparison_metrics* out);
+    // Ray-marched image of the current density into host memory (waits).
+    void render(const vapor_render_params& p, float* rgb_host);
     long long total_iterations() { return ws_.total_iterations(); }
     PhaseTimer& timer() { return ws_.timer(); }
 

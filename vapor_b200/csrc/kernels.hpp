@@ -263,6 +263,9 @@ void launch_log_coarse(const float* rc, size_t cells, float* log, int capacity, 
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
                               cudaStream_t s);
 
+// ---- headless rendering (kernels_render.cu) ----
+void render_volume(const float* density, int n, float box, const vapor_render_params& p, float* rgb, cudaStream_t s);
+
 // ---- diagnostics ----
 // Comparison metrics of (d, u, v, w) (kernels_metrics.cu); waits for the
 // stream; VAPOR_NON_FINITE on a non-finite divergence.

@@ -2,7 +2,8 @@
 comparison of the reference's diagnostic harness
 (tests/ReflectionComparison.hpp:9-75), run on the device.
 
-  python -m vapor_b200.diagnostics compare-reflection [--n 64 --frames 120 --iterations 40 --out DIR]
+  python -m vapor_b200.diagnostics compare-reflection [--n 64 --frames 120 --iterations 40 --out DIR
+                                                      --image 960]
 
 For each of the four variants (Reflection with semi-Lagrangian or MacCormack
 velocity and smoke) the scene of the harness is stepped at 60 frames per
@@ -11,7 +12,10 @@ second; every 60th frame and the last one print the harness's metric line
 CFL and boundary fallbacks, max CFL; computed on the device by
 vapor_mac3d_comparison_metrics) and write the raw density as
 DIR/v<variant>_f<frame>.density: n^3 little-endian FP32 values, x fastest,
-exactly the bytes the harness writes.
+exactly the bytes the harness writes, and its image as
+DIR/v<variant>_f<frame>.ppm: the headless CUDA ray-march of the density
+(vapor_mac3d_render, the reference's volume shader and camera) in place of
+the harness's OpenGL render.
 """
 import argparse
 import os
@@ -19,6 +23,17 @@ import os
 import numpy as np
 
 from . import MacSimulation3D, default_params
+
+
+def write_ppm(path, rgb):
+    """The harness's image file: binary PPM, 8-bit RGB, top row first
+    (rgb is (height, width, 3) in [0, 1] with row 0 at the bottom, as the
+    renderer writes it)."""
+    img = np.clip(np.rint(np.asarray(rgb, np.float32)[::-1] * 255.0), 0, 255).astype(np.uint8)
+    h, w = img.shape[:2]
+    with open(path, "wb") as f:
+        f.write(f"P6\n{w} {h}\n255\n".encode())
+        f.write(img.tobytes())
 
 
 def write_density(path, density):
@@ -53,10 +68,11 @@ def metric_line(variant, p, frame, m):
             f"smoke_boundary_fallback={m['boundary_fallback']} smoke_max_cfl={m['max_cfl']:.6g}")
 
 
-def compare_reflection(n=64, frames=120, iterations=40, out=None, render=None):
-    """Runs the four variants; returns their metric records. `render`, when
-    given, is called as render(density, n, path_without_extension) at every
-    reported frame (the harness's image)."""
+def compare_reflection(n=64, frames=120, iterations=40, out=None, image_size=960):
+    """Runs the four variants; returns their metric records. With `out`, every
+    reported frame also writes the raw density and the harness's ray-marched
+    image (image_size^2 pixels, 0: none) as .density and .ppm files."""
+    from .abi import RenderParams
     records = []
     if out:
         os.makedirs(out, exist_ok=True)
@@ -72,10 +88,9 @@ def compare_reflection(n=64, frames=120, iterations=40, out=None, render=None):
             print(metric_line(variant, p, frame, m), flush=True)
             if out:
                 base = os.path.join(out, f"v{variant}_f{frame}")
-                d = sim.download()[0]
-                write_density(base + ".density", d)
-                if render:
-                    render(d, n, base)
+                write_density(base + ".density", sim.download()[0])
+                if image_size:
+                    write_ppm(base + ".ppm", sim.render(RenderParams.harness(image_size, image_size)))
         sim.close()
     return records
 
@@ -88,8 +103,9 @@ def main():
     c.add_argument("--frames", type=int, default=120)
     c.add_argument("--iterations", type=int, default=40)
     c.add_argument("--out", default="reflection-comparison")
+    c.add_argument("--image", type=int, default=960, help="image size in pixels (0: no images)")
     args = ap.parse_args()
-    compare_reflection(args.n, args.frames, args.iterations, args.out)
+    compare_reflection(args.n, args.frames, args.iterations, args.out, args.image)
 
 
 if __name__ == "__main__":
