@@ -397,16 +397,17 @@ vapor_status vapor_advect_noalloc(int32_t n, float box, int32_t loc, float dt, f
  * recorded into graphs. vapor_b200/autotune.py measures and chooses it. */
 vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes);
 /* Tuning (extension): red+black iterations per launch of the temporally
- * blocked sweep (1 or 2, default 2), or 0 for one launch per colour (the
- * z-marching sweep). Applies to grids with n divisible by 8; results are bit
- * for bit the same either way. Process-wide; set it before recording steps. */
+ * blocked sweep (1 or 2), or 0 (default) for one launch per colour (the
+ * z-marching sweep, faster on B200 at the benchmark's sizes). Applies to
+ * grids with n divisible by 8; results are bit for bit the same either way.
+ * Process-wide; set it before recording steps. */
 vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch);
 /* Tuning (extension): z chunks per blocked launch for grids of size n (0 =
  * automatic: one wave of resident CTAs). Results do not depend on it. */
 vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks);
-/* Tuning (extension): 1 (default) runs the learned network's 3x3x3
- * convolutions that fit in shared memory on the warp-specialised tcgen05
- * kernel (producer, MMA and epilogue warps on mbarriers), 0 on the
+/* Tuning (extension): 1 runs the learned network's 3x3x3 convolutions that
+ * fit in shared memory on the warp-specialised tcgen05 kernel (producer, MMA
+ * and epilogue warps on mbarriers), 0 (default, measured faster) on the
  * block-synchronous z-marching kernel. Same results either way. */
 vapor_status vapor_tune_conv_kernel(int32_t warp_specialised);
 

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(autouse=True)
 def _restore_blocking():
     yield
-    vb.tune_sor_blocking(2)
+    vb.tune_sor_blocking(0)
 
 
 def _project(n, fields, kind, blocking, opts, omega=1.9, floor=6.0, mask=None, net=None):
@@ -132,3 +132,37 @@ def test_resident_plume_steps_blocked_equal_one_colour_sweeps():
         assert outs[0][0] == outs[1][0]
         for x, y in zip(outs[0][1], outs[1][1]):
             assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_batched_scenes_with_blocking_equal_one_colour_steps():
+    """Blocked sweeps inside batched scene graphs (several scenes' solve loops
+    running at once) against separate scenes stepped with the one-colour
+    sweep: the out-of-place blocked update must see no half-written halo."""
+    from oracle_lib import algorithm_params
+
+    def scene(n, alg, k):
+        p = algorithm_params(alg)
+        p.stir_strength = 0.5
+        p.emitter_center_x = 0.3 + 0.1 * k
+        p.use_solve_options = 1
+        p.solve = LinearSolveOptions.defaults(max_iterations=3000, relative_tolerance=1e-6, absolute_tolerance=0.0)
+        p.solver_kind = SOLVER_MIXED_REFINEMENT
+        return vb.MacSimulation3D(n, 1.0, p)
+
+    sizes = [(16, 3), (24, 1), (32, 2), (40, 0)]
+    vb.tune_sor_blocking(0)
+    single = [scene(n, a, k) for k, (n, a) in enumerate(sizes)]
+    for _ in range(4):
+        for s in single:
+            s.advance(0.01)
+    vb.tune_sor_blocking(2)
+    grouped = [scene(n, a, k) for k, (n, a) in enumerate(sizes)]
+    batch = vb.Batch(grouped)
+    for _ in range(4):
+        batch.advance(0.01)
+    batch.synchronize()
+    for a, b in zip(single, grouped):
+        assert a.total_iterations() == b.total_iterations()
+        for x, y in zip(a.download(), b.download()):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    batch.close()

@@ -151,9 +151,9 @@ def test_warp_specialised_convolutions_equal_block_synchronous(n):
             outs.append(out.cpu().numpy())
             grads.append(gp)
     finally:
-        vb.tune_conv_kernel(1)
+        vb.tune_conv_kernel(0)
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
-    assert np.abs(grads[0] - grads[1]).max() <= 1e-5 * np.abs(grads[0]).max()
+    assert np.abs(grads[0] - grads[1]).max() <= 1e-4 * np.abs(grads[0]).max()
 
 
 @pytest.mark.parametrize("ws", [0, 1])
@@ -179,7 +179,7 @@ def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     vb.check(net.lib.vapor_unet_set_wait_probe(net.h, 0))
     after = torch.zeros_like(before)
     vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), after.data_ptr()))
-    vb.tune_conv_kernel(1)
+    vb.tune_conv_kernel(0)
     assert torch.equal(after, before)
 
 

@@ -367,13 +367,13 @@ def tune_sor_planes(n, planes):
 
 
 def tune_sor_blocking(iterations_per_launch):
-    """Red+black iterations per temporally blocked sweep launch (1 or 2; 0:
-    one launch per colour). Same results either way."""
+    """Red+black iterations per temporally blocked sweep launch (1 or 2; 0,
+    the default: one launch per colour). Same results either way."""
     check(library().vapor_tune_sor_blocking(int(iterations_per_launch)))
 
 
 def tune_conv_kernel(warp_specialised):
-    """1: warp-specialised tcgen05 convolutions (default); 0: block-synchronous
+    """1: warp-specialised tcgen05 convolutions; 0 (default): block-synchronous
     z-marching ones. Same results either way."""
     check(library().vapor_tune_conv_kernel(int(warp_specialised)))
 

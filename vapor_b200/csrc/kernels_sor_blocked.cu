@@ -287,7 +287,9 @@ __global__ void __launch_bounds__(Blocked<K, TY>::THREADS, 2) k_sor_blocked(
 
 std::mutex g_blocked_mutex;
 std::map<int, int> g_blocked_chunks;  // grid size -> z chunks per launch (tuning)
-std::atomic<int> g_block_iterations{2};
+// Off by default: on B200 at 256^3 the blocked launch costs more per
+// iteration than two one-colour launches (see set_sor_block_iterations).
+std::atomic<int> g_block_iterations{0};
 
 template <int K, int TY, int FIRST, bool EXACT, bool RESID, bool FROM_ZERO, bool MASK>
 void launch_blocked(const ProjectionArgs& a, const float* xin, float* xout, const float* b, ProjControl* ctrl,

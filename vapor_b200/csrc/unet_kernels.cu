@@ -25,9 +25,10 @@ namespace {
 
 constexpr int kWaitLimit = 1 << 22;
 
-// Convolutions that fit take the warp-specialised kernel (else the
-// block-synchronous z-marching one); both give the same results.
-std::atomic<bool> g_conv_ws{true};
+// Convolutions that fit take the block-synchronous z-marching kernel unless
+// the warp-specialised one is selected; both give the same results (the
+// warp-specialised form measured no faster on B200).
+std::atomic<bool> g_conv_ws{false};
 
 __device__ __forceinline__ void decode(long v, int H, int W, int& x, int& y, int& z) {
     x = int(v % W);
