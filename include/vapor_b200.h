@@ -405,11 +405,14 @@ vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch);
 /* Tuning (extension): z chunks per blocked launch for grids of size n (0 =
  * automatic: one wave of resident CTAs). Results do not depend on it. */
 vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks);
-/* Tuning (extension): 1 runs the learned network's 3x3x3 convolutions that
- * fit in shared memory on the warp-specialised tcgen05 kernel (producer, MMA
- * and epilogue warps on mbarriers), 0 (default, measured faster) on the
- * block-synchronous z-marching kernel. Same results either way. */
-vapor_status vapor_tune_conv_kernel(int32_t warp_specialised);
+/* Tuning (extension): the tcgen05 kernel of the learned network's 3x3x3
+ * convolutions whose weights fit in shared memory. 0 (default): the
+ * block-synchronous z-march (27 MMAs of width cout per output plane); 1: its
+ * warp-specialised form (producer, MMA and epilogue warps on mbarriers; same
+ * results); 2: the plane-window form (9 MMAs of width 3 cout per input
+ * plane, three output planes per MMA; same results for 16 input channels,
+ * FP32-rounding differences for more). */
+vapor_status vapor_tune_conv_kernel(int32_t kind);
 
 /* ---- Batched scenes (extension, no reference counterpart) ----
  * Steps many resident simulations (uneven grid sizes allowed, each with its

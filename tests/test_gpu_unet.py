@@ -156,7 +156,37 @@ def test_warp_specialised_convolutions_equal_block_synchronous(n):
     assert np.abs(grads[0] - grads[1]).max() <= 1e-4 * np.abs(grads[0]).max()
 
 
-@pytest.mark.parametrize("ws", [0, 1])
+@pytest.mark.parametrize("n", [8, 16, 32])
+def test_plane_window_convolutions_match_torch_reference(n):
+    """The plane-window convolution kernel (three output planes per MMA)
+    against the PyTorch FP32 reference, forward and gradients, at the bars of
+    the block-synchronous kernel's tests."""
+    import torch
+    try:
+        vb.tune_conv_kernel(2)
+        net = Net(seed=11)
+        p = net.params()
+        x = features(n, 3)
+        xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+        out = torch.zeros(n * n * n, dtype=torch.float32, device="cuda")
+        vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+        got = out.cpu().numpy().reshape(n, n, n)
+        ref, *_ = torch_reference(p, xin.float().cpu().numpy())
+        ref = ref.detach().numpy()
+        err = np.abs(got - ref).max() / max(1e-6, np.abs(ref).max())
+        assert err < 2e-2, err
+        # against the block-synchronous kernel: the same network up to FP32
+        # rounding of the multi-chunk layers, carried through BF16 storage
+        vb.tune_conv_kernel(0)
+        out0 = torch.zeros_like(out)
+        vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out0.data_ptr()))
+        d = (out - out0).abs().max().item() / max(1e-6, out0.abs().max().item())
+        assert d < 1e-2, d
+    finally:
+        vb.tune_conv_kernel(0)
+
+
+@pytest.mark.parametrize("ws", [0, 1, 2])
 def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     """The convolutions' completion waits poll an mbarrier with an iteration
     limit. With the test hook they poll one that nothing completes, run out,

@@ -372,10 +372,11 @@ def tune_sor_blocking(iterations_per_launch):
     check(library().vapor_tune_sor_blocking(int(iterations_per_launch)))
 
 
-def tune_conv_kernel(warp_specialised):
-    """1: warp-specialised tcgen05 convolutions; 0 (default): block-synchronous
-    z-marching ones. Same results either way."""
-    check(library().vapor_tune_conv_kernel(int(warp_specialised)))
+def tune_conv_kernel(kind):
+    """tcgen05 convolution kernel: 0 (default) block-synchronous z-march, 1
+    its warp-specialised form, 2 the plane-window form (three output planes
+    per MMA)."""
+    check(library().vapor_tune_conv_kernel(int(kind)))
 
 
 def tune_sor_blocked_chunks(n, chunks):

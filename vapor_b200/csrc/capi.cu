@@ -330,10 +330,10 @@ VB_API vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes) {
     });
 }
 
-VB_API vapor_status vapor_tune_conv_kernel(int32_t warp_specialised) {
+VB_API vapor_status vapor_tune_conv_kernel(int32_t kind) {
     return guarded([&] {
-        require(warp_specialised == 0 || warp_specialised == 1, "0 or 1");
-        vb::unet::set_conv_warp_specialised(warp_specialised != 0);
+        require(kind >= 0 && kind <= 2, "0, 1 or 2");
+        vb::unet::set_conv_kernel(kind);
     });
 }
 VB_API vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch) {

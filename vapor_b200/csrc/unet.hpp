@@ -51,9 +51,11 @@ struct WGradArgs {
 
 // Sets the kernels' shared-memory limits (once per device, before use).
 void configure_conv_kernels();
-// Selects the warp-specialised convolution kernel (default) or the
-// block-synchronous one for every later launch (same results).
-void set_conv_warp_specialised(bool on);
+// Selects the kernel of every later convolution whose weights fit in shared
+// memory: 0 the block-synchronous z-march, 1 its warp-specialised form (same
+// results), 2 the plane-window form (same results with one input chunk,
+// FP32-rounding differences with several).
+void set_conv_kernel(int kind);
 void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
 void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,

@@ -25,10 +25,10 @@ namespace {
 
 constexpr int kWaitLimit = 1 << 22;
 
-// Convolutions that fit take the block-synchronous z-marching kernel unless
-// the warp-specialised one is selected; both give the same results (the
-// warp-specialised form measured no faster on B200).
-std::atomic<bool> g_conv_ws{false};
+// Kernel for the convolutions whose weights fit in shared memory: 0 the
+// block-synchronous z-march, 1 its warp-specialised form, 2 the plane-window
+// form (three output planes per MMA).
+std::atomic<int> g_conv_kind{0};
 
 __device__ __forceinline__ void decode(long v, int H, int W, int& x, int& y, int& z) {
     x = int(v % W);
@@ -600,6 +600,200 @@ __global__ void __launch_bounds__(ConvWS<N>::kThreads) k_conv3_ws(ConvArgs a, in
     if (warp == 1) tc::tmem_dealloc(tmem, W::kCols);
 }
 
+// Plane-window form of the z-marching convolution. The MMA's N dimension
+// holds the output channels of three consecutive output planes: for input
+// plane zi and in-plane tap (dy, dx), one MMA (M = 128 voxels, N = 3 cout,
+// K = 16 channels) multiplies the input voxels shifted by (dy, dx) with the
+// weights of taps (dz = -1, 0, +1; dy, dx) and accumulates into the TMEM
+// columns of output planes zi + 1, zi and zi - 1, which lie next to each
+// other: output plane z owns columns N (z1 + 1 - z) .. + N. So a CTA issues
+// 9 MMAs of width 3N per input plane and chunk instead of 27 of width N per
+// output plane, with every input plane staged once. An output plane is
+// complete once the MMAs of the input plane above it have finished; its
+// epilogue then runs while the next input plane's MMAs execute. The TMEM
+// window is cleared first, so every MMA accumulates. With one 16-channel
+// chunk the sum over the 27 taps runs in the same order as in k_conv3_zm
+// (dz, dy, dx), and the results are the same; with several chunks the order
+// is (dz, chunk, dy, dx) in place of (chunk, dz, dy, dx).
+template <int N>
+struct ConvWindow {
+    static constexpr int kPlane = 18 * 320;
+    static constexpr bool kSupported = 3 * N <= 256;
+    __host__ __device__ static uint32_t cols(int zt) {
+        const uint32_t need = uint32_t(N) * uint32_t(zt + 4);
+        uint32_t c = 32;
+        while (c < need) c <<= 1;
+        return c;
+    }
+    static int smem(int cin, int ring) { return 27 * N * cin * 2 + ring * (cin / 16) * kPlane + 1024; }
+    static bool fits(int cin, int ring, int zt) {
+        return kSupported && smem(cin, ring) <= 200 * 1024 && cols(zt) <= 512;
+    }
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_conv3_zn(ConvArgs a, int zt, int ring) {
+    using Wd = ConvWindow<N>;
+    constexpr int NW = 3 * N;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bars[3];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float s_bias[N];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16;
+    const int z0 = blockIdx.z * zt, z1 = min(a.D, z0 + zt);
+    const int inputs = z1 - z0 + 2;  // input planes z0 - 1 .. z1
+    const int chunks = a.cin / 16;
+    const uint32_t ncols = Wd::cols(zt);
+    const uint32_t sbase = tc::smem_addr(smem);
+    const uint32_t wbase = sbase;
+    const uint32_t rbase = sbase + uint32_t(27 * N * a.cin * 2);
+    const uint32_t plane_bytes = uint32_t(chunks * Wd::kPlane);
+    const uint32_t bar0 = tc::smem_addr(&bars[0]);  // commits of input planes alternate bar0, bar0 + 8
+    const uint32_t probe = bar0 + 16;               // never arrived on (timeout test hook)
+
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), ncols);
+    if (tid == 0) {
+        tc::mbar_init(bar0, 1);
+        tc::mbar_init(bar0 + 8, 1);
+        tc::mbar_init(probe, 1);
+        tc::fence_mbarrier_init();
+    }
+    for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
+    // weights as B rows (j, co) = tap (j * 9 + s), co: [chunk][s][3N rows / 8][2][8][16 B]
+    for (int i = tid; i < chunks * 9 * NW * 2; i += blockDim.x) {
+        const int half = i & 1, row = (i >> 1) % NW, cs = (i >> 1) / NW;  // cs = chunk * 9 + s
+        const int j = row / N, co = row - j * N, s = cs % 9, cc = cs / 9;
+        const int t = j * 9 + s;
+        const __nv_bfloat16* wsrc = a.w + (long(t) * N + co) * a.cin + cc * 16 + half * 8;
+        tc::cp_async16(wbase + uint32_t(cs * NW * 32 + (row >> 3) * 256 + half * 128 + (row & 7) * 16), wsrc, true);
+    }
+    auto slot_of = [&](int q) { return uint32_t(q % ring) * plane_bytes; };
+    // input plane q (zz = z0 - 1 + q, all chunks) into its ring slot; rows
+    // outside the grid read as zero
+    auto load_plane = [&](int q) {
+        const int zz = z0 - 1 + q;
+        const uint32_t slot = rbase + slot_of(q);
+        for (int i = tid; i < chunks * 18 * 20; i += blockDim.x) {
+            const int half = i & 1, v = (i >> 1) % 10, rc = (i >> 1) / 10;  // rc = chunk * 18 + ry
+            const int ry = rc % 18, cc = rc / 18;
+            const int x = x0 - 1 + v, y = y0 + ry - 1;
+            const bool valid = x >= 0 && x < a.W && y >= 0 && y < a.H && zz >= 0 && zz < a.D;
+            const __nv_bfloat16* src =
+                valid ? a.in + ((long(zz) * a.H + y) * a.W + x) * a.in_stride + cc * 16 + half * 8 : a.in;
+            tc::cp_async16(slot + uint32_t(rc * 320 + half * 160 + v * 16), src, valid);
+        }
+    };
+    // group 0: the weights and input planes 0, 1; then one group per plane
+    // ahead (planes 2 .. ring - 2)
+    load_plane(0);
+    load_plane(1);
+    tc::cp_async_commit();
+    for (int q = 2; q <= ring - 2; ++q) {
+        if (q < inputs) load_plane(q);
+        tc::cp_async_commit();
+    }
+    tc::tc_fence_before();
+    __syncthreads();  // the TMEM allocation is visible
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    {
+        // clear the accumulator window (warp w: the lanes of quarter w & 3,
+        // the columns of half w >> 2)
+        const uint32_t zero[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        const uint32_t half_cols = ncols / 2;
+        for (uint32_t c = 0; c < half_cols; c += 8)
+            tc::tmem_st8(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(warp >> 2) * half_cols + c, zero);
+    }
+    tc::cp_async_wait_group<0>();  // the weights and the first ring - 1 planes have landed
+    tc::fence_proxy_async();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    constexpr uint32_t idesc = tc::instr_desc_bf16(128, NW);
+    const uint64_t a_desc = tc::smem_desc(rbase, 160, 320);
+    const uint64_t b_desc = tc::smem_desc(wbase, 128, 256);
+    auto col_of = [&](int z) { return uint32_t(N * (z1 + 1 - z)); };  // output plane z's first column
+    // one thread: the 9 x chunks MMAs of input plane q, committed to bar0 + 8 (q & 1)
+    auto issue = [&](int q) {
+        tc::tc_fence_after();
+        const int zi = z0 - 1 + q;
+        if (zi >= 0 && zi < a.D) {  // planes outside the grid are zero and add nothing
+            const uint32_t d = tmem + col_of(zi + 1);
+            const uint64_t ad = a_desc + (slot_of(q) >> 4);
+#pragma unroll 1
+            for (int cc = 0; cc < chunks; ++cc)
+#pragma unroll
+                for (int s = 0; s < 9; ++s) {
+                    const int dy = s / 3, dx = s - 3 * dy;
+                    tc::mma_bf16(d, ad + uint32_t(cc * (Wd::kPlane >> 4)) + uint32_t((dy * 320 + dx * 16) >> 4),
+                                 b_desc + uint32_t((cc * 9 + s) * NW * 2), idesc, true);
+                }
+        }
+        tc::mma_commit(bar0 + uint32_t(8 * (q & 1)));
+    };
+    bool ok = true;
+    int commits[2] = {0, 0};  // per barrier, counted by every thread
+    auto wait_commit = [&](int q) {
+        const int k = q & 1;
+        const bool mine = a.wait_probe ? tc::mbar_wait(probe, 0u, a.wait_probe)
+                                       : tc::mbar_wait(bar0 + uint32_t(8 * k), uint32_t(commits[k] - 1) & 1u,
+                                                       kWaitLimit);
+        return __syncthreads_and(mine) != 0;
+    };
+    for (int q = 0; q < inputs; ++q) {
+        // input plane q has landed (its group and all earlier ones)
+        if (q >= 2) {
+            // plane q + ring - 2 goes into the slot of plane q - 2, whose MMAs
+            // completed (waited for in step q - 1); plane q was requested in
+            // step q - ring + 2, so all but the ring - 2 newest groups must land
+            if (q + ring - 2 < inputs) load_plane(q + ring - 2);
+            tc::cp_async_commit();
+            if (ring == 6) tc::cp_async_wait_group<4>();
+            else tc::cp_async_wait_group<2>();
+            tc::fence_proxy_async();
+            tc::tc_fence_before();
+            __syncthreads();
+        }
+        if (tid == 0) issue(q);
+        ++commits[q & 1];
+        if (q >= 1) {
+            // MMAs of input plane q - 1 complete: output plane z0 + q - 3 + 1
+            // = zi(q) - 2 has all its contributions
+            if (!wait_commit(q - 1)) {
+                ok = false;
+                break;
+            }
+            tc::tc_fence_after();
+            const int zo = z0 - 1 + q - 2;
+            if (zo >= z0 && zo < z1) conv_epilogue<N>(a, tmem + col_of(zo), s_bias, x0, y0, zo, warp, lane);
+        }
+    }
+    if (ok) {
+        // the last input plane's MMAs: output plane z1 - 1
+        if (!wait_commit(inputs - 1)) {
+            ok = false;
+        } else {
+            tc::tc_fence_after();
+            const int zo = z1 - 1;
+            if (zo >= z0) conv_epilogue<N>(a, tmem + col_of(zo), s_bias, x0, y0, zo, warp, lane);
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(a.error, 1u);
+        // drain every commit still in flight, bounded
+        bool drained = true;
+        for (int k = 0; k < 2; ++k)
+            if (commits[k] > 0) drained &= tc::mbar_wait(bar0 + uint32_t(8 * k), uint32_t(commits[k] - 1) & 1u, kWaitLimit);
+        if (!drained) atomicOr(a.error, 2u);
+        tc::cp_async_wait_all();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
 // ---- CUDA-core kernels -------------------------------------------------------
 
 // Input features: channel 0 = b / scale (from the solver's red-black split RHS,
@@ -1072,6 +1266,8 @@ void configure_n() {
                                  ConvTile<N>::kSmemMax));
     VB_CUDA(cudaFuncSetAttribute(k_conv3_zm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     VB_CUDA(cudaFuncSetAttribute(k_conv3_ws<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    if constexpr (ConvWindow<N>::kSupported)
+        VB_CUDA(cudaFuncSetAttribute(k_conv3_zn<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 }
 
 // Resident CTAs per SM of the warp-specialised convolution: shared memory,
@@ -1089,7 +1285,36 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
         fail(VAPOR_INVALID_ARGUMENT, "convolution channel counts and strides must be multiples of 16 / 8");
     const unsigned gx = unsigned((a.W + 7) / 8), gy = unsigned((a.H + 15) / 16);
     count_launch();
-    if (g_conv_ws.load() && ConvWS<N>::fits(a.cin, 4)) {
+    const int kind = g_conv_kind.load();
+    bool done = false;
+    if constexpr (ConvWindow<N>::kSupported) {
+        if (kind == 2 && ConvWindow<N>::fits(a.cin, 4, 2)) {
+        // planes per CTA: the count that minimises waves x (planes + 2), the
+        // input planes a CTA multiplies; resident CTAs by shared memory and
+        // by TMEM columns (512 per SM)
+        const int ring = ConvWindow<N>::fits(a.cin, 6, 2) ? 6 : 4;
+        const int sms = device_sm_count();
+        int best = 2;
+        long best_cost = -1;
+        for (int zt : {2, 4, 6, 8, 12, 16}) {
+            if (!ConvWindow<N>::fits(a.cin, ring, zt)) continue;
+            const int by_smem = std::max(1, (228 * 1024) / (ConvWindow<N>::smem(a.cin, ring) + 1536));
+            const int by_tmem = int(512 / ConvWindow<N>::cols(zt));
+            const long slots = long(std::max(1, std::min({by_smem, by_tmem, 8}))) * sms;
+            const long ctas = long(gx) * gy * ((a.D + zt - 1) / zt);
+            const long cost = ((ctas + slots - 1) / slots) * (std::min(zt, a.D) + 2);
+            if (best_cost < 0 || cost < best_cost) {
+                best_cost = cost;
+                best = zt;
+            }
+        }
+        const dim3 grid(gx, gy, unsigned((a.D + best - 1) / best));
+        k_conv3_zn<N><<<grid, 256, ConvWindow<N>::smem(a.cin, ring), s>>>(a, best, ring);
+        done = true;
+        }
+    }
+    if (done) {
+    } else if (kind == 1 && ConvWS<N>::fits(a.cin, 4)) {
         // planes per CTA: the smallest power of two (at least 2, up to 16)
         // whose grid runs in one wave of resident CTAs; the 6-plane ring when
         // it fits without lowering the resident count
@@ -1123,7 +1348,10 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
 
 }  // namespace
 
-void set_conv_warp_specialised(bool on) { g_conv_ws.store(on); }
+void set_conv_kernel(int kind) {
+    if (kind < 0 || kind > 2) fail(VAPOR_INVALID_ARGUMENT, "convolution kernel: 0, 1 or 2");
+    g_conv_kind.store(kind);
+}
 
 void configure_conv_kernels() {
     configure_n<16>();
