@@ -125,8 +125,11 @@ def test_reflection_plume_128_matches_oracle_and_fp64_error():
     three steps with the mixed-precision solve to relative divergence 1e-6,
     bit for bit against the FP32 oracle with equal iteration counts; then one
     step from the GPU's state against the FP64 oracle (the same step in
-    double), with the max relative error of every field stated and bounded
-    by 1e-5, the per-step FP32 bar."""
+    double). Both solve that step to relative divergence 1e-10, so that the
+    difference is the FP32 arithmetic, not two different stopping iterates
+    (at 1e-6 the projected velocities of the two solves differ by up to
+    4e-5 relative at this size); the max relative error of every field is
+    stated and bounded by 1e-5, the per-step FP32 bar."""
     n = 128
     p = scene_params(vb.default_params(), n, rel=1e-6, max_iterations=20000)
     fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=5)]
@@ -144,10 +147,13 @@ def test_reflection_plume_128_matches_oracle_and_fp64_error():
     state = sim.download()
     for x, y in zip(state, ref.fields()):
         assert bits_equal(x, y)
+    tight = scene_params(vb.default_params(), n, rel=1e-10, max_iterations=40000)
+    sim.set_parameters(tight)
     f64 = OracleSim(n, 1.0, dtype=np.float64)
-    f64.params = p
+    f64.params = tight
     f64.set_fields(*[x.astype(np.float64) for x in state])
     sim.advance(DT)
+    assert sim.last_projection().linear_solve.converged
     assert f64.advance(DT) == 0
     errs = {}
     for name, x, y in zip(("density", "u", "v", "w"), sim.download(), f64.fields()):
