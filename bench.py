@@ -433,9 +433,11 @@ def main():
     def sor_roofline(ph, sweeps):
         """The red-black sweep phase of one eager step covering `sweeps`
         red+black iterations: per-launch algorithmic bytes over the average
-        launch time. A one-colour launch moves 6 B/cell (its colour's x and b,
-        the other colour's x, its x written); a temporally blocked launch of
-        several iterations reads x and b and writes x once, 12 B/cell."""
+        launch time. One red+black iteration reads x and b and writes x,
+        12 B/cell, so a one-colour launch is charged half of that, 6 B/cell
+        (the other colour's half of x, written by the previous launch, is
+        mostly read back from L2); a temporally blocked launch of several
+        iterations reads x and b and writes x once, 12 B/cell."""
         sor = ph["sor"]
         launches = max(1, sor["launches"])
         launch_ms = sor["ms"] / launches
