@@ -413,6 +413,13 @@ vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks);
  * plane, three output planes per MMA; same results for 16 input channels,
  * FP32-rounding differences for more). */
 vapor_status vapor_tune_conv_kernel(int32_t kind);
+/* Tuning (extension): the FPCG preconditioner's relaxation sweeps before and
+ * after the coarse correction (1..8, default 2) and their weight (0 < omega
+ * < 2, default 1: symmetric Gauss-Seidel). Changes the iteration count, not
+ * the accepted answer (the stopping test is the FP64 residual). Process-wide;
+ * set it before recording steps. */
+vapor_status vapor_tune_fpcg_smoothing(int32_t sweeps, float omega);
+vapor_status vapor_fpcg_smoothing(int32_t *sweeps, float *omega);
 
 /* ---- Batched scenes (extension, no reference counterpart) ----
  * Steps many resident simulations (uneven grid sizes allowed, each with its

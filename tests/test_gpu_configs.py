@@ -125,11 +125,17 @@ def test_reflection_plume_128_matches_oracle_and_fp64_error():
     three steps with the mixed-precision solve to relative divergence 1e-6,
     bit for bit against the FP32 oracle with equal iteration counts; then one
     step from the GPU's state against the FP64 oracle (the same step in
-    double). Both solve that step to relative divergence 1e-10, so that the
-    difference is the FP32 arithmetic, not two different stopping iterates
-    (at 1e-6 the projected velocities of the two solves differ by up to
-    4e-5 relative at this size); the max relative error of every field is
-    stated and bounded by 1e-5, the per-step FP32 bar."""
+    double), both solved to relative divergence 1e-10 so that the difference
+    is the FP32 arithmetic, not two stopping iterates.
+
+    The MacCormack limiter clamps to the 8 source values around the cell that
+    contains the back-traced point, so where a trace ends within rounding of
+    a cell face the two precisions clamp to different bounds: a handful of
+    velocity samples differ by up to 4.3e-5 relative (1, 5 and 4 samples of
+    u, v, w above 1e-5 at this size; the FP32 oracle shows the same). The
+    test bounds the rms relative error by 1e-6, the samples above 1e-5 by
+    1e-5 of the grid, and the max by 1e-4; the semi-Lagrangian step, which
+    has no such switch, is held to 1e-5 at every sample by the next test."""
     n = 128
     p = scene_params(vb.default_params(), n, rel=1e-6, max_iterations=20000)
     fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=5)]
@@ -155,11 +161,48 @@ def test_reflection_plume_128_matches_oracle_and_fp64_error():
     sim.advance(DT)
     assert sim.last_projection().linear_solve.converged
     assert f64.advance(DT) == 0
-    errs = {}
-    for name, x, y in zip(("density", "u", "v", "w"), sim.download(), f64.fields()):
-        errs[name] = float(np.abs(x.astype(np.float64) - y).max() / max(1e-30, float(np.abs(y).max())))
-    print("128^3 plume step vs FP64 oracle, max relative error:", errs)
-    assert max(errs.values()) <= 1e-5, errs
+    errs = fp64_errors(sim.download(), f64.fields())
+    print("128^3 plume step vs FP64 oracle (max, rms, samples above 1e-5):", errs)
+    for name, (mx, rms, above) in errs.items():
+        assert mx <= 1e-4 and rms <= 1e-6 and above <= 1e-5 * n ** 3, (name, errs)
+
+
+def fp64_errors(got, want):
+    """Per field: max and rms of |got - want| relative to max |want|, and the
+    count of samples whose error exceeds 1e-5 of it."""
+    out = {}
+    for name, x, y in zip(("density", "u", "v", "w"), got, want):
+        d = np.abs(x.astype(np.float64) - y)
+        m = max(1e-30, float(np.abs(y).max()))
+        out[name] = (float(d.max() / m), float(np.sqrt((d * d).mean()) / m), int((d > 1e-5 * m).sum()))
+    return out
+
+
+def test_semi_lagrangian_plume_step_fp64_error():
+    """The plume step with semi-Lagrangian velocity and smoke (every stage a
+    continuous function of its inputs) at 64^3 from an evolved state, solved
+    to 1e-10, against the FP64 oracle: every sample of every field within
+    1e-5 relative of the double-precision step (measured: below 1e-6)."""
+    n = 64
+    p = scene_params(vb.default_params(), n, rel=1e-10, max_iterations=40000)
+    p.mac_cormack_vel = 0
+    p.mac_cormack_smoke = 0
+    fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=5)]
+    sim = vb.MacSimulation3D(n, 1.0, p)
+    sim.upload(*fields)
+    for _ in range(3):
+        sim.advance(DT)
+    state = sim.download()
+    f64 = OracleSim(n, 1.0, dtype=np.float64)
+    f64.params = p
+    f64.set_fields(*[x.astype(np.float64) for x in state])
+    sim.advance(DT)
+    assert sim.last_projection().linear_solve.converged
+    assert f64.advance(DT) == 0
+    errs = fp64_errors(sim.download(), f64.fields())
+    print("64^3 semi-Lagrangian plume step vs FP64 oracle (max, rms, samples above 1e-5):", errs)
+    for name, (mx, rms, above) in errs.items():
+        assert mx <= 1e-5 and above == 0, (name, errs)
 
 
 def test_plume_256_learned_arm_matches_plain_arm():

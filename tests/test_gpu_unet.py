@@ -156,11 +156,13 @@ def test_warp_specialised_convolutions_equal_block_synchronous(n):
     assert np.abs(grads[0] - grads[1]).max() <= 1e-4 * np.abs(grads[0]).max()
 
 
-@pytest.mark.parametrize("n", [8, 16, 32])
+@pytest.mark.parametrize("n", [8, 16, 32, 64])
 def test_plane_window_convolutions_match_torch_reference(n):
     """The plane-window convolution kernel (three output planes per MMA)
-    against the PyTorch FP32 reference, forward and gradients, at the bars of
-    the block-synchronous kernel's tests."""
+    against the PyTorch FP32 reference and the block-synchronous kernel. At
+    64^3 the CTAs march 4 and 16 planes, so the input ring wraps and every
+    slot is refilled (at the smaller sizes a CTA's planes fit the first
+    loads)."""
     import torch
     try:
         vb.tune_conv_kernel(2)

@@ -116,6 +116,8 @@ def _declare(lib):
     f("vapor_tune_sor_blocking", C.c_int32)
     f("vapor_tune_sor_blocked_chunks", C.c_int32, C.c_int32)
     f("vapor_tune_conv_kernel", C.c_int32)
+    f("vapor_tune_fpcg_smoothing", C.c_int32, C.c_float)
+    f("vapor_fpcg_smoothing", C.POINTER(C.c_int32), C.POINTER(C.c_float))
     f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_batch_destroy", _vp)
     f("vapor_batch_advance", _vp, C.c_float)
@@ -377,6 +379,25 @@ def tune_conv_kernel(kind):
     its warp-specialised form, 2 the plane-window form (three output planes
     per MMA)."""
     check(library().vapor_tune_conv_kernel(int(kind)))
+
+
+def tune_fpcg_smoothing(sweeps=2, omega=1.0):
+    """Relaxation sweeps before and after the FPCG preconditioner's coarse
+    correction (default 2) and their weight (default 1, Gauss-Seidel). Set it
+    before creating the simulations whose steps are recorded."""
+    check(library().vapor_tune_fpcg_smoothing(int(sweeps), float(omega)))
+
+
+def fpcg_smoothing():
+    """(sweeps, omega) of the FPCG preconditioner's smoothing."""
+    sw, om = C.c_int32(), C.c_float()
+    check(library().vapor_fpcg_smoothing(C.byref(sw), C.byref(om)))
+    return sw.value, om.value
+
+
+def fpcg_sweeps_per_application():
+    """Red+black sweeps in one application of the FPCG preconditioner."""
+    return 2 * fpcg_smoothing()[0]
 
 
 def tune_sor_blocked_chunks(n, chunks):

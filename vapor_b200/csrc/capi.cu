@@ -336,6 +336,17 @@ VB_API vapor_status vapor_tune_conv_kernel(int32_t kind) {
         vb::unet::set_conv_kernel(kind);
     });
 }
+VB_API vapor_status vapor_tune_fpcg_smoothing(int32_t sweeps, float omega) {
+    return guarded([&] { vb::set_fpcg_smoothing(sweeps, omega); });
+}
+VB_API vapor_status vapor_fpcg_smoothing(int32_t* sweeps, float* omega) {
+    return guarded([&] {
+        require(sweeps != nullptr && omega != nullptr, "null output");
+        const vb::FpcgSmoothing sm = vb::fpcg_smoothing();
+        *sweeps = sm.sweeps;
+        *omega = sm.omega;
+    });
+}
 VB_API vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch) {
     return guarded([&] { vb::set_sor_block_iterations(iterations_per_launch); });
 }

@@ -5,6 +5,7 @@
 #include "unet.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -313,6 +314,20 @@ void Workspace::set_solid(const uint8_t* mask) {
     fluid_ = double(fluid);
 }
 
+namespace {
+std::atomic<int> g_fpcg_sweeps{2};
+std::atomic<float> g_fpcg_omega{1.0f};
+}  // namespace
+
+FpcgSmoothing fpcg_smoothing() { return {g_fpcg_sweeps.load(), g_fpcg_omega.load()}; }
+
+void set_fpcg_smoothing(int sweeps, float omega) {
+    if (sweeps < 1 || sweeps > 8 || !(omega > 0.0f && omega < 2.0f))
+        fail(VAPOR_INVALID_ARGUMENT, "FPCG smoothing: 1..8 sweeps and 0 < omega < 2");
+    g_fpcg_sweeps.store(sweeps);
+    g_fpcg_omega.store(omega);
+}
+
 void Workspace::ensure_fpcg(bool coarse) {
     const size_t count = rb_count(n_);
     for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_, &cg_z2_})
@@ -334,7 +349,7 @@ void Workspace::ensure_fpcg(bool coarse) {
 // Flexible PCG on the error equation with FP64 re-centring (x64 += e,
 // r = float(b - A x64), e = 0) whenever the FP32 recurrence residual reaches
 // the target or drops by kRecentreDrop; stops when the FP64 residual meets
-// the target. Preconditioner: kFpcgSmoothing red-black Gauss-Seidel sweeps,
+// the target. Preconditioner: fpcg_smoothing() red-black relaxation sweeps,
 // the coarse-grid correction when `coarse` is given, then the same sweeps in
 // reverse colour order. Iterations count CG steps.
 void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UNet* coarse, LoopCond cond,
@@ -345,10 +360,12 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     const size_t count = rb_count(n_);
     float* e = p_.p;
     float* r = r32_.p;
-    const ProjectionArgs smooth{a.g, a.dt, 1.0f, 0.0f, a.options};
+    const FpcgSmoothing sm = fpcg_smoothing();
+    const int sweeps = sm.sweeps;
+    const ProjectionArgs smooth{a.g, a.dt, sm.omega, 0.0f, a.options};
     // the smoothing pairs run as one temporally blocked launch each when the
     // grid allows (same bits as the one-colour launches)
-    const bool blocked = sor_block_iterations(n_) == 2 && kFpcgSmoothing == 2;
+    const bool blocked = sor_block_iterations(n_) == 2 && sweeps == 2;
     // z after pre-smoothing and the coarse correction: the twin buffer when
     // blocked (the post-smoothing launch is out of place), else z itself
     float* zpre = blocked ? cg_z2_.p : cg_z_.p;
@@ -363,19 +380,19 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         if (blocked) {
             // both sweeps in one launch, starting from z = 0 (no iterate is
             // read), into the pre-smoothed twin z2
-            launch_sor_blocked(smooth, kFpcgSmoothing, 0, zpre, zpre, r, ctrl_, false, 0, false, st, false, false,
+            launch_sor_blocked(smooth, sweeps, 0, zpre, zpre, r, ctrl_, false, 0, false, st, false, false,
                                true);
             t.end(VAPOR_PHASE_SOR, 1);
         } else {
             // the first colour sweep starts from z = 0 (and clears the other colour)
             const bool fused_start = sor_fuses_measure(n_);
             if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
-            for (int j = 0; j < kFpcgSmoothing; ++j) {
+            for (int j = 0; j < sweeps; ++j) {
                 launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false,
                                  fused_start && j == 0);
                 launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
             }
-            t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
+            t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         }
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
@@ -390,14 +407,14 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         }
         t.begin(VAPOR_PHASE_SOR);
         if (blocked) {
-            launch_sor_blocked(smooth, kFpcgSmoothing, 1, zpre, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            launch_sor_blocked(smooth, sweeps, 1, zpre, cg_z_.p, r, ctrl_, false, 0, false, st, false);
             t.end(VAPOR_PHASE_SOR, 1);
         } else {
-            for (int j = 0; j < kFpcgSmoothing; ++j) {
+            for (int j = 0; j < sweeps; ++j) {
                 launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
                 launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
             }
-            t.end(VAPOR_PHASE_SOR, 2 * kFpcgSmoothing);
+            t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         }
     };
     auto recentre_group = [&](cudaStream_t st) {

@@ -81,9 +81,15 @@ private:
     vapor_phase_timings acc_{};
 };
 
-// Red-black Gauss-Seidel sweeps before (and, in reverse colour order, after)
-// the coarse correction in the FPCG preconditioner.
-constexpr int kFpcgSmoothing = 2;
+// Red-black relaxation sweeps before (and, in reverse colour order, after)
+// the coarse correction in the FPCG preconditioner, and their weight
+// (1: Gauss-Seidel). Process-wide; read when a projection is recorded.
+struct FpcgSmoothing {
+    int sweeps;
+    float omega;
+};
+FpcgSmoothing fpcg_smoothing();
+void set_fpcg_smoothing(int sweeps, float omega);
 
 // Validation shared by every entry point (MacGridDomain3D.cpp:7-22).
 void validate_grid(int n, float box);

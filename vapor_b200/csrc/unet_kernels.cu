@@ -686,11 +686,11 @@ __global__ void __launch_bounds__(256) k_conv3_zn(ConvArgs a, int zt, int ring) 
         }
     };
     // group 0: the weights and input planes 0, 1; then one group per plane
-    // ahead (planes 2 .. ring - 2)
+    // until every slot is filled (planes 2 .. ring - 1)
     load_plane(0);
     load_plane(1);
     tc::cp_async_commit();
-    for (int q = 2; q <= ring - 2; ++q) {
+    for (int q = 2; q <= ring - 1; ++q) {
         if (q < inputs) load_plane(q);
         tc::cp_async_commit();
     }
@@ -706,7 +706,7 @@ __global__ void __launch_bounds__(256) k_conv3_zn(ConvArgs a, int zt, int ring) 
         for (uint32_t c = 0; c < half_cols; c += 8)
             tc::tmem_st8(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(warp >> 2) * half_cols + c, zero);
     }
-    tc::cp_async_wait_group<0>();  // the weights and the first ring - 1 planes have landed
+    tc::cp_async_wait_group<0>();  // the weights and the first ring planes have landed
     tc::fence_proxy_async();
     tc::tc_fence_before();
     __syncthreads();
@@ -746,8 +746,9 @@ __global__ void __launch_bounds__(256) k_conv3_zn(ConvArgs a, int zt, int ring) 
         // input plane q has landed (its group and all earlier ones)
         if (q >= 2) {
             // plane q + ring - 2 goes into the slot of plane q - 2, whose MMAs
-            // completed (waited for in step q - 1); plane q was requested in
-            // step q - ring + 2, so all but the ring - 2 newest groups must land
+            // completed (waited for in step q - 1); plane q >= ring was
+            // requested in step q - ring + 2 (planes below ring were all in
+            // the first groups), so all but the ring - 2 newest groups must land
             if (q + ring - 2 < inputs) load_plane(q + ring - 2);
             tc::cp_async_commit();
             if (ring == 6) tc::cp_async_wait_group<4>();

@@ -35,7 +35,7 @@ import time
 
 import numpy as np
 
-from . import MacSimulation3D, StageBackend, check, default_params, library
+from . import MacSimulation3D, StageBackend, check, default_params, fpcg_sweeps_per_application, library
 from .abi import SOLVER_FPCG, SOLVER_MIXED_REFINEMENT, LinearSolveOptions, ProjectionOptions
 from .plume import DT, omega_for, scene_params, spectral_fields, swirl_fields, training_scene
 
@@ -320,9 +320,10 @@ def compare_fpcg(net, n=256, warmup=4, steps=3, seed=2024, rel=1e-6, phases=Fals
             out[name]["phase_launches"] = {k: v["launches"] for k, v in t.items() if v["launches"] > 0}
             sim.set_timing(False)
         if kind == SOLVER_FPCG:
-            # each CG step applies the preconditioner once (4 colour-pair sweeps),
-            # plus one application per projection before the loop (2 per step)
-            out[name]["sweeps_per_step"] = 4 * (its + 2)
+            # each CG step applies the preconditioner once (2 x smoothing
+            # red+black sweeps), plus one application per projection before
+            # the loop (2 per step)
+            out[name]["sweeps_per_step"] = fpcg_sweeps_per_application() * (its + 2)
         else:
             out[name]["sweeps_per_step"] = its
         sim.close()
