@@ -406,16 +406,18 @@ vapor_status vapor_tune_sor_blocking(int32_t iterations_per_launch);
  * automatic: one wave of resident CTAs). Results do not depend on it. */
 vapor_status vapor_tune_sor_blocked_chunks(int32_t n, int32_t chunks);
 /* Tuning (extension): the tcgen05 kernel of the learned network's 3x3x3
- * convolutions whose weights fit in shared memory. 0 (default): the
+ * convolutions whose weights fit in shared memory. 0: the
  * block-synchronous z-march (27 MMAs of width cout per output plane); 1: its
  * warp-specialised form (producer, MMA and epilogue warps on mbarriers; same
  * results); 2: the plane-window form (9 MMAs of width 3 cout per input
  * plane, three output planes per MMA; same results for 16 input channels,
- * FP32-rounding differences for more). */
+ * FP32-rounding differences for more); 3 (default): the plane-window form
+ * fed by the TMA unit (weights in one bulk copy, input planes as tensor-map
+ * boxes; the same results as 2; grids narrower than 10 x 18 voxels run 0). */
 vapor_status vapor_tune_conv_kernel(int32_t kind);
 /* Tuning (extension): the FPCG preconditioner's relaxation sweeps before and
  * after the coarse correction (1..8, default 2) and their weight (0 < omega
- * < 2, default 1: symmetric Gauss-Seidel). Changes the iteration count, not
+ * < 2, default 1.2; 1 is symmetric Gauss-Seidel). Changes the iteration count, not
  * the accepted answer (the stopping test is the FP64 residual). Process-wide;
  * set it before recording steps. */
 vapor_status vapor_tune_fpcg_smoothing(int32_t sweeps, float omega);

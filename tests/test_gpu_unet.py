@@ -151,7 +151,7 @@ def test_warp_specialised_convolutions_equal_block_synchronous(n):
             outs.append(out.cpu().numpy())
             grads.append(gp)
     finally:
-        vb.tune_conv_kernel(0)
+        vb.tune_conv_kernel(vb.DEFAULT_CONV_KERNEL)
     assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
     assert np.abs(grads[0] - grads[1]).max() <= 1e-4 * np.abs(grads[0]).max()
 
@@ -179,16 +179,47 @@ def test_plane_window_convolutions_match_torch_reference(n):
         assert err < 2e-2, err
         # against the block-synchronous kernel: the same network up to FP32
         # rounding of the multi-chunk layers, carried through BF16 storage
-        vb.tune_conv_kernel(0)
+        vb.tune_conv_kernel(vb.DEFAULT_CONV_KERNEL)
         out0 = torch.zeros_like(out)
         vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out0.data_ptr()))
         d = (out - out0).abs().max().item() / max(1e-6, out0.abs().max().item())
         assert d < 1e-2, d
     finally:
-        vb.tune_conv_kernel(0)
+        vb.tune_conv_kernel(vb.DEFAULT_CONV_KERNEL)
 
 
-@pytest.mark.parametrize("ws", [0, 1, 2])
+@pytest.mark.parametrize("n", [32, 64])
+def test_tma_plane_window_convolutions_match_torch_reference(n):
+    """The TMA-fed plane-window kernel (kind 3: packed weights in one bulk
+    copy, input planes as tensor-map boxes, no block barrier in the march)
+    against the PyTorch FP32 reference at the bar of the other kernels, and
+    against the cp.async plane-window kernel (kind 2), whose MMAs it repeats
+    operand for operand on the grids of at least 10 x 18 voxels (64^3 and
+    32^3 here); on the smaller grids it runs the z-march, whose multi-chunk
+    layers round differently in FP32."""
+    import torch
+    net = Net(seed=17)
+    p = net.params()
+    x = features(n, 23)
+    xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+    outs = []
+    try:
+        for kind in (2, 3):
+            vb.tune_conv_kernel(kind)
+            out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+            vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+            outs.append(out.cpu().numpy())
+    finally:
+        vb.tune_conv_kernel(vb.DEFAULT_CONV_KERNEL)
+    ref, *_ = torch_reference(p, xin.float().cpu().numpy())
+    ref = ref.detach().numpy().reshape(-1)
+    err = np.abs(outs[1] - ref).max() / max(1e-6, np.abs(ref).max())
+    assert err < 2e-2, err
+    d = np.abs(outs[1] - outs[0]).max() / max(1e-6, np.abs(outs[0]).max())
+    assert d < 1e-2, d
+
+
+@pytest.mark.parametrize("ws", [0, 1, 2, 3])
 def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     """The convolutions' completion waits poll an mbarrier with an iteration
     limit. With the test hook they poll one that nothing completes, run out,
@@ -198,7 +229,7 @@ def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     import torch
     vb.tune_conv_kernel(ws)
     net = Net(seed=5)
-    n = 8
+    n = 32 if ws == 3 else 8  # the TMA-fed kernel runs on grids of 18 voxels or more
     xin = torch.tensor(features(n, 9)).to(torch.bfloat16).cuda().contiguous()
     before = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
     vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), before.data_ptr()))
@@ -211,7 +242,7 @@ def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
     vb.check(net.lib.vapor_unet_set_wait_probe(net.h, 0))
     after = torch.zeros_like(before)
     vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), after.data_ptr()))
-    vb.tune_conv_kernel(0)
+    vb.tune_conv_kernel(vb.DEFAULT_CONV_KERNEL)
     assert torch.equal(after, before)
 
 

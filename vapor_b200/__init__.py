@@ -374,17 +374,24 @@ def tune_sor_blocking(iterations_per_launch):
     check(library().vapor_tune_sor_blocking(int(iterations_per_launch)))
 
 
+# Convolution kernel and FPCG smoothing the library starts with (the measured
+# fastest on the 256^3 benchmark plume).
+DEFAULT_CONV_KERNEL = 3
+DEFAULT_FPCG_SMOOTHING = (2, 1.2)
+
+
 def tune_conv_kernel(kind):
-    """tcgen05 convolution kernel: 0 (default) block-synchronous z-march, 1
-    its warp-specialised form, 2 the plane-window form (three output planes
-    per MMA)."""
+    """tcgen05 convolution kernel: 0 block-synchronous z-march, 1 its
+    warp-specialised form, 2 the plane-window form (three output planes per
+    MMA), 3 (default) the plane-window form fed by TMA (same results as 2;
+    grids under 10 x 18 voxels run 0)."""
     check(library().vapor_tune_conv_kernel(int(kind)))
 
 
-def tune_fpcg_smoothing(sweeps=2, omega=1.0):
+def tune_fpcg_smoothing(sweeps=DEFAULT_FPCG_SMOOTHING[0], omega=DEFAULT_FPCG_SMOOTHING[1]):
     """Relaxation sweeps before and after the FPCG preconditioner's coarse
-    correction (default 2) and their weight (default 1, Gauss-Seidel). Set it
-    before creating the simulations whose steps are recorded."""
+    correction (default 2) and their weight (default 1.2). Set it before
+    creating the simulations whose steps are recorded."""
     check(library().vapor_tune_fpcg_smoothing(int(sweeps), float(omega)))
 
 

@@ -332,7 +332,7 @@ VB_API vapor_status vapor_tune_sor_planes(int32_t n, int32_t planes) {
 
 VB_API vapor_status vapor_tune_conv_kernel(int32_t kind) {
     return guarded([&] {
-        require(kind >= 0 && kind <= 2, "0, 1 or 2");
+        require(kind >= 0 && kind <= 3, "0, 1, 2 or 3");
         vb::unet::set_conv_kernel(kind);
     });
 }

@@ -316,7 +316,7 @@ void Workspace::set_solid(const uint8_t* mask) {
 
 namespace {
 std::atomic<int> g_fpcg_sweeps{2};
-std::atomic<float> g_fpcg_omega{1.0f};
+std::atomic<float> g_fpcg_omega{1.2f};  // measured: 57 CG steps per 256^3 plume step against 59 at 1.0
 }  // namespace
 
 FpcgSmoothing fpcg_smoothing() { return {g_fpcg_sweeps.load(), g_fpcg_omega.load()}; }

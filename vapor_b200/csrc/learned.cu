@@ -30,6 +30,7 @@ UNet::UNet(cudaStream_t stream) : s_(stream), own_(stream) {
     m_.allocate(P);
     v_.allocate(P);
     wbf_.allocate(P);
+    wpack_.allocate(P);
     long maxw = 0;
     for (const auto& l : kLayers) maxw = std::max(maxw, 27L * l.cout * l.cin);
     wflip_.allocate(maxw);
@@ -68,6 +69,7 @@ void UNet::set_parameters(const float* host) {
     const long P = parameter_count();
     VB_CUDA(cudaMemcpyAsync(params_.p, host, P * sizeof(float), cudaMemcpyHostToDevice, s_));
     launch_to_bf16(P, params_.p, bf(wbf_), s_);
+    pack_weights();
     m_.zero(s_);
     v_.zero(s_);
     VB_CUDA(cudaStreamSynchronize(s_));
@@ -127,6 +129,14 @@ void UNet::ensure(int n) {
     gout_.release();
 }
 
+// The plane-window kernels' image of every layer's BF16 weights, at the
+// layers' offsets in wbf_ (refreshed whenever wbf_ changes).
+void UNet::pack_weights() {
+    for (int l = 0; l < kConvLayers; ++l)
+        launch_pack_window(kLayers[l].cout, kLayers[l].cin, bf(wbf_) + weight_offset(l), bf(wpack_) + weight_offset(l),
+                           s_);
+}
+
 void UNet::conv(int layer, int D, int H, int W, const __nv_bfloat16* in, int in_stride, void* out, int out_stride,
                 int out_offset, bool relu, bool fp32_out) {
     ConvArgs a{};
@@ -145,6 +155,7 @@ void UNet::conv(int layer, int D, int H, int W, const __nv_bfloat16* in, int in_
     a.relu = relu ? 1 : 0;
     a.error = error_.p;
     a.wait_probe = wait_probe_;
+    a.w_window = bf(wpack_) + weight_offset(layer);
     launch_conv3(a, kLayers[layer].cout, s_);
 }
 
@@ -322,6 +333,7 @@ double UNet::train_step(int n, const float* b_split, const float* p_split, const
     backward(n);
     ++step_;
     launch_adam(parameter_count(), params_.p, m_.p, v_.p, grad_.p, bf(wbf_), lr, step_, s_);
+    pack_weights();
     VB_CUDA(cudaStreamSynchronize(s_));
     check_error();
     loss = loss_host_;

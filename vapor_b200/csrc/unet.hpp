@@ -37,6 +37,7 @@ struct ConvArgs {
     unsigned int* error;          // bit 1: a bounded wait timed out; bit 2: in-flight MMAs could not be drained
     int wait_probe;               // test hook: > 0 makes each CTA's first completion wait poll a barrier
                                   // that nothing completes, wait_probe times, so that it runs out
+    const __nv_bfloat16* w_window;  // w packed for the plane-window kernels (launch_pack_window), or null
 };
 
 struct WGradArgs {
@@ -54,8 +55,13 @@ void configure_conv_kernels();
 // Selects the kernel of every later convolution whose weights fit in shared
 // memory: 0 the block-synchronous z-march, 1 its warp-specialised form (same
 // results), 2 the plane-window form (same results with one input chunk,
-// FP32-rounding differences with several).
+// FP32-rounding differences with several), 3 the plane-window form fed by TMA
+// (the same MMAs as 2, so the same results; needs ConvArgs::w_window, else 2
+// runs).
 void set_conv_kernel(int kind);
+// Packs one layer's weights [27][cout][cin] into the shared-memory image of
+// the plane-window kernels (27 cout cin values).
+void launch_pack_window(int cout, int cin, const __nv_bfloat16* w, __nv_bfloat16* packed, cudaStream_t s);
 void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
 void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,
@@ -170,6 +176,7 @@ private:
     void ensure(int n);
     void forward(int n);
     void backward(int n);
+    void pack_weights();
     void conv(int layer, int D, int H, int W, const __nv_bfloat16* in, int in_stride, void* out, int out_stride,
               int out_offset, bool relu, bool fp32_out = false);
 
@@ -180,6 +187,7 @@ private:
     unsigned long long generation_ = 0;
     DevArray<float> params_, grad_, m_, v_;
     DevArray<uint16_t> wbf_;   // BF16 copy of the parameters
+    DevArray<uint16_t> wpack_;  // wbf_'s weights packed for the plane-window kernels (same offsets)
     DevArray<uint16_t> wflip_;  // flipped/transposed weights of one layer
     // activations (BF16, channels-last)
     DevArray<uint16_t> in0_, e1a_, dec1_, e2in_, e2a_, dec2_, e3in_, e3a_, e3b_, d2a_, d2b_, d1a_, d1b_;

@@ -11,6 +11,7 @@
 // gradients, pooling, upsampling, the 1x1 output head, the loss and Adam are
 // memory-bound or small and run on CUDA cores.
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -27,8 +28,9 @@ constexpr int kWaitLimit = 1 << 22;
 
 // Kernel for the convolutions whose weights fit in shared memory: 0 the
 // block-synchronous z-march, 1 its warp-specialised form, 2 the plane-window
-// form (three output planes per MMA).
-std::atomic<int> g_conv_kind{0};
+// form (three output planes per MMA), 3 (default) the plane-window form fed
+// by TMA.
+std::atomic<int> g_conv_kind{3};
 
 __device__ __forceinline__ void decode(long v, int H, int W, int& x, int& y, int& z) {
     x = int(v % W);
@@ -795,6 +797,209 @@ __global__ void __launch_bounds__(256) k_conv3_zn(ConvArgs a, int zt, int ring) 
     if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
+// The plane-window convolution fed by the TMA unit. The MMAs, their operands'
+// values and their order are those of k_conv3_zn; what changes is how the
+// operands reach shared memory and how the CTA synchronises:
+//   - the layer's weights arrive in one bulk copy from their packed image
+//     (launch_pack_window: the shared-memory layout of k_conv3_zn), and each
+//     input plane as 2 x chunks tensor-map boxes of 8 channels x 10 x 18
+//     voxels (zero outside the grid), each completing on the plane slot's
+//     `full` mbarrier. The A operand of chunk c sits at [half][y][x][16 B]:
+//     K halves 2944 bytes apart (LBO), 8-voxel rows 160 bytes apart (SBO);
+//   - thread 0 issues plane q's MMAs once its slot is full and commits them
+//     to cbar[q & 1]; every thread waits for the MMAs of plane q - 1, thread 0
+//     refills their slot with plane q - 1 + ring, and the epilogue of the
+//     output plane they completed runs. No block-wide barrier sits in the
+//     march, so warps 1-7 drain plane q - 2 while thread 0 issues plane q.
+// Every wait is bounded; a timeout sets the error flag and an abort flag that
+// ends the other threads' waits, and thread 0 drains its MMAs and copies
+// (bounded) before TMEM is freed and the CTA exits.
+template <int N>
+struct ConvTma {
+    static constexpr int kHalf = 2944;           // one K half of a chunk's plane: 18 x 10 x 16 B, 128-byte padded
+    static constexpr int kChunk = 2 * kHalf;     // one chunk of one plane
+    static constexpr uint32_t kBox = 8 * 10 * 18 * 2;  // bytes of one box
+    static constexpr int kMaxRing = 6;
+    static int smem(int cin, int ring) { return 27 * N * cin * 2 + ring * (cin / 16) * kChunk + 1024; }
+    static bool fits(int cin, int ring, int zt) {
+        return ConvWindow<N>::kSupported && smem(cin, ring) <= 200 * 1024 && ConvWindow<N>::cols(zt) <= 512;
+    }
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_conv3_zt(const __grid_constant__ CUtensorMap in_map, ConvArgs a, int zt,
+                                                  int ring) {
+    using Wd = ConvWindow<N>;
+    using Tm = ConvTma<N>;
+    constexpr int NW = 3 * N;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bars[Tm::kMaxRing + 4];  // full[ring], weights, cbar[2], probe
+    __shared__ uint32_t tmem_slot;
+    __shared__ float s_bias[N];
+    __shared__ volatile int s_abort;
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16;
+    const int z0 = blockIdx.z * zt, z1 = min(a.D, z0 + zt);
+    const int inputs = z1 - z0 + 2;  // input planes z0 - 1 .. z1
+    const int chunks = a.cin / 16;
+    const uint32_t ncols = Wd::cols(zt);
+    const uint32_t wbytes = uint32_t(27 * N * a.cin * 2);
+    const uint32_t wbase = tc::smem_addr(smem);
+    const uint32_t rbase = wbase + wbytes;
+    const uint32_t plane_bytes = uint32_t(chunks * Tm::kChunk);
+    const uint32_t full0 = tc::smem_addr(&bars[0]);  // slot r's barrier at full0 + 8 r
+    const uint32_t wbar = tc::smem_addr(&bars[Tm::kMaxRing]);
+    const uint32_t cbar0 = wbar + 8;                 // commits of input planes alternate cbar0, cbar0 + 8
+    const uint32_t probe = wbar + 24;                // never arrived on (timeout test hook)
+    const uint32_t tx_plane = uint32_t(chunks * 2) * Tm::kBox;
+
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), ncols);
+    if (tid == 0) {
+        for (int r = 0; r < ring; ++r) tc::mbar_init(full0 + 8u * r, 1);
+        tc::mbar_init(wbar, 1);
+        tc::mbar_init(cbar0, 1);
+        tc::mbar_init(cbar0 + 8, 1);
+        tc::mbar_init(probe, 1);
+        tc::fence_mbarrier_init();
+        s_abort = 0;
+    }
+    for (int i = tid; i < N; i += blockDim.x) s_bias[i] = a.bias ? a.bias[i] : 0.f;
+    tc::tc_fence_before();
+    __syncthreads();  // barriers initialised, TMEM allocation visible
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    // input plane q (zz = z0 - 1 + q, all chunks, both K halves) into its
+    // slot (thread 0; fills counted per slot for the drain)
+    int filled[Tm::kMaxRing] = {0, 0, 0, 0, 0, 0};
+    auto load_plane = [&](int q) {
+        const uint32_t slot = rbase + uint32_t(q % ring) * plane_bytes;
+        const uint32_t bar = full0 + 8u * uint32_t(q % ring);
+        ++filled[q % ring];
+        tc::mbar_expect_tx(bar, tx_plane);
+        for (int cc = 0; cc < chunks; ++cc)
+            for (int h = 0; h < 2; ++h)
+                tc::tma_load_4d(slot + uint32_t(cc * Tm::kChunk + h * Tm::kHalf), &in_map, cc * 16 + h * 8, x0 - 1,
+                                y0 - 1, z0 - 1 + q, bar);
+    };
+    if (tid == 0) {
+        tc::mbar_expect_tx(wbar, wbytes);
+        tc::bulk_load(wbase, a.w_window, wbytes, wbar);
+        for (int q = 0; q < min(ring, inputs); ++q) load_plane(q);
+    }
+    {
+        // clear the accumulator window (warp w: the lanes of quarter w & 3,
+        // the columns of half w >> 2)
+        const uint32_t zero[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        const uint32_t half_cols = ncols / 2;
+        for (uint32_t c = 0; c < half_cols; c += 8)
+            tc::tmem_st8(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(warp >> 2) * half_cols + c, zero);
+    }
+    tc::tc_fence_before();
+    __syncthreads();  // the cleared window precedes every MMA
+    tc::tc_fence_after();
+    constexpr uint32_t idesc = tc::instr_desc_bf16(128, NW);
+    const uint64_t a_desc = tc::smem_desc(rbase, Tm::kHalf, 160);
+    const uint64_t b_desc = tc::smem_desc(wbase, 128, 256);
+    auto col_of = [&](int z) { return uint32_t(N * (z1 + 1 - z)); };  // output plane z's first column
+    int commits = 0;     // MMA commits issued (thread 0)
+    bool ok = true;
+    auto fail_wait = [&]() {
+        s_abort = 1;
+        atomicOr(a.error, 1u);
+        ok = false;
+    };
+    for (int q = 0; q < inputs && ok; ++q) {
+        if (tid == 0) {
+            bool ready = q > 0 || tc::mbar_wait_or_abort(wbar, 0u, kWaitLimit, &s_abort);
+            ready = ready && tc::mbar_wait_or_abort(full0 + 8u * uint32_t(q % ring), uint32_t(q / ring) & 1u,
+                                                    kWaitLimit, &s_abort);
+            if (!ready) {
+                fail_wait();
+            } else {
+                tc::tc_fence_after();
+                const int zi = z0 - 1 + q;
+                if (zi >= 0 && zi < a.D) {  // planes outside the grid are zero and add nothing
+                    const uint32_t d = tmem + col_of(zi + 1);
+                    const uint64_t ad = a_desc + (uint32_t(q % ring) * plane_bytes >> 4);
+#pragma unroll 1
+                    for (int cc = 0; cc < chunks; ++cc)
+#pragma unroll
+                        for (int s = 0; s < 9; ++s) {
+                            const int dy = s / 3, dx = s - 3 * dy;
+                            tc::mma_bf16(d, ad + uint32_t(cc * (Tm::kChunk >> 4)) + uint32_t((dy * 160 + dx * 16) >> 4),
+                                         b_desc + uint32_t((cc * 9 + s) * NW * 2), idesc, true);
+                        }
+                }
+                tc::mma_commit(cbar0 + uint32_t(8 * (q & 1)));
+                ++commits;
+            }
+        }
+        if (q >= 1 && ok && !s_abort) {
+            // MMAs of input plane q - 1 complete: output plane zi(q) - 2 has
+            // all its contributions and slot (q - 1) % ring is free
+            const int p = q - 1;
+            const bool done = a.wait_probe
+                                  ? tc::mbar_wait_or_abort(probe, 0u, a.wait_probe, &s_abort)
+                                  : tc::mbar_wait_or_abort(cbar0 + uint32_t(8 * (p & 1)), uint32_t(p >> 1) & 1u,
+                                                           kWaitLimit, &s_abort);
+            if (!done) {
+                fail_wait();
+            } else {
+                tc::tc_fence_after();
+                if (tid == 0 && p + ring < inputs) load_plane(p + ring);
+                const int zo = z0 - 1 + q - 2;
+                if (zo >= z0 && zo < z1) conv_epilogue<N>(a, tmem + col_of(zo), s_bias, x0, y0, zo, warp, lane);
+            }
+        }
+        if (s_abort) ok = false;
+    }
+    if (ok) {
+        // the last input plane's MMAs: output plane z1 - 1
+        const int p = inputs - 1;
+        if (!tc::mbar_wait_or_abort(cbar0 + uint32_t(8 * (p & 1)), uint32_t(p >> 1) & 1u, kWaitLimit, &s_abort)) {
+            fail_wait();
+        } else {
+            tc::tc_fence_after();
+            const int zo = z1 - 1;
+            if (zo >= z0) conv_epilogue<N>(a, tmem + col_of(zo), s_bias, x0, y0, zo, warp, lane);
+        }
+    }
+    __syncthreads();
+    if (s_abort && tid == 0) {
+        // drain (bounded): the last commit covers every MMA issued before it,
+        // and every slot's latest fill must land before the CTA exits
+        bool drained = true;
+        if (commits > 0)
+            drained &= tc::mbar_wait(cbar0 + uint32_t(8 * ((commits - 1) & 1)), uint32_t((commits - 1) >> 1) & 1u,
+                                     kWaitLimit);
+        drained &= tc::mbar_wait(wbar, 0u, kWaitLimit);
+        for (int r = 0; r < ring; ++r)  // the f-th fill of a slot completes its phase f - 1
+            if (filled[r] > 0)
+                drained &= tc::mbar_wait(full0 + 8u * uint32_t(r), uint32_t(filled[r] - 1) & 1u, kWaitLimit);
+        if (!drained) atomicOr(a.error, 2u);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+// Packs [27][cout][cin] weights into k_conv3_zn's shared-memory image: B rows
+// (j, co) = tap j * 9 + s, co, as [chunk][s][3 cout / 8][2][8][16 B].
+__global__ void k_pack_window(int cout, int cin, const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ out) {
+    const int NW = 3 * cout;
+    const long pieces = 27L * cout * cin / 8;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < pieces; i += long(gridDim.x) * blockDim.x) {
+        const int half = int(i & 1), row = int((i >> 1) % NW);
+        const long cs = (i >> 1) / NW;  // chunk * 9 + s
+        const int j = row / cout, co = row - j * cout, sidx = int(cs % 9), cc = int(cs / 9);
+        const int t = j * 9 + sidx;
+        const uint4 v = *reinterpret_cast<const uint4*>(w + (long(t) * cout + co) * cin + cc * 16 + half * 8);
+        const long byte = cs * NW * 32 + (row >> 3) * 256 + half * 128 + (row & 7) * 16;
+        *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(out) + byte) = v;
+    }
+}
+
 // ---- CUDA-core kernels -------------------------------------------------------
 
 // Input features: channel 0 = b / scale (from the solver's red-black split RHS,
@@ -1267,8 +1472,42 @@ void configure_n() {
                                  ConvTile<N>::kSmemMax));
     VB_CUDA(cudaFuncSetAttribute(k_conv3_zm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     VB_CUDA(cudaFuncSetAttribute(k_conv3_ws<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    if constexpr (ConvWindow<N>::kSupported)
+    if constexpr (ConvWindow<N>::kSupported) {
         VB_CUDA(cudaFuncSetAttribute(k_conv3_zn<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        VB_CUDA(cudaFuncSetAttribute(k_conv3_zt<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    }
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q);
+        return (e == cudaSuccess && q == cudaDriverEntryPointSuccess)
+                   ? reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f)
+                   : nullptr;
+    }();
+    if (!fn) fail(VAPOR_RUNTIME_ERROR, "cuTensorMapEncodeTiled is not available from the CUDA driver");
+    return fn;
+}
+
+// 4D map (channel, x, y, z) over a channels-last BF16 activation with
+// in_stride channels per voxel; box = 8 channels x 10 x 18 x 1 (one K half of
+// one 16-channel chunk of a halo plane).
+CUtensorMap activation_map(const ConvArgs& a) {
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {cuuint64_t(a.in_stride), cuuint64_t(a.W), cuuint64_t(a.H), cuuint64_t(a.D)};
+    const cuuint64_t row = cuuint64_t(a.in_stride) * 2;
+    const cuuint64_t strides[3] = {row, row * cuuint64_t(a.W), row * cuuint64_t(a.W) * cuuint64_t(a.H)};
+    const cuuint32_t box[4] = {8, 10, 18, 1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(a.in),
+                                            dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(VAPOR_RUNTIME_ERROR, "cuTensorMapEncodeTiled failed for a convolution input");
+    return map;
 }
 
 // Resident CTAs per SM of the warp-specialised convolution: shared memory,
@@ -1289,7 +1528,37 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
     const int kind = g_conv_kind.load();
     bool done = false;
     if constexpr (ConvWindow<N>::kSupported) {
-        if (kind == 2 && ConvWindow<N>::fits(a.cin, 4, 2)) {
+        // the TMA-fed form: packed weights, a 16-byte aligned input, and a
+        // grid at least as wide as the 10 x 18 box
+        const bool tma = kind == 3 && a.w_window != nullptr && ConvTma<N>::fits(a.cin, 3, 2) && a.W >= 10 &&
+                         a.H >= 18 && (reinterpret_cast<uintptr_t>(a.in) & 15) == 0;
+        if (tma) {
+            // planes per CTA and ring depth: the pair that minimises waves x
+            // (planes + 2), the input planes a CTA multiplies; resident CTAs
+            // by shared memory and by TMEM columns (512 per SM); on ties the
+            // deeper ring
+            const int sms = device_sm_count();
+            int best = 2, best_ring = 3;
+            long best_cost = -1;
+            for (int ring : {6, 4, 3})
+                for (int zt : {2, 4, 6, 8, 12, 16}) {
+                    if (!ConvTma<N>::fits(a.cin, ring, zt)) continue;
+                    const int by_smem = std::max(1, (228 * 1024) / (ConvTma<N>::smem(a.cin, ring) + 1536));
+                    const int by_tmem = int(512 / ConvWindow<N>::cols(zt));
+                    const long slots = long(std::max(1, std::min({by_smem, by_tmem, 8}))) * sms;
+                    const long ctas = long(gx) * gy * ((a.D + zt - 1) / zt);
+                    const long cost = ((ctas + slots - 1) / slots) * (std::min(zt, a.D) + 2);
+                    if (best_cost < 0 || cost < best_cost) {
+                        best_cost = cost;
+                        best = zt;
+                        best_ring = ring;
+                    }
+                }
+            const CUtensorMap map = activation_map(a);
+            const dim3 grid(gx, gy, unsigned((a.D + best - 1) / best));
+            k_conv3_zt<N><<<grid, 256, ConvTma<N>::smem(a.cin, best_ring), s>>>(map, a, best, best_ring);
+            done = true;
+        } else if (kind == 2 && ConvWindow<N>::fits(a.cin, 4, 2)) {
         // planes per CTA: the count that minimises waves x (planes + 2), the
         // input planes a CTA multiplies; resident CTAs by shared memory and
         // by TMEM columns (512 per SM)
@@ -1350,7 +1619,7 @@ void launch_conv_n(const ConvArgs& a, cudaStream_t s) {
 }  // namespace
 
 void set_conv_kernel(int kind) {
-    if (kind < 0 || kind > 2) fail(VAPOR_INVALID_ARGUMENT, "convolution kernel: 0, 1 or 2");
+    if (kind < 0 || kind > 3) fail(VAPOR_INVALID_ARGUMENT, "convolution kernel: 0, 1, 2 or 3");
     g_conv_kind.store(kind);
 }
 
@@ -1360,6 +1629,11 @@ void configure_conv_kernels() {
     configure_n<48>();
     configure_n<64>();
     configure_n<96>();
+}
+
+void launch_pack_window(int cout, int cin, const __nv_bfloat16* w, __nv_bfloat16* packed, cudaStream_t s) {
+    count_launch();
+    k_pack_window<<<blocks_for(27L * cout * cin / 8), 256, 0, s>>>(cout, cin, w, packed);
 }
 
 void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s) {
