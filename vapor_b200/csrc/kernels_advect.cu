@@ -56,16 +56,17 @@ __device__ __forceinline__ void forward_point(const Grid& g, float ih, float dt,
                                               float* const* vel_out = nullptr) {
     float px, py, pz;
     position<LOC>(x, y, z, g.h, px, py, pz);
-    const Vel vel = velocity_at<POW2>(u, v, w, g.n, g.h, px, py, pz, ih);
+    const Vel vel = POW2 ? velocity_at_node<LOC>(u, v, w, g.n, x, y, z)
+                         : velocity_at<POW2>(u, v, w, g.n, g.h, px, py, pz, ih);
+    const int i = int(index_of(g.n, LOC, x, y, z));
     if (vel_out) {
-        const size_t i = index_of(g.n, LOC, x, y, z);
         vel_out[0][i] = vel.x;
         vel_out[1][i] = vel.y;
         vel_out[2][i] = vel.z;
     }
     const float qx = px - vel.x * dt, qy = py - vel.y * dt, qz = pz - vel.z * dt;
     const float value = sample<LOC, POW2>(src, g.n, g.h, qx, qy, qz, ih);
-    out[index_of(g.n, LOC, x, y, z)] = value * post_scale;
+    out[i] = value * post_scale;
 }
 
 template <int LOC, bool POW2>
@@ -77,7 +78,7 @@ __device__ __forceinline__ void maccormack_point(const Grid& g, float ih, float 
                                                  float* const* vel_in = nullptr) {
     const int n = g.n;
     const float h = g.h, box = g.box;
-    const size_t i = index_of(n, LOC, x, y, z);
+    const int i = int(index_of(n, LOC, x, y, z));
     float px, py, pz;
     position<LOC>(x, y, z, h, px, py, pz);
     Vel vel;
@@ -86,7 +87,7 @@ __device__ __forceinline__ void maccormack_point(const Grid& g, float ih, float 
         vel.y = __ldg(vel_in[1] + i);
         vel.z = __ldg(vel_in[2] + i);
     } else {
-        vel = velocity_at<POW2>(u, v, w, n, h, px, py, pz, ih);
+        vel = POW2 ? velocity_at_node<LOC>(u, v, w, n, x, y, z) : velocity_at<POW2>(u, v, w, n, h, px, py, pz, ih);
     }
     const float fx = px - vel.x * dt, fy = py - vel.y * dt, fz = pz - vel.z * dt;
     const float bx = px + vel.x * dt, by = py + vel.y * dt, bz = pz + vel.z * dt;
@@ -105,12 +106,14 @@ __device__ __forceinline__ void maccormack_point(const Grid& g, float ih, float 
         const int gy = donor<LOC == FACE_Y, POW2>(fy, h, ih, n);
         const int gz = donor<LOC == FACE_Z, POW2>(fz, h, ih, n);
         const int x1 = min(gx + 1, ex - 1), y1 = min(gy + 1, ey - 1), z1 = min(gz + 1, ez - 1);
-        const float s000 = __ldg(src + index_of(n, LOC, gx, gy, gz));
+        // row offsets of the donor cube (32-bit: fields hold < 2^31 values)
+        const int r00 = ex * (gy + ey * gz), r10 = ex * (y1 + ey * gz);
+        const int r01 = ex * (gy + ey * z1), r11 = ex * (y1 + ey * z1);
+        const float s000 = __ldg(src + (r00 + gx));
         float lo = s000, hi = s000;
-        const float s[7] = {__ldg(src + index_of(n, LOC, x1, gy, gz)), __ldg(src + index_of(n, LOC, gx, y1, gz)),
-                            __ldg(src + index_of(n, LOC, x1, y1, gz)), __ldg(src + index_of(n, LOC, gx, gy, z1)),
-                            __ldg(src + index_of(n, LOC, x1, gy, z1)), __ldg(src + index_of(n, LOC, gx, y1, z1)),
-                            __ldg(src + index_of(n, LOC, x1, y1, z1))};
+        const float s[7] = {__ldg(src + (r00 + x1)), __ldg(src + (r10 + gx)), __ldg(src + (r10 + x1)),
+                            __ldg(src + (r01 + gx)), __ldg(src + (r01 + x1)), __ldg(src + (r11 + gx)),
+                            __ldg(src + (r11 + x1))};
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
             lo = minf_ref(lo, s[k]);

@@ -91,6 +91,22 @@ __device__ __forceinline__ float trilinear(float f000, float f100, float f010, f
     return s;
 }
 
+// Trilinear lookup of a field at location LOC from the three axes' brackets,
+// with the reference's fixed 8-term order and left-to-right products. Offsets
+// are 32-bit: every field of a valid grid has fewer than 2^31 values.
+template <int LOC>
+__device__ __forceinline__ float sample_at(const float* __restrict__ f, int n, const Bracket& bx, const Bracket& by,
+                                           const Bracket& bz) {
+    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
+    const int r00 = ex * (by.i0 + ey * bz.i0);
+    const int r10 = ex * (by.i1 + ey * bz.i0);
+    const int r01 = ex * (by.i0 + ey * bz.i1);
+    const int r11 = ex * (by.i1 + ey * bz.i1);
+    return trilinear(__ldg(f + (r00 + bx.i0)), __ldg(f + (r00 + bx.i1)), __ldg(f + (r10 + bx.i0)),
+                     __ldg(f + (r10 + bx.i1)), __ldg(f + (r01 + bx.i0)), __ldg(f + (r01 + bx.i1)),
+                     __ldg(f + (r11 + bx.i0)), __ldg(f + (r11 + bx.i1)), bx.t, by.t, bz.t);
+}
+
 // Trilinear sample of a field at location LOC, world position (px,py,pz), with
 // the reference's fixed 8-term order and left-to-right products.
 template <int LOC, bool POW2 = false>
@@ -99,14 +115,7 @@ __device__ __forceinline__ float sample(const float* __restrict__ f, int n, floa
     const Bracket bx = bracket<LOC == FACE_X, POW2>(px, h, n, ih);
     const Bracket by = bracket<LOC == FACE_Y, POW2>(py, h, n, ih);
     const Bracket bz = bracket<LOC == FACE_Z, POW2>(pz, h, n, ih);
-    const int ex = n + (LOC == FACE_X), ey = n + (LOC == FACE_Y);
-    const size_t r00 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i0));
-    const size_t r10 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i0));
-    const size_t r01 = size_t(ex) * (size_t(by.i0) + size_t(ey) * size_t(bz.i1));
-    const size_t r11 = size_t(ex) * (size_t(by.i1) + size_t(ey) * size_t(bz.i1));
-    return trilinear(__ldg(f + r00 + bx.i0), __ldg(f + r00 + bx.i1), __ldg(f + r10 + bx.i0),
-                     __ldg(f + r10 + bx.i1), __ldg(f + r01 + bx.i0), __ldg(f + r01 + bx.i1),
-                     __ldg(f + r11 + bx.i0), __ldg(f + r11 + bx.i1), bx.t, by.t, bz.t);
+    return sample_at<LOC>(f, n, bx, by, bz);
 }
 
 // Red-black split storage of the projection's cell arrays (b, p, e, r32,
@@ -134,15 +143,58 @@ struct Vel {
     float x, y, z;
 };
 
-// MacGridSampler3D::velocity (MacGridSampler3D.cpp:73-75).
+// MacGridSampler3D::velocity (MacGridSampler3D.cpp:73-75). The three
+// components share their brackets: per axis one staggered (the component
+// along it) and one centred (the other two).
 template <bool POW2 = false>
 __device__ __forceinline__ Vel velocity_at(const float* __restrict__ u, const float* __restrict__ v,
                                            const float* __restrict__ w, int n, float h, float px, float py,
                                            float pz, float ih = 0.f) {
+    const Bracket sx = bracket<true, POW2>(px, h, n, ih), cx = bracket<false, POW2>(px, h, n, ih);
+    const Bracket sy = bracket<true, POW2>(py, h, n, ih), cy = bracket<false, POW2>(py, h, n, ih);
+    const Bracket sz = bracket<true, POW2>(pz, h, n, ih), cz = bracket<false, POW2>(pz, h, n, ih);
     Vel r;
-    r.x = sample<FACE_X, POW2>(u, n, h, px, py, pz, ih);
-    r.y = sample<FACE_Y, POW2>(v, n, h, px, py, pz, ih);
-    r.z = sample<FACE_Z, POW2>(w, n, h, px, py, pz, ih);
+    r.x = sample_at<FACE_X>(u, n, sx, cy, cz);
+    r.y = sample_at<FACE_Y>(v, n, cx, sy, cz);
+    r.z = sample_at<FACE_Z>(w, n, cx, cy, sz);
+    return r;
+}
+
+// The brackets of a grid coordinate g = k / 2 (k = 2 i at a staggered
+// position i h, 2 i + 1 at a centred one) when h is a power of two: the
+// position, its product with 1 / h and the 0.5 shift are then exact, so the
+// float brackets above reduce to this integer arithmetic, bit for bit.
+__device__ __forceinline__ Bracket bracket_half(int k, int n, bool staggered) {
+    Bracket b;
+    if (staggered) {
+        const int c = min(max(k, 0), 2 * n);  // clamp(g, 0, n)
+        b.i0 = min(c >> 1, n - 1);
+        b.i1 = b.i0 + 1;
+        b.t = 0.5f * float(c - 2 * b.i0);
+    } else {
+        const int c = min(max(k - 1, 0), 2 * (n - 1));  // clamp(g - .5, 0, n - 1)
+        b.i0 = c >> 1;
+        b.i1 = min(b.i0 + 1, n - 1);
+        b.t = 0.5f * float(c & 1);
+    }
+    return b;
+}
+
+// velocity_at at the sample point of location LOC's node (x, y, z), for a
+// power-of-two cell size: the same values from integer brackets.
+template <int LOC>
+__device__ __forceinline__ Vel velocity_at_node(const float* __restrict__ u, const float* __restrict__ v,
+                                                const float* __restrict__ w, int n, int x, int y, int z) {
+    const int kx = 2 * x + (LOC == FACE_X ? 0 : 1);
+    const int ky = 2 * y + (LOC == FACE_Y ? 0 : 1);
+    const int kz = 2 * z + (LOC == FACE_Z ? 0 : 1);
+    const Bracket sx = bracket_half(kx, n, true), cx = bracket_half(kx, n, false);
+    const Bracket sy = bracket_half(ky, n, true), cy = bracket_half(ky, n, false);
+    const Bracket sz = bracket_half(kz, n, true), cz = bracket_half(kz, n, false);
+    Vel r;
+    r.x = sample_at<FACE_X>(u, n, sx, cy, cz);
+    r.y = sample_at<FACE_Y>(v, n, cx, sy, cz);
+    r.z = sample_at<FACE_Z>(w, n, cx, cy, sz);
     return r;
 }
 
