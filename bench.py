@@ -311,6 +311,30 @@ def network_flops(nc):
     return 2.0 * macs
 
 
+# Algorithmic bytes per cell of one Reflection-MacCormack step by phase
+# (compulsory FP32 traffic, counted per pass): forcing = emit + buoyancy +
+# walls 12; advection = velocity with flow as source 24 + velocity with the
+# reflected field as source 36 + smoke with decay 20; divergence 16 per
+# projection; gradient 52 with the reflection + 28 without, plus the final
+# FP64 residual 8 per projection.
+PHASE_BYTES_PER_CELL = {"forcing": 12.0, "advect": 80.0, "rhs": 32.0, "gradient": 96.0}
+
+
+def phase_rooflines(phases, steps, cells, peak, peak_kind):
+    """HBM fraction of the memory-bound phases outside the solve: algorithmic
+    bytes per step over the phase's event time per step (launch gaps
+    included, so a lower bound on the kernels' own fractions)."""
+    out = {}
+    for name, per_cell in PHASE_BYTES_PER_CELL.items():
+        ms = phases.get(name, {}).get("ms", 0.0) / max(1, steps)
+        if ms <= 0:
+            continue
+        achieved = per_cell * cells / (ms * 1e-3) / 1e9
+        out[name] = {"bytes_per_cell": per_cell, "ms_per_step": ms, "achieved": achieved, "unit": "GB/s",
+                     "frac": achieved / peak, "peak": peak, "peak_kind": peak_kind}
+    return out
+
+
 def run_arm(vb, torch, args, n, fields, kind, net, dist, clocks=None):
     """Warm-up, then K timed steps (CUDA-graph replays) of one solver arm."""
     params = scene_params(vb.default_params(), n, args.rel, args.max_iterations, omega_for(n, args.omega),
@@ -504,6 +528,7 @@ def main():
                             "ms_per_application": coarse_ms,
                             "note": "time includes restriction, normalization, Galerkin scale and prolongation"},
         "phases_ms_per_step": {k: v["ms"] / roof_steps for k, v in phases.items() if v["ms"] > 0},
+        "phase_rooflines": phase_rooflines(phases, roof_steps, cells, peak, peak_kind),
         "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},
         "clocks": learned["clocks"], "wall_s": learned["wall_s"],

@@ -550,9 +550,9 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
     if (fpcg) {
         project_fpcg(a, warm, coarse, cond, handle);
         t.begin(VAPOR_PHASE_GRADIENT);
-        launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
-        if (ui) launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
-        t.end(VAPOR_PHASE_GRADIENT, 5);
+        const int finish = launch_finish_projection64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, ui, vi,
+                                                      wi, uo, vo, wo, uh, vh, wh, s);
+        t.end(VAPOR_PHASE_GRADIENT, finish);
     } else if (mixed) {
         // FP32 red-black sweeps on the error equation A e = r32. Every check
         // interval the FP32 residual of that equation decides whether to
@@ -602,9 +602,9 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
             }
         }
         t.begin(VAPOR_PHASE_GRADIENT);
-        launch_pressure_mean64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, s);
-        if (ui) launch_gradient64(a, ui, vi, wi, uo, vo, wo, uh, vh, wh, ctrl_, s);
-        t.end(VAPOR_PHASE_GRADIENT, 5);
+        const int finish = launch_finish_projection64(a, b_.p, p_.p, partials_.p, partial_capacity_, ctrl_, ui, vi,
+                                                      wi, uo, vo, wo, uh, vh, wh, s);
+        t.end(VAPOR_PHASE_GRADIENT, finish);
     } else {
         if (warm) warm->infer_into(n_, b_.p, ctrl_, p_.p, nullptr);  // x0 = network prediction
         if (o.fixed_iterations) {

@@ -200,14 +200,16 @@ void launch_check_gated(ProjControl* ctrl, LoopCond cond, cudaStream_t s);
 void launch_loop_condition(const ProjControl* ctrl, LoopCond cond, cudaStream_t s);
 void launch_zero_error_gated(const ProjectionArgs& a, float* e, const ProjControl* ctrl, cudaStream_t s);
 // Mixed precision epilogue: FP64 pressure mean, final FP64 residual, float
-// pressure copy (x64 - mean) into p32 with ctrl->p_mean_f = 0.
-void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
-                            int partial_capacity, ProjControl* ctrl, cudaStream_t s);
-// Gradient step with the FP64 pressure (x64 - mean): the difference, scaling
-// and subtraction run in FP64, then round to FP32.
-void launch_gradient64(const ProjectionArgs& a, const float* u_in, const float* v_in, const float* w_in,
-                       float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat, float* w_hat,
-                       ProjControl* ctrl, cudaStream_t s);
+// pressure copy (x64 - mean) into p32 with ctrl->p_mean_f = 0, then (u_in
+// given) the gradient step with the FP64 pressure (x64 - mean): the
+// difference, scaling and subtraction in FP64, rounded to FP32; walls,
+// reflection hat (u_hat given) and divergence after. Unmasked grids with n %
+// 4 == 0 run the residual and the gradient as one pass. Returns the number
+// of kernels launched.
+int launch_finish_projection64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
+                               int partial_capacity, ProjControl* ctrl, const float* u_in, const float* v_in,
+                               const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat,
+                               float* v_hat, float* w_hat, cudaStream_t s);
 // FP64 infinity norm of (b - mean_b) - A (x - mean_x) into ctrl->res_bits;
 // `final_pass` subtracts the pressure mean.
 void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,

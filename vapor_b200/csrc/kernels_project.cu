@@ -737,6 +737,164 @@ __global__ void __launch_bounds__(kThreads) k_gradient64(Grid g, float dt,
     }
 }
 
+// The two FP64 passes that end a mixed-precision or FPCG projection, fused
+// for unmasked grids with n % 4 == 0: the final residual of x64 - mean
+// (k_residual64: same neighbour order, missing neighbours contribute -1 * 0,
+// which leaves the FP64 sum's bits unchanged), the float pressure copy, and
+// the gradient step with walls, reflection hat and divergence after
+// (k_gradient64: same expressions). One thread owns 4 consecutive cells of a
+// row (2 slots of each colour of the split layout) for zb consecutive planes
+// and marches up z keeping the pressure rows of planes z - 1, z, z + 1 in
+// registers, so x64 is read once from DRAM and every access is a 16-byte
+// vector load except the row-end neighbours and the x faces.
+__global__ void __launch_bounds__(kThreads) k_finish64(Grid g, float dt, const float* __restrict__ b,
+                                                       float* __restrict__ p32, ProjControl* ctrl,
+                                                       const float* __restrict__ u, const float* __restrict__ v,
+                                                       const float* __restrict__ w, float* __restrict__ uo,
+                                                       float* __restrict__ vo, float* __restrict__ wo,
+                                                       float* __restrict__ uh, float* __restrict__ vh,
+                                                       float* __restrict__ wh, int zb) {
+    __shared__ double s_res[32];
+    __shared__ float s_div[32];
+    const int n = g.n;
+    const int hw = n >> 1, groups = n >> 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = t / groups;
+    double rmax = 0.0;
+    float dmax = 0.f;
+    unsigned int bad_solve = 0u, bad_div = 0u;
+    if (y < n) {
+        const int j = t - y * groups;
+        const int x0 = 4 * j;
+        const double* __restrict__ X = ctrl->x64[ctrl->x64_cur];
+        const double pm = ctrl->p_mean64;
+        const float bm = ctrl->rhs_mean_f;
+        const double hInv = 1.0 / double(g.h), dtd = double(dt);
+        const size_t stride = size_t(n) * n * hw;  // values per colour
+        // natural-order cells x0 .. x0 + 3 of row (yy, zz) minus the mean:
+        // slots 2j, 2j + 1 of colour (yy + zz) & 1 hold x0, x0 + 2, those of
+        // the other colour x0 + 1, x0 + 3
+        auto row = [&](int yy, int zz, double (&o)[4]) {
+            const size_t base = (size_t(zz) * n + yy) * hw + 2 * j;
+            const int c0 = (yy + zz) & 1;
+            const double2 A = *reinterpret_cast<const double2*>(X + size_t(c0) * stride + base);
+            const double2 B = *reinterpret_cast<const double2*>(X + size_t(1 - c0) * stride + base);
+            o[0] = A.x - pm;
+            o[1] = B.x - pm;
+            o[2] = A.y - pm;
+            o[3] = B.y - pm;
+        };
+        const int z0 = blockIdx.y * zb, z1 = min(n, z0 + zb);
+        double zm[4] = {0.0, 0.0, 0.0, 0.0}, zc[4], zp[4];
+        if (z0 > 0) row(y, z0 - 1, zm);
+        row(y, z0, zc);
+        const size_t nn = size_t(n) * n;
+        for (int z = z0; z < z1; ++z) {
+            if (z + 1 < n) row(y, z + 1, zp);
+            double ym[4] = {0.0, 0.0, 0.0, 0.0}, yp[4] = {0.0, 0.0, 0.0, 0.0};
+            if (y > 0) row(y - 1, z, ym);
+            if (y + 1 < n) row(y + 1, z, yp);
+            const size_t rb = (size_t(z) * n + y) * hw + 2 * j;
+            const int c0 = (y + z) & 1;
+            // row-end neighbours: x0 - 1 (odd, the colour of x0 + 1) and
+            // x0 + 4 (even, the colour of x0)
+            const double left = x0 > 0 ? X[size_t(1 - c0) * stride + rb - 1] - pm : 0.0;
+            const double right = x0 + 4 < n ? X[size_t(c0) * stride + rb + 2] - pm : 0.0;
+            const float2 bA = *reinterpret_cast<const float2*>(b + size_t(c0) * stride + rb);
+            const float2 bB = *reinterpret_cast<const float2*>(b + size_t(1 - c0) * stride + rb);
+            const float bv[4] = {bA.x, bB.x, bA.y, bB.y};
+            const double xl[6] = {left, zc[0], zc[1], zc[2], zc[3], right};  // cells x0 - 1 .. x0 + 4
+            const size_t ix0 = size_t(n + 1) * (size_t(y) + size_t(n) * z) + x0;
+            const size_t iy0 = size_t(n) * (size_t(y) + size_t(n + 1) * z) + x0;
+            const size_t iz0 = nn * z + size_t(y) * n + x0;
+            float uin[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) uin[k] = u[ix0 + k];
+            const float4 v0 = *reinterpret_cast<const float4*>(v + iy0);
+            const float4 v1 = *reinterpret_cast<const float4*>(v + iy0 + n);
+            const float4 w0 = *reinterpret_cast<const float4*>(w + iz0);
+            const float4 w1 = *reinterpret_cast<const float4*>(w + iz0 + nn);
+            const float vin0[4] = {v0.x, v0.y, v0.z, v0.w}, vin1[4] = {v1.x, v1.y, v1.z, v1.w};
+            const float win0[4] = {w0.x, w0.y, w0.z, w0.w}, win1[4] = {w1.x, w1.y, w1.z, w1.w};
+            float p32v[4], ux0[4], ux1[4], vy0[4], vy1[4], wz0[4], wz1[4];
+            const int nyz = int(y > 0) + int(y + 1 < n) + int(z > 0) + int(z + 1 < n);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int x = x0 + k;
+                const double pc = zc[k];
+                // residual, neighbour order x-1, x+1, y-1, y+1, z-1, z+1
+                const int dcell = int(x > 0) + int(x + 1 < n) + nyz;
+                double ax = double(float(dcell)) * pc;
+                if (x > 0) ax += -1.0 * xl[k];
+                if (x + 1 < n) ax += -1.0 * xl[k + 2];
+                if (y > 0) ax += -1.0 * ym[k];
+                if (y + 1 < n) ax += -1.0 * yp[k];
+                if (z > 0) ax += -1.0 * zm[k];
+                if (z + 1 < n) ax += -1.0 * zp[k];
+                const float bi = bv[k] - bm;
+                if (!isfinite(pc)) bad_solve = 1u;
+                p32v[k] = float(pc);
+                const double a = fabs(double(bi) - ax);
+                rmax = rmax < a ? a : rmax;
+                // gradient, walls closed
+                ux0[k] = x == 0 ? 0.f : float(double(uin[k]) - dtd * (pc - xl[k]) * hInv);
+                ux1[k] = x + 1 == n ? 0.f : float(double(uin[k + 1]) - dtd * (xl[k + 2] - pc) * hInv);
+                vy0[k] = y == 0 ? 0.f : float(double(vin0[k]) - dtd * (pc - ym[k]) * hInv);
+                vy1[k] = y + 1 == n ? 0.f : float(double(vin1[k]) - dtd * (yp[k] - pc) * hInv);
+                wz0[k] = z == 0 ? 0.f : float(double(win0[k]) - dtd * (pc - zm[k]) * hInv);
+                wz1[k] = z + 1 == n ? 0.f : float(double(win1[k]) - dtd * (zp[k] - pc) * hInv);
+                const float div = (ux1[k] - ux0[k] + vy1[k] - vy0[k] + wz1[k] - wz0[k]) / g.h;
+                if (!isfinite(div)) bad_div = 1u;
+                dmax = maxf_ref(dmax, fabsf(div));
+            }
+            *reinterpret_cast<float2*>(p32 + size_t(c0) * stride + rb) = make_float2(p32v[0], p32v[2]);
+            *reinterpret_cast<float2*>(p32 + size_t(1 - c0) * stride + rb) = make_float2(p32v[1], p32v[3]);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) uo[ix0 + k] = ux0[k];
+            *reinterpret_cast<float4*>(vo + iy0) = make_float4(vy0[0], vy0[1], vy0[2], vy0[3]);
+            *reinterpret_cast<float4*>(wo + iz0) = make_float4(wz0[0], wz0[1], wz0[2], wz0[3]);
+            const bool xwall = x0 + 4 == n, ywall = y + 1 == n, zwall = z + 1 == n;
+            if (xwall) uo[ix0 + 4] = ux1[3];
+            if (ywall) *reinterpret_cast<float4*>(vo + iy0 + n) = make_float4(vy1[0], vy1[1], vy1[2], vy1[3]);
+            if (zwall) *reinterpret_cast<float4*>(wo + iz0 + nn) = make_float4(wz1[0], wz1[1], wz1[2], wz1[3]);
+            if (uh) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) uh[ix0 + k] = 2.f * ux0[k] - uin[k];
+                *reinterpret_cast<float4*>(vh + iy0) =
+                    make_float4(2.f * vy0[0] - vin0[0], 2.f * vy0[1] - vin0[1], 2.f * vy0[2] - vin0[2],
+                                2.f * vy0[3] - vin0[3]);
+                *reinterpret_cast<float4*>(wh + iz0) =
+                    make_float4(2.f * wz0[0] - win0[0], 2.f * wz0[1] - win0[1], 2.f * wz0[2] - win0[2],
+                                2.f * wz0[3] - win0[3]);
+                if (xwall) uh[ix0 + 4] = 2.f * ux1[3] - uin[4];
+                if (ywall)
+                    *reinterpret_cast<float4*>(vh + iy0 + n) =
+                        make_float4(2.f * vy1[0] - vin1[0], 2.f * vy1[1] - vin1[1], 2.f * vy1[2] - vin1[2],
+                                    2.f * vy1[3] - vin1[3]);
+                if (zwall)
+                    *reinterpret_cast<float4*>(wh + iz0 + nn) =
+                        make_float4(2.f * wz1[0] - win1[0], 2.f * wz1[1] - win1[1], 2.f * wz1[2] - win1[2],
+                                    2.f * wz1[3] - win1[3]);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                zm[k] = zc[k];
+                zc[k] = zp[k];
+            }
+        }
+    }
+    const double br = block_max(rmax, s_res);
+    const float bd = block_max(dmax, s_div);
+    const int any_solve = __syncthreads_or(int(bad_solve));
+    const int any_div = __syncthreads_or(int(bad_div));
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(&ctrl->res_bits, br);
+        atomic_max_nonneg(&ctrl->div_after_bits, bd);
+        if (any_solve) atomicOr(&ctrl->nonfinite, 4u);
+        if (any_div) atomicOr(&ctrl->nonfinite, 2u);
+    }
+}
+
 // FP64 infinity norm of b' - A x' (StencilLinearSystem.cpp:53-70) with
 // b' = b - rhs mean and, on the final pass, x' = x - pressure mean.
 __global__ void __launch_bounds__(kThreads) k_residual(Grid g, const float* __restrict__ x,
@@ -1153,27 +1311,37 @@ void launch_zero_error_gated(const ProjectionArgs& a, float* e, const ProjContro
     k_zero_error_gated<<<kMaxReductionBlocks, kThreads, 0, s>>>(e, count, ctrl);
 }
 
-void launch_pressure_mean64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
-                            int partial_capacity, ProjControl* ctrl, cudaStream_t s) {
-    const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
+int launch_finish_projection64(const ProjectionArgs& a, const float* b, float* p32, double* partials,
+                               int partial_capacity, ProjControl* ctrl, const float* u_in, const float* v_in,
+                               const float* w_in, float* u_out, float* v_out, float* w_out, float* u_hat,
+                               float* v_hat, float* w_hat, cudaStream_t s) {
+    const int n = a.g.n;
+    const size_t cells = size_t(n) * n * n;
     const int blocks = std::min(reduction_blocks(cells), partial_capacity);
     count_launch();
     k_psum64<<<blocks, kThreads, 0, s>>>(a.g, ctrl, partials);
     count_launch();
     k_psum64_finish<<<1, 1024, 0, s>>>(ctrl, partials, blocks, a.solid ? a.fluid : double(cells));
+    if (u_in && !a.solid && !a.diag && n % 4 == 0) {
+        // residual, pressure copy and gradient in one z-marching pass
+        constexpr int zb = 8;
+        const dim3 grid(unsigned((size_t(n) * (n / 4) + kThreads - 1) / kThreads), unsigned((n + zb - 1) / zb));
+        count_launch();
+        k_finish64<<<grid, kThreads, 0, s>>>(a.g, a.dt, b, p32, ctrl, u_in, v_in, w_in, u_out, v_out, w_out,
+                                             u_hat, v_hat, w_hat, zb);
+        count_launch();
+        k_final_check<<<1, 1, 0, s>>>(ctrl);
+        return 4;
+    }
     count_launch();
     k_residual64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, b, p32, ctrl, a.diag);
     count_launch();
     k_final_check<<<1, 1, 0, s>>>(ctrl);
-}
-
-void launch_gradient64(const ProjectionArgs& a, const float* u_in, const float* v_in, const float* w_in,
-                       float* u_out, float* v_out, float* w_out, float* u_hat, float* v_hat, float* w_hat,
-                       ProjControl* ctrl, cudaStream_t s) {
-    const size_t cells = size_t(a.g.n) * a.g.n * a.g.n;
+    if (!u_in) return 4;
     count_launch();
     k_gradient64<<<reduction_blocks(cells), kThreads, 0, s>>>(a.g, a.dt, u_in, v_in, w_in, u_out, v_out, w_out,
                                                               u_hat, v_hat, w_hat, ctrl, a.solid);
+    return 5;
 }
 
 void launch_residual(const ProjectionArgs& a, const float* x, const float* b, ProjControl* ctrl, bool final_pass,
