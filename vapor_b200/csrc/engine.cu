@@ -330,7 +330,7 @@ void set_fpcg_smoothing(int sweeps, float omega) {
 
 void Workspace::ensure_fpcg(bool coarse) {
     const size_t count = rb_count(n_);
-    for (DevArray<float>* v : {&cg_p_, &cg_q_, &cg_z_, &cg_z2_})
+    for (DevArray<float>* v : {&cg_p_, &cg_p2_, &cg_q_, &cg_z_, &cg_z2_})
         if (v->n != count) {
             v->allocate(count);
             v->zero(stream_);
@@ -417,14 +417,25 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
             t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         }
     };
+    // n % 8 == 0: the direction update, A p and the deferred error update run
+    // as one pass (launch_cg_direction_apply), with the direction in two
+    // buffers; same values as the separate passes
+    const bool fused = n_ % 8 == 0;
+    float* const pbuf[2] = {cg_p_.p, cg_p2_.p};
     auto recentre_group = [&](cudaStream_t st) {
+        if (fused) launch_cg_fold(count, e, pbuf, cg_, ctrl_, st);
         launch_refine_residual_gated(a, b_.p, e, r, ctrl_, st);
         launch_check_gated(ctrl_, LoopCond{}, st);
         launch_zero_error_gated(a, e, ctrl_, st);
     };
+    auto update = [&](cudaStream_t st, LoopCond if_cond) {
+        if (fused) launch_cg_update_r(count, r, cg_q_.p, cg_, ctrl_, if_cond, st);
+        else launch_cg_update(count, e, r, cg_p_.p, cg_q_.p, cg_, ctrl_, if_cond, st);
+    };
     auto iteration = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_KRYLOV);
-        launch_apply_A_alpha(n_, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
+        if (fused) launch_cg_direction_apply(n_, cg_z_.p, pbuf, e, cg_q_.p, cg_partials_.p, cg_, st);
+        else launch_apply_A_alpha(n_, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
         t.end(VAPOR_PHASE_KRYLOV, 2);
         t.begin(VAPOR_PHASE_RESIDUAL);
         if (graph) {
@@ -432,24 +443,24 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
             LoopCond if_cond;
             if_cond.active = 1;
             if_cond.handle = (unsigned long long)ifh;
-            launch_cg_update(count, e, r, cg_p_.p, cg_q_.p, cg_, ctrl_, if_cond, st);
+            update(st, if_cond);
             add_conditional(st, body_stream2_.s, ifh, cudaGraphCondTypeIf,
                             [&](cudaStream_t is) { recentre_group(is); });
         } else {
-            launch_cg_update(count, e, r, cg_p_.p, cg_q_.p, cg_, ctrl_, LoopCond{}, st);
+            update(st, LoopCond{});
             recentre_group(st);
         }
-        t.end(VAPOR_PHASE_RESIDUAL, 5);
+        t.end(VAPOR_PHASE_RESIDUAL, fused ? 7 : 5);
         precondition(st);
         t.begin(VAPOR_PHASE_KRYLOV);
         launch_cg_beta(count, cg_z_.p, r, cg_q_.p, cg_partials_.p, cg_, st);
-        launch_cg_direction(count, cg_p_.p, cg_z_.p, cg_, st);
-        t.end(VAPOR_PHASE_KRYLOV, 3);
+        if (!fused) launch_cg_direction(count, cg_p_.p, cg_z_.p, cg_, st);
+        t.end(VAPOR_PHASE_KRYLOV, fused ? 2 : 3);
         launch_loop_condition(ctrl_, cond, st);
     };
     precondition(s);
     launch_cg_rho(count, cg_z_.p, r, cg_partials_.p, cg_, s);
-    VB_CUDA(cudaMemcpyAsync(cg_p_.p, cg_z_.p, cg_z_.bytes(), cudaMemcpyDeviceToDevice, s));
+    if (!fused) VB_CUDA(cudaMemcpyAsync(cg_p_.p, cg_z_.p, cg_z_.bytes(), cudaMemcpyDeviceToDevice, s));
     if (graph) {
         add_while_loop(s, body_stream_.s, handle, iteration);
     } else {

@@ -54,6 +54,13 @@ struct CgControl {
     double pq;       // p.Ap
     double gamma;    // scale of the coarse-grid correction (Galerkin)
     double zc_mean;  // mean of the coarse correction, removed before use
+    // fused step (n % 8 == 0): the direction lives in two buffers, p_cur the
+    // current one; alpha_pending * p_cur is the error update not yet added
+    // to e (added by the next direction kernel, or folded before a
+    // re-centring). flags: bit 0 a direction exists, bit 1 an update is pending.
+    double alpha_pending;
+    int p_cur;
+    int flags;
 };
 
 // Simulation-wide reduction outputs (diagnostics).
@@ -255,6 +262,19 @@ void launch_cg_beta(size_t count, const float* z, const float* r, const float* q
                     cudaStream_t s);
 // p = z + beta p.
 void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s);
+// The fused form of one CG step's direction and update passes (n % 8 == 0),
+// with the direction in two buffers p[2] (cg->p_cur the current):
+// launch_cg_direction_apply: e += alpha_pending p_cur (the previous step's
+// deferred update), p_new = z + beta p_cur (z when beta == 0) into the other
+// buffer, q = A p_new, alpha = rho / (p_new.q), p_cur = new, alpha_pending =
+// alpha. launch_cg_update_r: r -= alpha q with max |r|, then the decision.
+// launch_cg_fold (gated, before a re-centring): e += alpha_pending p_cur,
+// alpha_pending = 0. Same values as the unfused sequence, bit for bit.
+void launch_cg_direction_apply(int n, const float* z, float* const* p, float* e, float* q, double* partials,
+                               CgControl* cg, cudaStream_t s);
+void launch_cg_update_r(size_t count, float* r, const float* q, const CgControl* cg, ProjControl* ctrl,
+                        LoopCond recentre_cond, cudaStream_t s);
+void launch_cg_fold(size_t count, float* e, float* const* p, CgControl* cg, const ProjControl* ctrl, cudaStream_t s);
 // rc = 4^3 block sums of r - A z on the (n/4)^3 grid (natural layout); n % 4 == 0.
 // `rows` holds n^3 / 4 floats of scratch.
 void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s);

@@ -153,6 +153,145 @@ __global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __
     }
 }
 
+// Fused direction step on row pairs (n % 8 == 0), grid as k_apply_A_dot:
+// with po = p[p_cur] and pn the other buffer, e += alpha_pending po (when an
+// update is pending), pn = z + beta po (a copy of z for the first direction),
+// q = A pn and FP64 block partials of pn.q. The stencil reads pn at the
+// neighbours as z + beta po, the value the neighbour's thread stores, so q
+// equals A applied to the stored pn.
+__device__ __forceinline__ float dir_value(float zv, float pv, float beta, bool first) {
+    return first ? zv : zv + beta * pv;
+}
+__device__ __forceinline__ RowEO dir_eo(const float* __restrict__ z, const float* __restrict__ po, int stride,
+                                        int off, int sy, float beta, bool first) {
+    const RowEO a = load_eo(z, stride, off, sy);
+    if (first) return a;
+    const RowEO b = load_eo(po, stride, off, sy);
+    RowEO r;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        r.e[k] = a.e[k] + beta * b.e[k];
+        r.o[k] = a.o[k] + beta * b.o[k];
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_direction_apply(int n, const float* __restrict__ zs, float* P0, float* P1,
+                                                              float* __restrict__ es, float* __restrict__ qs,
+                                                              const CgControl* __restrict__ cg,
+                                                              double* __restrict__ partials) {
+    __shared__ double s_sum[32];
+    const float* __restrict__ po = cg->p_cur ? P1 : P0;
+    float* __restrict__ pn = cg->p_cur ? P0 : P1;
+    const float beta = float(cg->beta), ap = float(cg->alpha_pending);
+    const bool first = (cg->flags & 1) == 0, pending = (cg->flags & 2) != 0;
+    const int hw = n >> 1, groups = hw >> 2;
+    const int plane = n * hw, stride = n * plane;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y, y = t / groups, j = t - y * groups;
+    double acc = 0.0;
+    if (y < n) {
+        const int off = z * plane + y * hw + 4 * j;
+        const int sy = (y + z) & 1;
+        const RowEO me = dir_eo(zs, po, stride, off, sy, beta, first);
+        const RowEO ym = y > 0 ? dir_eo(zs, po, stride, off - hw, (y + z - 1) & 1, beta, first) : zero_eo();
+        const RowEO yp = y + 1 < n ? dir_eo(zs, po, stride, off + hw, (y + z + 1) & 1, beta, first) : zero_eo();
+        const RowEO zm = z > 0 ? dir_eo(zs, po, stride, off - plane, (y + z - 1) & 1, beta, first) : zero_eo();
+        const RowEO zp = z + 1 < n ? dir_eo(zs, po, stride, off + plane, (y + z + 1) & 1, beta, first) : zero_eo();
+        const int x0 = 8 * j;
+        const int lo = (sy ? 0 : stride) + off - 1, ro = (sy ? stride : 0) + off + 4;
+        const float left = x0 > 0 ? dir_value(zs[lo], po[lo], beta, first) : 0.f;
+        const float right = x0 + 8 < n ? dir_value(zs[ro], po[ro], beta, first) : 0.f;
+        const int nyz = (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+        float q[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {  // apply_pair's operation order
+            const int x = x0 + m, k = m >> 1;
+            const bool even = (m & 1) == 0;
+            const float v = even ? me.e[k] : me.o[k];
+            float ax = float((x > 0) + (x + 1 < n) + nyz) * v;
+            if (x > 0) ax -= even ? (m > 0 ? me.o[k - 1 < 0 ? 0 : k - 1] : left) : me.e[k];
+            if (x + 1 < n) ax -= even ? me.o[k] : (m < 7 ? me.e[k + 1 > 3 ? 3 : k + 1] : right);
+            if (y > 0) ax -= even ? ym.e[k] : ym.o[k];
+            if (y + 1 < n) ax -= even ? yp.e[k] : yp.o[k];
+            if (z > 0) ax -= even ? zm.e[k] : zm.o[k];
+            if (z + 1 < n) ax -= even ? zp.e[k] : zp.o[k];
+            q[m] = ax;
+        }
+        const int ev = (sy ? stride : 0) + off, od = (sy ? 0 : stride) + off;
+        *reinterpret_cast<float4*>(qs + ev) = make_float4(q[0], q[2], q[4], q[6]);
+        *reinterpret_cast<float4*>(qs + od) = make_float4(q[1], q[3], q[5], q[7]);
+        *reinterpret_cast<float4*>(pn + ev) = make_float4(me.e[0], me.e[1], me.e[2], me.e[3]);
+        *reinterpret_cast<float4*>(pn + od) = make_float4(me.o[0], me.o[1], me.o[2], me.o[3]);
+        if (pending) {
+            const RowEO pe = load_eo(po, stride, off, sy);
+            const RowEO ee = load_eo(es, stride, off, sy);
+            *reinterpret_cast<float4*>(es + ev) = make_float4(ee.e[0] + ap * pe.e[0], ee.e[1] + ap * pe.e[1],
+                                                              ee.e[2] + ap * pe.e[2], ee.e[3] + ap * pe.e[3]);
+            *reinterpret_cast<float4*>(es + od) = make_float4(ee.o[0] + ap * pe.o[0], ee.o[1] + ap * pe.o[1],
+                                                              ee.o[2] + ap * pe.o[2], ee.o[3] + ap * pe.o[3]);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc += double(me.e[k]) * q[2 * k] + double(me.o[k]) * q[2 * k + 1];
+    }
+    const double b = block_sum(acc, s_sum);
+    if (threadIdx.x == 0) {
+        const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+        partials[2 * blk] = b;
+        partials[2 * blk + 1] = 0.0;
+    }
+}
+
+// r -= alpha q and max |r| (FP32) into ctrl->res32_bits (count % 4 == 0).
+__global__ void __launch_bounds__(kThreads) k_update_r4(size_t count4, float4* __restrict__ r,
+                                                        const float4* __restrict__ q,
+                                                        const CgControl* __restrict__ cg, ProjControl* ctrl) {
+    __shared__ float s_max[32];
+    const float alpha = float(cg->alpha);
+    float m = 0.f;
+    unsigned int bad = 0u;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count4; i += size_t(gridDim.x) * blockDim.x) {
+        const float4 qv = q[i];
+        float4 rv = r[i];
+        rv.x = rv.x - alpha * qv.x;
+        rv.y = rv.y - alpha * qv.y;
+        rv.z = rv.z - alpha * qv.z;
+        rv.w = rv.w - alpha * qv.w;
+        r[i] = rv;
+        if (!isfinite(rv.x) || !isfinite(rv.y) || !isfinite(rv.z) || !isfinite(rv.w)) bad = 1u;
+        m = fmaxf(m, fmaxf(fmaxf(fabsf(rv.x), fabsf(rv.y)), fmaxf(fabsf(rv.z), fabsf(rv.w))));
+    }
+    const float bm = block_max(m, s_max);
+    const int any_bad = __syncthreads_or(int(bad));
+    if (threadIdx.x == 0) {
+        atomicMax(&ctrl->res32_bits, __float_as_uint(bm));
+        if (any_bad) atomicOr(&ctrl->nonfinite, 4u);
+    }
+}
+
+// Before a re-centring (gated on ctrl->recentre): e += alpha_pending p_cur.
+__global__ void __launch_bounds__(kThreads) k_fold_pending(size_t count4, float4* __restrict__ e,
+                                                           const float4* __restrict__ P0, const float4* __restrict__ P1,
+                                                           const CgControl* __restrict__ cg,
+                                                           const ProjControl* __restrict__ ctrl) {
+    if (!ctrl->recentre || (cg->flags & 2) == 0) return;
+    const float ap = float(cg->alpha_pending);
+    const float4* __restrict__ p = cg->p_cur ? P1 : P0;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count4; i += size_t(gridDim.x) * blockDim.x) {
+        const float4 pv = p[i];
+        float4 ev = e[i];
+        ev.x = ev.x + ap * pv.x;
+        ev.y = ev.y + ap * pv.y;
+        ev.z = ev.z + ap * pv.z;
+        ev.w = ev.w + ap * pv.w;
+        e[i] = ev;
+    }
+}
+
+__global__ void k_fold_clear(CgControl* cg, const ProjControl* __restrict__ ctrl) {
+    if (ctrl->recentre) cg->flags &= ~2;
+}
+
 // Restriction pass 1 on row pairs (n % 16 == 0): the residuals r - A z of the
 // 8 cells, summed per coarse block in x order, into rows[(z n + y) nc + cx].
 // Grid as k_apply_A_dot.
@@ -228,12 +367,34 @@ __device__ void sum2(const double* __restrict__ partials, int blocks, double* s_
     b = block_sum(y, s_sum);
 }
 
-// rho = z.r for the first direction.
+// rho = z.r for the first direction (which the fused step forms as z: beta
+// 0, nothing pending, buffer 0 current).
 __global__ void k_rho_finish(const double* __restrict__ partials, int blocks, CgControl* cg) {
     __shared__ double s_sum[32];
     double zr, unused;
     sum2(partials, blocks, s_sum, zr, unused);
-    if (threadIdx.x == 0) cg->rho = zr;
+    if (threadIdx.x == 0) {
+        cg->rho = zr;
+        cg->beta = 0.0;
+        cg->alpha_pending = 0.0;
+        cg->p_cur = 0;
+        cg->flags = 0;
+    }
+}
+
+// The fused step's alpha: as k_alpha_finish, then the new direction becomes
+// current and its update pending.
+__global__ void k_alpha_finish_pp(const double* __restrict__ partials, int blocks, CgControl* cg) {
+    __shared__ double s_sum[32];
+    double pq, unused;
+    sum2(partials, blocks, s_sum, pq, unused);
+    if (threadIdx.x == 0) {
+        cg->pq = pq;
+        cg->alpha = (pq > 0.0 && isfinite(cg->rho / pq)) ? cg->rho / pq : 0.0;
+        cg->alpha_pending = cg->alpha;
+        cg->p_cur ^= 1;
+        cg->flags = 3;
+    }
 }
 
 // alpha = rho / (p.q).
@@ -564,6 +725,33 @@ void launch_cg_beta(size_t count, const float* z, const float* r, const float* q
 void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s) {
     count_launch();
     k_p_update<<<blocks_for(count), kThreads, 0, s>>>(count, p, z, cg);
+}
+
+void launch_cg_direction_apply(int n, const float* z, float* const* p, float* e, float* q, double* partials,
+                               CgControl* cg, cudaStream_t s) {
+    const dim3 grid = pair_grid(n);
+    count_launch();
+    k_direction_apply<<<grid, kThreads, 0, s>>>(n, z, p[0], p[1], e, q, cg, partials);
+    count_launch();
+    k_alpha_finish_pp<<<1, 1024, 0, s>>>(partials, int(grid.x * grid.y), cg);
+}
+
+void launch_cg_update_r(size_t count, float* r, const float* q, const CgControl* cg, ProjControl* ctrl,
+                        LoopCond recentre_cond, cudaStream_t s) {
+    count_launch();
+    k_update_r4<<<blocks_for(count / 4), kThreads, 0, s>>>(count / 4, reinterpret_cast<float4*>(r),
+                                                          reinterpret_cast<const float4*>(q), cg, ctrl);
+    count_launch();
+    k_cg_decide<<<1, 1, 0, s>>>(ctrl, recentre_cond.active, (cudaGraphConditionalHandle)recentre_cond.handle);
+}
+
+void launch_cg_fold(size_t count, float* e, float* const* p, CgControl* cg, const ProjControl* ctrl, cudaStream_t s) {
+    count_launch();
+    k_fold_pending<<<blocks_for(count / 4), kThreads, 0, s>>>(count / 4, reinterpret_cast<float4*>(e),
+                                                             reinterpret_cast<const float4*>(p[0]),
+                                                             reinterpret_cast<const float4*>(p[1]), cg, ctrl);
+    count_launch();
+    k_fold_clear<<<1, 1, 0, s>>>(cg, ctrl);
 }
 
 void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s) {
