@@ -95,8 +95,9 @@ def test_iteration_cap_inside_a_blocked_launch():
 
 @pytest.mark.parametrize("n", [32, 64])
 def test_fpcg_smoothing_blocked_equals_one_colour_sweeps(n):
-    """The FPCG preconditioner's 2 + 2 smoothing sweeps (from zero, then in
-    reverse colour order) as two blocked launches."""
+    """The FPCG preconditioner's smoothing runs one-colour sweeps whatever
+    the blocking setting (its last sweep also forms the dot products of the
+    direction update): the setting leaves the solve's bits unchanged."""
     from vapor_b200.learned import COARSE_WEIGHTS, WarmStartNet
     net = WarmStartNet.load(COARSE_WEIGHTS)
     _, u, v, w = random_fields(n, seed=940 + n)

@@ -330,7 +330,7 @@ void set_fpcg_smoothing(int sweeps, float omega) {
 
 void Workspace::ensure_fpcg(bool coarse) {
     const size_t count = rb_count(n_);
-    for (DevArray<float>* v : {&cg_p_, &cg_p2_, &cg_q_, &cg_z_, &cg_z2_})
+    for (DevArray<float>* v : {&cg_p_, &cg_p2_, &cg_q_, &cg_z_})
         if (v->n != count) {
             v->allocate(count);
             v->zero(stream_);
@@ -363,59 +363,48 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     const FpcgSmoothing sm = fpcg_smoothing();
     const int sweeps = sm.sweeps;
     const ProjectionArgs smooth{a.g, a.dt, sm.omega, 0.0f, a.options};
-    // the smoothing pairs run as one temporally blocked launch each when the
-    // grid allows (same bits as the one-colour launches)
-    const bool blocked = sor_block_iterations(n_) == 2 && sweeps == 2;
-    // z after pre-smoothing and the coarse correction: the twin buffer when
-    // blocked (the post-smoothing launch is out of place), else z itself
-    float* zpre = blocked ? cg_z2_.p : cg_z_.p;
     if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);
     else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
     t.begin(VAPOR_PHASE_RESIDUAL);
     launch_refine_residual(a, b_.p, e, r, ctrl_, s);
     launch_check(ctrl_, 0, false, true, cond, s);
     t.end(VAPOR_PHASE_RESIDUAL, 2);
-    auto precondition = [&](cudaStream_t st) {
+    // The preconditioner, z = M r, with one-colour sweeps (the temporally
+    // blocked sweep measured slower at these sizes). With `dot`, the last
+    // sweep also writes the partials of z.r and z.q for beta; returns their
+    // block count, or 0 when they were not written.
+    auto precondition = [&](cudaStream_t st, bool dot) {
         t.begin(VAPOR_PHASE_SOR);
-        if (blocked) {
-            // both sweeps in one launch, starting from z = 0 (no iterate is
-            // read), into the pre-smoothed twin z2
-            launch_sor_blocked(smooth, sweeps, 0, zpre, zpre, r, ctrl_, false, 0, false, st, false, false,
-                               true);
-            t.end(VAPOR_PHASE_SOR, 1);
-        } else {
-            // the first colour sweep starts from z = 0 (and clears the other colour)
-            const bool fused_start = sor_fuses_measure(n_);
-            if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
-            for (int j = 0; j < sweeps; ++j) {
-                launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false,
-                                 fused_start && j == 0);
-                launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
-            }
-            t.end(VAPOR_PHASE_SOR, 2 * sweeps);
+        // the first colour sweep starts from z = 0 (and clears the other colour)
+        const bool fused_start = sor_fuses_measure(n_);
+        if (!fused_start) VB_CUDA(cudaMemsetAsync(cg_z_.p, 0, cg_z_.bytes(), st));
+        for (int j = 0; j < sweeps; ++j) {
+            launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false, false, fused_start && j == 0);
+            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
         }
+        t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
-            launch_restrict_residual(n_, r, zpre, cg_rows_.p, cg_rc_.p, st);
+            launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
             if (coarse_log_)
                 launch_log_coarse(cg_rc_.p, cg_rc_.n, coarse_log_, coarse_log_capacity_, coarse_log_counter_, st);
             coarse->set_stream(st);
             const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
             coarse->set_stream(s);
-            launch_coarse_correction(n_, zpre, zc, cg_rc_.p, cg_partials_.p, cg_, st);
+            launch_coarse_correction(n_, cg_z_.p, zc, cg_rc_.p, cg_partials_.p, cg_, st);
             t.end(VAPOR_PHASE_COARSE, 0);
         }
         t.begin(VAPOR_PHASE_SOR);
-        if (blocked) {
-            launch_sor_blocked(smooth, sweeps, 1, zpre, cg_z_.p, r, ctrl_, false, 0, false, st, false);
-            t.end(VAPOR_PHASE_SOR, 1);
-        } else {
-            for (int j = 0; j < sweeps; ++j) {
-                launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
-                launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
-            }
-            t.end(VAPOR_PHASE_SOR, 2 * sweeps);
+        int dot_blocks = 0;
+        for (int j = 0; j < sweeps; ++j) {
+            launch_sor_color(smooth, 1, cg_z_.p, r, ctrl_, false, 0, false, st, false);
+            if (dot && j + 1 == sweeps)
+                dot_blocks = launch_sor_color_dot(smooth, 0, cg_z_.p, r, cg_q_.p, cg_partials_.p,
+                                                  int(cg_partials_.n), ctrl_, st);
+            if (dot_blocks == 0) launch_sor_color(smooth, 0, cg_z_.p, r, ctrl_, false, 0, false, st, false);
         }
+        t.end(VAPOR_PHASE_SOR, 2 * sweeps);
+        return dot_blocks;
     };
     // n % 8 == 0: the direction update, A p and the deferred error update run
     // as one pass (launch_cg_direction_apply), with the direction in two
@@ -451,14 +440,15 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
             recentre_group(st);
         }
         t.end(VAPOR_PHASE_RESIDUAL, fused ? 7 : 5);
-        precondition(st);
+        const int dot_blocks = precondition(st, true);
         t.begin(VAPOR_PHASE_KRYLOV);
-        launch_cg_beta(count, cg_z_.p, r, cg_q_.p, cg_partials_.p, cg_, st);
+        if (dot_blocks > 0) launch_cg_beta_finish(cg_partials_.p, dot_blocks, cg_, st);
+        else launch_cg_beta(count, cg_z_.p, r, cg_q_.p, cg_partials_.p, cg_, st);
         if (!fused) launch_cg_direction(count, cg_p_.p, cg_z_.p, cg_, st);
-        t.end(VAPOR_PHASE_KRYLOV, fused ? 2 : 3);
+        t.end(VAPOR_PHASE_KRYLOV, (dot_blocks > 0 ? 1 : 2) + (fused ? 0 : 1));
         launch_loop_condition(ctrl_, cond, st);
     };
-    precondition(s);
+    precondition(s, false);
     launch_cg_rho(count, cg_z_.p, r, cg_partials_.p, cg_, s);
     if (!fused) VB_CUDA(cudaMemcpyAsync(cg_p_.p, cg_z_.p, cg_z_.bytes(), cudaMemcpyDeviceToDevice, s));
     if (graph) {

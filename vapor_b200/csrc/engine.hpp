@@ -174,7 +174,6 @@ private:
     DevArray<float> r32_;               // mixed-precision inner right-hand side (FPCG: the residual)
     DevArray<float> cg_p_, cg_q_, cg_z_;  // FPCG direction, A p, preconditioned residual
     DevArray<float> cg_p2_;             // second direction buffer of the fused step (n % 8 == 0)
-    DevArray<float> cg_z2_;             // FPCG pre-smoothed residual (out-of-place blocked smoothing)
     DevArray<float> x_alt_;             // twin of the iterate for out-of-place blocked sweeps
     DevArray<float> cg_rc_;             // FPCG coarse right-hand side ((n/4)^3, natural layout)
     DevArray<float> cg_rows_;           // FPCG restriction scratch (n^2 * n/4 row sums)

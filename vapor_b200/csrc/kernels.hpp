@@ -158,6 +158,12 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
                       bool guarded, int sweep_index, bool subtract_mean, cudaStream_t s, bool exact = true,
                       bool measure = false, bool from_zero = false);
 bool sor_fuses_measure(int n);
+// The fast relaxation sweep (no mask, unguarded) of colour `parity` that
+// also writes FP64 block partials of x.b and x.q (x after the sweep, both
+// colours) to partials[2 * block]; returns the number of blocks, or 0 when
+// the grid has no such form (then nothing ran).
+int launch_sor_color_dot(const ProjectionArgs& a, int parity, float* x, const float* b, const float* q,
+                         double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s);
 // Temporally blocked form of the same sweeps (kernels_sor_blocked.cu):
 // `iterations` (1 or 2) red+black iterations in one launch, starting with
 // colour `first_colour`, bit-identical to 2 * iterations one-colour launches
@@ -260,6 +266,8 @@ void launch_cg_update(size_t count, float* e, float* r, const float* p, const fl
 // beta = -alpha z.q / rho; rho = z.r.
 void launch_cg_beta(size_t count, const float* z, const float* r, const float* q, double* partials, CgControl* cg,
                     cudaStream_t s);
+// beta and rho from `blocks` pairs of partials of z.r and z.q already written.
+void launch_cg_beta_finish(const double* partials, int blocks, CgControl* cg, cudaStream_t s);
 // p = z + beta p.
 void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s);
 // The fused form of one CG step's direction and update passes (n % 8 == 0),

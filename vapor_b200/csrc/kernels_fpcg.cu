@@ -722,6 +722,11 @@ void launch_cg_beta(size_t count, const float* z, const float* r, const float* q
     k_beta_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
 }
 
+void launch_cg_beta_finish(const double* partials, int blocks, CgControl* cg, cudaStream_t s) {
+    count_launch();
+    k_beta_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
+}
+
 void launch_cg_direction(size_t count, float* p, const float* z, const CgControl* cg, cudaStream_t s) {
     count_launch();
     k_p_update<<<blocks_for(count), kThreads, 0, s>>>(count, p, z, cg);

@@ -283,12 +283,19 @@ __global__ void __launch_bounds__(kThreads) k_sor_rb(Grid g, int colour, float o
 // d * 0) * w == 0 + b * w). Replaces clearing x and the first colour sweep.
 // PLAIN: no solid mask and n even (selected by the launcher), which allows
 // the interior-x form of the update below.
-template <bool EXACT, bool RESID, bool FROM_ZERO = false, bool PLAIN = false>
-__global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
+// DOT (with PLAIN; the FPCG preconditioner's last sweep): also FP64 block
+// partials of z.r and z.q over both colours, where z is the iterate after
+// this sweep, r = b and q a further vector (2 values per block at
+// partials[2 * block]); the other colour's z is the row this thread already
+// holds, so the dot products cost three more vector loads per plane.
+template <bool EXACT, bool RESID, bool FROM_ZERO = false, bool PLAIN = false, bool DOT = false>
+__global__ void __launch_bounds__(kThreads, (RESID || DOT) ? 4 : 5) k_sor_rbz(Grid g, int colour, float omega, float floor_diag,
                                                       RelaxTable wr, float* __restrict__ xs,
                                                       const float* __restrict__ bs, ProjControl* ctrl,
                                                       int guarded, int sweep_index, int subtract_mean, int zb,
-                                                      const uint8_t* __restrict__ diag) {
+                                                      const uint8_t* __restrict__ diag,
+                                                      const float* __restrict__ qs = nullptr,
+                                                      double* __restrict__ partials = nullptr) {
     if (guarded && (ctrl->done || ctrl->iterations + sweep_index >= ctrl->max_iterations)) return;
     const int n = g.n;
     const int hw = (n + 1) >> 1;
@@ -296,6 +303,7 @@ __global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = t / groups;
     float rmax = 0.f;
+    double dzr = 0.0, dzq = 0.0;
     if (y < n) {
         const int i0 = (t - y * groups) << 2;
         const int plane = n * hw;
@@ -303,6 +311,9 @@ __global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int
         float* __restrict__ own = xs + colour * stride + y * hw + i0;
         const float* __restrict__ oth = xs + (1 - colour) * stride + y * hw + i0;
         const float* __restrict__ rhs = bs + colour * stride + y * hw + i0;
+        const float* __restrict__ rhs_o = bs + (1 - colour) * stride + y * hw + i0;
+        const float* __restrict__ q_own = DOT ? qs + colour * stride + y * hw + i0 : nullptr;
+        const float* __restrict__ q_oth = DOT ? qs + (1 - colour) * stride + y * hw + i0 : nullptr;
         const uint8_t* __restrict__ dg = diag ? diag + colour * stride + y * hw + i0 : nullptr;
         const float bm = subtract_mean ? ctrl->rhs_mean_f : 0.f;
         const int z0 = blockIdx.y * zb;
@@ -374,6 +385,18 @@ __global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int
                         rmax = fmaxf(rmax, fabsf(rr));
                     }
                 }
+                if (DOT) {
+                    const float4 ro = __ldg(reinterpret_cast<const float4*>(rhs_o + zoff));
+                    const float4 qa = __ldg(reinterpret_cast<const float4*>(q_own + zoff));
+                    const float4 qb = __ldg(reinterpret_cast<const float4*>(q_oth + zoff));
+                    const float zo[4] = {cc.x, cc.y, cc.z, cc.w}, rv[4] = {ro.x, ro.y, ro.z, ro.w};
+                    const float qv[4] = {qa.x, qa.y, qa.z, qa.w}, qw[4] = {qb.x, qb.y, qb.z, qb.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        dzr += double(res[k]) * double(bv[k]) + double(zo[k]) * double(rv[k]);
+                        dzq += double(res[k]) * double(qv[k]) + double(zo[k]) * double(qw[k]);
+                    }
+                }
             } else {  // general form: any n, optional solid mask
                 uchar4 dm = make_uchar4(0, 0, 0, 0);
                 if (dg) dm = *reinterpret_cast<const uchar4*>(dg + zoff);
@@ -420,6 +443,16 @@ __global__ void __launch_bounds__(kThreads, RESID ? 4 : 5) k_sor_rbz(Grid g, int
         __shared__ float s_max[32];
         const float br = block_max(rmax, s_max);
         if (threadIdx.x == 0 && br > 0.f) atomicMax(&ctrl->res32_bits, __float_as_uint(br));
+    }
+    if (DOT) {
+        __shared__ double s_sum[32];
+        const double a = block_sum(dzr, s_sum);
+        const double b = block_sum(dzq, s_sum);
+        if (threadIdx.x == 0) {
+            const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+            partials[2 * blk] = a;
+            partials[2 * blk + 1] = b;
+        }
     }
 }
 
@@ -1193,6 +1226,24 @@ static int sor_planes(int n, int blocks_x) {
     const long per_plane = long(blocks_x);
     int zb = int(std::max(1L, (per_plane * n) / target_blocks));
     return std::min(zb, 8);
+}
+
+int launch_sor_color_dot(const ProjectionArgs& a, int parity, float* x, const float* b, const float* q,
+                         double* partials, int partial_capacity, ProjControl* ctrl, cudaStream_t s) {
+    const int n = a.g.n;
+    const RBLayout L = rb_layout(n);
+    if (!sor_fuses_measure(n) || a.diag != nullptr || n % 2 != 0) return 0;
+    const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
+    const int zb = sor_planes(n, bx);
+    const dim3 grid(bx, (n + zb - 1) / zb);
+    const int blocks = int(grid.x * grid.y);
+    if (2 * blocks > partial_capacity) return 0;
+    RelaxTable wr;
+    for (int d = 0; d < 7; ++d) wr.w[d] = a.omega / std::max(float(d), a.diagonal_floor);
+    count_launch();
+    k_sor_rbz<false, false, false, true, true><<<grid, kThreads, 0, s>>>(
+        a.g, parity, a.omega, a.diagonal_floor, wr, x, b, ctrl, 0, 0, 0, zb, nullptr, q, partials);
+    return blocks;
 }
 
 void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float* b, ProjControl* ctrl,
