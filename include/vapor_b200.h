@@ -361,6 +361,12 @@ vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
  * and pressure means run over fluid cells. Needs VAPOR_SOLVER_MIXED_REFINEMENT;
  * a mask without fluid cells is VAPOR_INVALID_ARGUMENT. */
 vapor_status vapor_stage_set_solid(vapor_stage *stage, const uint8_t *mask);
+/* The same obstacle mask (extension) for every later projection of a
+ * resident simulation's steps: solid cells carry no pressure and the faces
+ * touching them are closed; advection, forcing and smoke are unchanged.
+ * Needs solver_kind VAPOR_SOLVER_MIXED_REFINEMENT (the step fails otherwise);
+ * mask NULL removes it. Waits for the simulation's stream. */
+vapor_status vapor_mac3d_set_solid(vapor_mac3d *sim, const uint8_t *mask);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 
 /* Advection of one staggered field that allocates no device memory. No

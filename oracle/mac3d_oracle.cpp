@@ -582,6 +582,7 @@ struct Simulation {
     std::vector<T> d, u, v, w;
     vapor_projection_result last{};
     long long totalIterations = 0;
+    std::vector<uint8_t> solid;  // n^3 obstacle mask used by every projection (empty: none)
 
     Simulation(int n, T box) : g(n, box) {
         vapor_mac3d_default_params(&p);
@@ -691,8 +692,10 @@ struct Simulation {
             o.reserved0 = 0;
         }
         std::vector<T> pressure;
+        tSolid = solid.empty() ? nullptr : solid.data();
         const int status = project(g, u.data(), v.data(), w.data(), dt, T(p.sor_omega), T(6), o,
                                    p.solver_kind, last, pressure);
+        tSolid = nullptr;
         totalIterations += last.linear_solve.iterations;
         return status;
     }
@@ -868,6 +871,12 @@ VO_EXPORT vapor_status vapor_mac3d_default_params(vapor_mac3d_params* o) {
         *p = static_cast<Simulation<T>*>(h)->p;                                                             \
     }                                                                                                       \
     VO_EXPORT void vo_sim_reset_##SUF(void* h) { static_cast<Simulation<T>*>(h)->reset(); }                 \
+    VO_EXPORT void vo_sim_set_solid_##SUF(void* h, const uint8_t* mask) {                                   \
+        Simulation<T>* sim = static_cast<Simulation<T>*>(h);                                                \
+        const size_t cells = size_t(sim->g.n) * sim->g.n * sim->g.n;                                        \
+        if (mask) sim->solid.assign(mask, mask + cells);                                                    \
+        else sim->solid.clear();                                                                            \
+    }                                                                                                       \
     VO_EXPORT int vo_sim_advance_##SUF(void* h, T dt) { return static_cast<Simulation<T>*>(h)->advance(dt); } \
     VO_EXPORT void vo_sim_get_fields_##SUF(void* h, T* d, T* u, T* v, T* w) {                               \
         auto* s = static_cast<Simulation<T>*>(h);                                                           \

@@ -48,6 +48,7 @@ def _setup_oracle(lib):
         f("vo_sim_set_params", None, _vp, C.POINTER(MacParams))
         f("vo_sim_get_params", None, _vp, C.POINTER(MacParams))
         f("vo_sim_reset", None, _vp)
+        f("vo_sim_set_solid", None, _vp, _vp)
         f("vo_sim_advance", C.c_int, _vp, T)
         f("vo_sim_get_fields", None, _vp, P, P, P, P)
         f("vo_sim_set_fields", None, _vp, P, P, P, P)
@@ -169,6 +170,15 @@ class OracleSim:
 
     def reset(self):
         self._fn("vo_sim_reset")(self.h)
+
+    def set_solid(self, mask):
+        """Obstacle mask (n^3, z, y, x order, nonzero = solid; None clears) for
+        every later projection."""
+        if mask is None:
+            self._fn("vo_sim_set_solid")(self.h, None)
+            return
+        self._mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        self._fn("vo_sim_set_solid")(self.h, self._mask.ctypes.data)
 
     def advance(self, dt):
         return self._fn("vo_sim_advance")(self.h, dt)

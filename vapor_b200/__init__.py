@@ -138,6 +138,7 @@ def _declare(lib):
     f("vapor_mac3d_train_warm_start", _vp, _vp, C.c_float, C.POINTER(C.c_double))
     f("vapor_mac3d_evaluate_warm_start", _vp, _vp, C.POINTER(C.c_double))
     f("vapor_mac3d_set_preconditioner", _vp, _vp)
+    f("vapor_mac3d_set_solid", _vp, _vp)
     f("vapor_stage_set_preconditioner", _vp, _vp)
     f("vapor_stage_train_network", _vp, _vp, C.c_float, C.POINTER(C.c_double))
     return lib
@@ -361,6 +362,18 @@ class MacSimulation3D:
         """Learned coarse-grid correction of the FPCG solver (None: smoothing only)."""
         check(library().vapor_mac3d_set_preconditioner(self._h, net.handle if net is not None else None))
         self._coarse = net
+
+    def set_solid(self, mask):
+        """Obstacles for every later projection of the steps: n^3 uint8 mask
+        (z, y, x order, nonzero = solid) or None. Needs the mixed-precision
+        solver."""
+        if mask is None:
+            check(library().vapor_mac3d_set_solid(self._h, None))
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.size != self.n ** 3:
+            raise ValueError(f"mask needs {self.n ** 3} cells")
+        check(library().vapor_mac3d_set_solid(self._h, m.ctypes.data))
 
 
 def tune_sor_planes(n, planes):

@@ -468,6 +468,9 @@ VB_API vapor_status vapor_mac3d_set_coarse_log(vapor_mac3d* sim, float* log_devi
               require(log_device == nullptr || capacity > 0, "capacity must be positive");
               sim->sim.set_coarse_log(log_device, capacity, counter_device));
 }
+VB_API vapor_status vapor_mac3d_set_solid(vapor_mac3d* sim, const uint8_t* mask) {
+    SIM_GUARD(sim->sim.set_solid(mask));
+}
 VB_API vapor_status vapor_mac3d_set_preconditioner(vapor_mac3d* sim, vapor_unet* net) {
     SIM_GUARD(sim->sim.set_preconditioner(net ? &net->net : nullptr));
 }

@@ -869,6 +869,12 @@ void Simulation::set_preconditioner(unet::UNet* net) {
     }
 }
 
+void Simulation::set_solid(const uint8_t* mask) {
+    VB_CUDA(cudaStreamSynchronize(ws_.stream()));
+    release_graphs();
+    ws_.set_solid(mask);
+}
+
 void Simulation::release_graphs() {
     for (auto& g : graphs_) {
         if (g.exec) cudaGraphExecDestroy(g.exec);

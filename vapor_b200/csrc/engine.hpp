@@ -254,6 +254,9 @@ public:
     // Learned coarse-grid correction of the FPCG solver (VAPOR_SOLVER_FPCG;
     // null: smoothing-only preconditioner). Needs n divisible by 16.
     void set_preconditioner(unet::UNet* net);
+    // Obstacle mask (n^3, x fastest, nonzero = solid; null clears) for every
+    // later projection of this simulation; needs the mixed-precision solver.
+    void set_solid(const uint8_t* mask);
     unet::UNet* preconditioner() const { return coarse_; }
     Workspace& workspace() { return ws_; }
 
