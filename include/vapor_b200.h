@@ -522,6 +522,55 @@ vapor_status vapor_stage_solve_rhs(vapor_stage *stage, const float *rhs,
 vapor_status vapor_stage_train_network(vapor_stage *stage, vapor_unet *net, float learning_rate,
                                        double *loss);
 
+/* ---- MAC 2D smoke solver (src/solvers/mac2d/MacGridFluidSolver2D.cpp) ----
+ * The reference's 2D solver on the device: closed square box, semi-Lagrangian
+ * advection with clamped bilinear sampling (SemiLagrangian2D.cpp:13-50),
+ * buoyancy (d^1/4 averaged onto the v faces), replenished Gaussian emitter,
+ * FP64 red-black SOR projection (CpuPressureSolver2D.cpp:8-82), density
+ * decay exp(-dt decay), and the midpoint-reflection variant
+ * (MacGridFluidSolver2D.cpp:104-128). Layout as MacGridState2D: density
+ * n^2 (x fastest), u (n+1) x n (idX = x + (n+1) y), v n x (n+1)
+ * (idY = x + n y). Each call waits for its work. */
+typedef struct vapor_mac2d vapor_mac2d;
+/* MacGridParameters2D (MacGridFluidSolver2D.hpp:5-15). */
+typedef struct vapor_mac2d_params {
+    int32_t reflection;            /* 0: simple step, 1: midpoint reflection */
+    float source_strength;
+    float emitter_kick_multiplier;
+    float emitter_radius;          /* fraction of the box */
+    float emitter_center_x, emitter_center_y;
+    float buoyancy;
+    float smoke_decay;
+    float sor_omega;
+    int32_t project_iterations;    /* SOR iteration budget of each projection */
+} vapor_mac2d_params;
+/* The struct's defaults (MacGridFluidSolver2D.hpp:5-15). */
+vapor_status vapor_mac2d_default_params(vapor_mac2d_params *out);
+/* The scene of the default-constructed solver (MacGridFluidSolver2D.cpp:8-14:
+ * radius .04, strength 1, buoyancy .8, decay .3007525, 120 iterations). */
+vapor_status vapor_mac2d_plume_params(vapor_mac2d_params *out);
+/* MacGridFluidSolver2D(resolution, boxSize) + its parameters; zero state. */
+vapor_status vapor_mac2d_create(int32_t n, float box, const vapor_mac2d_params *params, vapor_mac2d **out);
+vapor_status vapor_mac2d_destroy(vapor_mac2d *sim);
+vapor_status vapor_mac2d_get_params(const vapor_mac2d *sim, vapor_mac2d_params *out);
+vapor_status vapor_mac2d_set_params(vapor_mac2d *sim, const vapor_mac2d_params *params);
+/* advance(dt) (MacGridFluidSolver2D.cpp:22-44), with the reference's
+ * argument checks; non-finite fields give VAPOR_NON_FINITE. */
+vapor_status vapor_mac2d_advance(vapor_mac2d *sim, float dt);
+/* resetState() and setBoxSize() (MacGridFluidSolver2D.cpp:130-141). */
+vapor_status vapor_mac2d_reset(vapor_mac2d *sim);
+vapor_status vapor_mac2d_set_box(vapor_mac2d *sim, float box);
+/* Host arrays in the layout above; any pointer may be NULL to skip it. */
+vapor_status vapor_mac2d_upload(vapor_mac2d *sim, const float *density, const float *u, const float *v);
+vapor_status vapor_mac2d_download(vapor_mac2d *sim, float *density, float *u, float *v);
+/* lastProjection() / midpointProjection(): the step's final projection and,
+ * with reflection, the midpoint one (zero otherwise). */
+vapor_status vapor_mac2d_last_projection(vapor_mac2d *sim, vapor_projection_result *out);
+vapor_status vapor_mac2d_midpoint_projection(vapor_mac2d *sim, vapor_projection_result *out);
+/* diagnostics() (MacGridFluidSolver2D.cpp:142-153): FP64 kinetic energy
+ * summed in the reference's order, max |velocity|, max |div|. */
+vapor_status vapor_mac2d_diagnostics(vapor_mac2d *sim, vapor_fluid_diagnostics *out);
+
 #ifdef __cplusplus
 }
 #endif

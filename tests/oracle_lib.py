@@ -351,3 +351,78 @@ def render_volume(n, box, density, params):
     rgb = np.zeros((params.height, params.width, 3), np.float32)
     oracle().vo_render_volume(n, box, np.ascontiguousarray(density, np.float32), C.addressof(params), rgb)
     return rgb
+
+
+# ---- the reference's MAC 2D solver (oracle/_ref/libvapor_ref2d.so) ----
+
+REF2D_SO = os.path.join(ROOT, "oracle", "_ref", "libvapor_ref2d.so")
+_ref2d = None
+
+
+def ref2d_available():
+    return os.path.exists(REF2D_SO)
+
+
+def _ref2d_lib():
+    global _ref2d
+    if _ref2d is None:
+        from vapor_b200.abi import Mac2DParams
+        lib = C.CDLL(REF2D_SO)
+
+        def f(name, res, *args):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = list(args)
+        f("ref2_create", _vp, C.c_int, C.c_float, _vp, _vp, _vp)
+        f("ref2_destroy", None, _vp)
+        f("ref2_set_params", None, _vp, C.POINTER(Mac2DParams))
+        f("ref2_advance", C.c_int, _vp, C.c_float)
+        f("ref2_get_fields", None, _vp, _vp, _vp, _vp)
+        f("ref2_last_projection", None, _vp, C.POINTER(ProjectionResult))
+        f("ref2_midpoint_projection", None, _vp, C.POINTER(ProjectionResult))
+        f("ref2_diagnostics", None, _vp, C.POINTER(FluidDiagnostics))
+        _ref2d = lib
+    return _ref2d
+
+
+class RefSim2D:
+    """The reference's MacGridFluidSolver2D on a given state (CPU)."""
+
+    def __init__(self, n, box, params, density=None, u=None, v=None):
+        from vapor_b200.abi import field_shapes_2d
+        self.n = n
+        self.lib = _ref2d_lib()
+        keep = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (density, u, v)]
+        self.h = self.lib.ref2_create(n, box, *[None if a is None else a.ctypes.data for a in keep])
+        if not self.h:
+            raise ValueError("the reference rejected the 2D grid")
+        self.lib.ref2_set_params(self.h, C.byref(params))
+        self.shapes = field_shapes_2d(n)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref2_destroy(self.h)
+            self.h = None
+
+    def advance(self, dt):
+        return self.lib.ref2_advance(self.h, dt)
+
+    def fields(self):
+        out = [np.zeros(s, np.float32) for s in self.shapes]
+        self.lib.ref2_get_fields(self.h, *[a.ctypes.data for a in out])
+        return out
+
+    def last_projection(self):
+        r = ProjectionResult()
+        self.lib.ref2_last_projection(self.h, C.byref(r))
+        return r
+
+    def midpoint_projection(self):
+        r = ProjectionResult()
+        self.lib.ref2_midpoint_projection(self.h, C.byref(r))
+        return r
+
+    def diagnostics(self):
+        d = FluidDiagnostics()
+        self.lib.ref2_diagnostics(self.h, C.byref(d))
+        return d

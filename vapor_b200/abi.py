@@ -174,3 +174,16 @@ def field_sizes(n):
 def field_shapes(n):
     """numpy shapes (z, y, x) of density, u, v, w in the reference layout."""
     return (n, n, n), (n, n, n + 1), (n, n + 1, n), (n + 1, n, n)
+
+
+class Mac2DParams(C.Structure):
+    """vapor_mac2d_params (MacGridParameters2D, MacGridFluidSolver2D.hpp:5-15)."""
+    _fields_ = [("reflection", C.c_int32), ("source_strength", C.c_float),
+                ("emitter_kick_multiplier", C.c_float), ("emitter_radius", C.c_float),
+                ("emitter_center_x", C.c_float), ("emitter_center_y", C.c_float), ("buoyancy", C.c_float),
+                ("smoke_decay", C.c_float), ("sor_omega", C.c_float), ("project_iterations", C.c_int32)]
+
+
+def field_shapes_2d(n):
+    """numpy shapes (y, x) of density, u, v of the MAC 2D state (MacGridState2D.hpp:7)."""
+    return (n, n), (n, n + 1), (n + 1, n)
