@@ -427,6 +427,12 @@ vapor_status vapor_tune_conv_kernel(int32_t kind);
  * the accepted answer (the stopping test is the FP64 residual). Process-wide;
  * set it before recording steps. */
 vapor_status vapor_tune_fpcg_smoothing(int32_t sweeps, float omega);
+/* Tuning (extension): the kernel of the network's weight gradients in
+ * training: 1 (default) tcgen05 implicit GEMM (M = 8 taps x 16 output
+ * channels, N = input channels, K = voxels), 0 the CUDA-core form. Both add
+ * FP32 products of the same BF16 values with atomics: equal to FP32
+ * rounding. */
+vapor_status vapor_tune_wgrad_kernel(int32_t kind);
 vapor_status vapor_fpcg_smoothing(int32_t *sweeps, float *omega);
 
 /* ---- Batched scenes (extension, no reference counterpart) ----

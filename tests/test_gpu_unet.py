@@ -247,7 +247,18 @@ def test_bounded_wait_that_runs_out_reports_an_error_and_recovers(ws):
 
 
 def test_gradients_match_torch_autograd():
-    """dL/dparams for L = sum(out * g) against PyTorch autograd in FP32."""
+    """dL/dparams for L = sum(out * g) against PyTorch autograd in FP32, with
+    a smooth upstream gradient g. The reference mirrors the BF16 storage of
+    activations and activation gradients, but rounding flips still differ
+    (the forward outputs agree to 2e-2): measured per layer, the weight
+    gradients agree within 4.8 % (relative L2, cosine >= 0.9988; the first
+    layer, farthest from the output, is the worst), the bias gradients within
+    3 % and the head within 0.2 %; the bounds below are about 1.5x those. (A
+    white-noise g cancels in the voxel sums and magnifies the same noise to
+    ~7 %.) The
+    kernels themselves are pinned tighter: the tensor-core weight gradient
+    equals the CUDA-core one to 1e-5, and the convolutions equal the
+    reference's to BF16 rounding."""
     import torch
     n = 16
     net = Net(seed=5)
@@ -256,7 +267,9 @@ def test_gradients_match_torch_autograd():
     xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
     out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
     vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
-    g = np.random.default_rng(1).standard_normal(n ** 3).astype(np.float32) / n ** 3
+    zz, yy, xx = np.meshgrid(*[np.arange(n)] * 3, indexing="ij")
+    g = (np.cos(2 * np.pi * xx / n) * np.sin(2 * np.pi * yy / n + 0.3) + 0.5 * np.cos(2 * np.pi * zz / n))
+    g = (g / n ** 3).astype(np.float32).reshape(-1)
     gdev = torch.tensor(g).cuda()
     grads = np.zeros(net.P, np.float32)
     vb.check(net.lib.vapor_unet_backward(net.h, n, gdev.data_ptr(), grads.ctypes.data))
@@ -269,11 +282,11 @@ def test_gradients_match_torch_autograd():
         rw = ws[i].grad.numpy()
         cos = float((w_g * rw).sum() / (np.linalg.norm(w_g) * np.linalg.norm(rw) + 1e-30))
         rel = float(np.linalg.norm(w_g - rw) / (np.linalg.norm(rw) + 1e-30))
-        assert cos > 0.995 and rel < 0.1, (i, cos, rel)  # BF16 storage: ~1e-2 per layer
         rb = bs[i].grad.numpy()
-        assert np.linalg.norm(b_g - rb) <= 0.1 * np.linalg.norm(rb) + 1e-7, i
+        relb = float(np.linalg.norm(b_g - rb) / (np.linalg.norm(rb) + 1e-30))
+        assert cos > 0.998 and rel < 0.075 and relb < 0.05, (i, cos, rel, relb)
     head = grads[-17:-1]
-    assert np.linalg.norm(head - hw.grad.numpy()) <= 0.05 * np.linalg.norm(hw.grad.numpy())
+    assert np.linalg.norm(head - hw.grad.numpy()) <= 0.003 * np.linalg.norm(hw.grad.numpy())
 
 
 def _plume(n, rel=1e-6):
@@ -317,3 +330,42 @@ def test_training_reduces_the_loss_on_one_scene():
     # the network handle stays usable after its simulation is gone
     sim.close()
     assert np.isfinite(net.parameters()).all()
+
+
+@pytest.mark.parametrize("n", [8, 16, 32])
+def test_tensor_core_weight_gradients_equal_the_cuda_core_form(n):
+    """The tcgen05 weight gradient (M = 8 taps x 16 output channels, N = input
+    channels, K = voxels) against the CUDA-core kernel on the same backward
+    pass: both add FP32 products of the same BF16 values, in different
+    orders, so every parameter gradient agrees to FP32 rounding (max
+    difference within 1e-5 of the largest gradient); the bias and head
+    gradients, which neither touches (but which accumulate with atomics in
+    no fixed order), agree to the same bar."""
+    import torch
+    net = Net(seed=19)
+    x = features(n, 29)
+    xin = torch.tensor(x).to(torch.bfloat16).cuda().contiguous()
+    g = torch.tensor(np.random.default_rng(4).standard_normal(n ** 3).astype(np.float32)).cuda()
+    grads = []
+    try:
+        for kind in (0, 1):
+            vb.tune_wgrad_kernel(kind)
+            out = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+            vb.check(net.lib.vapor_unet_forward_features(net.h, n, xin.data_ptr(), out.data_ptr()))
+            gp = np.zeros(net.P, np.float32)
+            vb.check(net.lib.vapor_unet_backward(net.h, n, g.data_ptr(), gp.ctypes.data))
+            grads.append(gp)
+    finally:
+        vb.tune_wgrad_kernel(1)
+    a, b = grads
+    assert np.abs(a).max() > 0
+    off = 0
+    for cin, cout in LAYERS:
+        w = slice(off, off + 27 * cout * cin)
+        off += 27 * cout * cin
+        scale = max(1e-30, float(np.abs(a[w]).max()))
+        assert np.abs(a[w] - b[w]).max() <= 1e-5 * scale, (cin, cout)
+        bias = slice(off, off + cout)
+        assert np.abs(a[bias] - b[bias]).max() <= 1e-5 * max(1e-30, float(np.abs(a[bias]).max()))
+        off += cout
+    assert np.abs(a[off:] - b[off:]).max() <= 1e-5 * max(1e-30, float(np.abs(a[off:]).max()))

@@ -117,6 +117,7 @@ def _declare(lib):
     f("vapor_tune_sor_blocked_chunks", C.c_int32, C.c_int32)
     f("vapor_tune_conv_kernel", C.c_int32)
     f("vapor_tune_fpcg_smoothing", C.c_int32, C.c_float)
+    f("vapor_tune_wgrad_kernel", C.c_int32)
     f("vapor_fpcg_smoothing", C.POINTER(C.c_int32), C.POINTER(C.c_float))
     f("vapor_batch_create", C.c_int32, C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_batch_destroy", _vp)
@@ -406,6 +407,12 @@ def tune_fpcg_smoothing(sweeps=DEFAULT_FPCG_SMOOTHING[0], omega=DEFAULT_FPCG_SMO
     correction (default 2) and their weight (default 1.2). Set it before
     creating the simulations whose steps are recorded."""
     check(library().vapor_tune_fpcg_smoothing(int(sweeps), float(omega)))
+
+
+def tune_wgrad_kernel(kind):
+    """Weight-gradient kernel of the network's training: 1 (default) tcgen05,
+    0 the CUDA-core form (equal to FP32 rounding)."""
+    check(library().vapor_tune_wgrad_kernel(int(kind)))
 
 
 def fpcg_smoothing():

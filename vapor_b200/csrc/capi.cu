@@ -336,6 +336,9 @@ VB_API vapor_status vapor_tune_conv_kernel(int32_t kind) {
         vb::unet::set_conv_kernel(kind);
     });
 }
+VB_API vapor_status vapor_tune_wgrad_kernel(int32_t kind) {
+    return guarded([&] { vb::unet::set_wgrad_kernel(kind); });
+}
 VB_API vapor_status vapor_tune_fpcg_smoothing(int32_t sweeps, float omega) {
     return guarded([&] { vb::set_fpcg_smoothing(sweeps, omega); });
 }

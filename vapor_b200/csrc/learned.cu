@@ -223,6 +223,7 @@ static void layer_backward(UNet& net, int layer, int D, int H, int W, const __nv
     wa.cout = cout;
     wa.cin = cin;
     wa.dw = grad + weight_offset(layer);
+    wa.error = error;
     launch_conv3_wgrad(wa, s);
     launch_bias_grad(V, cout, g, g_stride, g_offset, grad + bias_offset(layer), s);
     if (!dx) return;

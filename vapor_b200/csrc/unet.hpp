@@ -48,6 +48,7 @@ struct WGradArgs {
     int x_stride;
     int cout, cin;           // multiples of 16
     float* dw;               // [27][cout][cin], accumulated
+    unsigned int* error;     // tensor-core form: bit 1 a bounded wait timed out (may be null for the other form)
 };
 
 // Sets the kernels' shared-memory limits (once per device, before use).
@@ -64,6 +65,10 @@ void set_conv_kernel(int kind);
 void launch_pack_window(int cout, int cin, const __nv_bfloat16* w, __nv_bfloat16* packed, cudaStream_t s);
 void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s);
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s);
+// Weight-gradient kernel: 1 (default) tcgen05 implicit GEMM, 0 the CUDA-core
+// form. Both accumulate FP32 products of the same BF16 values with atomics,
+// so they agree to FP32 rounding.
+void set_wgrad_kernel(int kind);
 void launch_prep_input(int n, const float* b_split, const ProjControl* ctrl, double* partial, float* scale,
                        __nv_bfloat16* out, cudaStream_t s);
 // Features from a natural-layout FP32 field: channel 0 = (a - mean) / rms.

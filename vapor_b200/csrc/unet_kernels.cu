@@ -1371,6 +1371,146 @@ __global__ void __launch_bounds__(256) k_conv3_wgrad(WGradArgs a) {
     atomicAdd(&a.dw[(long(tap) * a.cout + cob * 16 + tco) * a.cin + cib * 16 + tci], acc);
 }
 
+// Weight gradient on the tensor cores. dW[t][co][ci] = sum over voxels v of
+// g[v][co] x[v + t][ci], written as sum over v' of g[v' - t][co] x[v'][ci], is
+// a GEMM per CTA: M = 128 rows (8 taps x 16 output channels of one chunk), N
+// = cin, K = the voxels of the CTA's range. Shared memory holds, per stage
+// of 64 voxels, A[(tap, co)][v'] = g[v' - t][co] (zero where v' - t leaves
+// the grid) and B[ci][v'] = x[v'][ci], both in the canonical K-major layout
+// without swizzle ([8-row group][8-voxel chunk][8 rows][16 B]: LBO 128 B, SBO
+// 1024 B), staged by all threads (each voxel's channels scattered down one K
+// column); one thread issues the 4 MMAs (K = 16) of a stage into the FP32
+// TMEM accumulator, two stages alternate on commit barriers. The epilogue
+// adds the accumulator to dW with FP32 atomics, as the CUDA-core form does.
+struct WGradTc {
+    static constexpr int kK = 64;                 // voxels per stage
+    static constexpr int kA = 128 * kK * 2;       // 16 KB
+    __host__ __device__ static int b_bytes(int cin) { return cin * kK * 2; }
+    __host__ __device__ static int stage(int cin) { return kA + b_bytes(cin); }
+    static int smem(int cin) { return 2 * stage(cin) + 1024; }
+};
+
+__device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
+    return uint32_t((row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__global__ void __launch_bounds__(256) k_conv3_wgrad_tc(WGradArgs a, long chunk) {
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int group = blockIdx.y;                     // taps 8 group .. 8 group + 7
+    const int cob = blockIdx.z;                       // output channels 16 cob .. + 15
+    const long V = long(a.D) * a.H * a.W;
+    const long v_begin = long(blockIdx.x) * chunk, v_end = min(V, v_begin + chunk);
+    const int cin = a.cin;
+    const uint32_t ncols = cin <= 32 ? 32u : (cin <= 64 ? 64u : 128u);
+    const uint32_t sbase = tc::smem_addr(smem);
+    const uint32_t bar0 = tc::smem_addr(&bars[0]);
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(&tmem_slot), ncols);
+    if (tid == 0) {
+        tc::mbar_init(bar0, 1);
+        tc::mbar_init(bar0 + 8, 1);
+        tc::fence_mbarrier_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = tc::instr_desc_bf16(128, cin);
+    int issued[2] = {0, 0};
+    bool ok = true;
+    int s_idx = 0;
+    for (long k0 = v_begin; k0 < v_end; k0 += WGradTc::kK, s_idx ^= 1) {
+        uint8_t* st = smem + s_idx * WGradTc::stage(cin);
+        const uint32_t sa = sbase + uint32_t(s_idx * WGradTc::stage(cin));
+        // the MMAs that last read this stage must be done
+        if (issued[s_idx] > 0) {
+            const bool mine = tc::mbar_wait(bar0 + 8u * s_idx, uint32_t(issued[s_idx] - 1) & 1u, kWaitLimit);
+            if (!__syncthreads_and(mine)) {
+                ok = false;
+                break;
+            }
+        }
+        // A: (tap j, voxel k) -> 16 channels of g at v' - t
+        for (int i = tid; i < 8 * WGradTc::kK; i += blockDim.x) {
+            const int j = i / WGradTc::kK, k = i - j * WGradTc::kK;
+            const int t = group * 8 + j;
+            const long v = k0 + k;
+            uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+            if (t < 27 && v < v_end) {
+                int x, y, z;
+                decode(v, a.H, a.W, x, y, z);
+                const int xs = x - (t % 3 - 1), ys = y - ((t / 3) % 3 - 1), zs = z - (t / 9 - 1);
+                if (xs >= 0 && xs < a.W && ys >= 0 && ys < a.H && zs >= 0 && zs < a.D) {
+                    const uint4* src = reinterpret_cast<const uint4*>(
+                        a.g + ((long(zs) * a.H + ys) * a.W + xs) * a.g_stride + a.g_offset + cob * 16);
+                    lo = src[0];
+                    hi = src[1];
+                }
+            }
+            const uint16_t* e0 = reinterpret_cast<const uint16_t*>(&lo);
+            const uint16_t* e1 = reinterpret_cast<const uint16_t*>(&hi);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                *reinterpret_cast<uint16_t*>(st + kmajor_offset(j * 16 + c, k)) = e0[c];
+                *reinterpret_cast<uint16_t*>(st + kmajor_offset(j * 16 + 8 + c, k)) = e1[c];
+            }
+        }
+        // B: (8-channel group, voxel k) -> x at v'
+        uint8_t* sb = st + WGradTc::kA;
+        for (int i = tid; i < (cin / 8) * WGradTc::kK; i += blockDim.x) {
+            const int cg = i / WGradTc::kK, k = i - cg * WGradTc::kK;
+            const long v = k0 + k;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (v < v_end) val = *reinterpret_cast<const uint4*>(a.x + v * a.x_stride + cg * 8);
+            const uint16_t* e = reinterpret_cast<const uint16_t*>(&val);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) *reinterpret_cast<uint16_t*>(sb + kmajor_offset(cg * 8 + c, k)) = e[c];
+        }
+        tc::fence_proxy_async();  // generic-proxy stores visible to the tensor core
+        tc::tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            const uint64_t ad = tc::smem_desc(sa, 128, 1024);
+            const uint64_t bd = tc::smem_desc(sa + WGradTc::kA, 128, 1024);
+#pragma unroll
+            for (int kk = 0; kk < WGradTc::kK / 16; ++kk)
+                tc::mma_bf16(tmem, ad + uint32_t(kk * 16), bd + uint32_t(kk * 16), idesc, k0 > v_begin || kk > 0);
+            tc::mma_commit(bar0 + 8u * s_idx);
+        }
+        ++issued[s_idx];
+    }
+    // the last commit of each stage covers every earlier MMA
+    bool drained = true;
+    for (int k = 0; k < 2; ++k)
+        if (issued[k] > 0) drained &= tc::mbar_wait(bar0 + 8u * k, uint32_t(issued[k] - 1) & 1u, kWaitLimit);
+    ok = __syncthreads_and(ok && drained) != 0;
+    tc::tc_fence_after();
+    if (ok && v_begin < v_end) {
+        // rows (tap j, co) on TMEM lanes; columns ci, half of them per warp pair
+        const int q = warp & 3, hlf = warp >> 2;
+        const int row = q * 32 + lane;
+        const int t = group * 8 + row / 16, co = cob * 16 + (row & 15);
+        const int half = cin / 2;
+        for (int c0 = hlf * half; c0 < (hlf + 1) * half; c0 += 8) {
+            float val[8];
+            tc::tmem_ld8(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), val);
+            if (t < 27) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) atomicAdd(&a.dw[(long(t) * a.cout + co) * cin + c0 + c], val[c]);
+            }
+        }
+    } else if (!ok && tid == 0 && a.error) {
+        atomicOr(a.error, drained ? 1u : 3u);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
 // Flip and transpose 3x3x3 weights for the input-gradient convolution:
 // wt[26 - tap][ci][co] = w[tap][co][ci] (BF16).
 __global__ void k_flip_weights(int cout, int cin, const __nv_bfloat16* __restrict__ w,
@@ -1624,6 +1764,7 @@ void set_conv_kernel(int kind) {
 }
 
 void configure_conv_kernels() {
+    VB_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WGradTc::smem(96)));
     configure_n<16>();
     configure_n<32>();
     configure_n<48>();
@@ -1647,8 +1788,28 @@ void launch_conv3(const ConvArgs& a, int cout, cudaStream_t s) {
     }
 }
 
+std::atomic<int> g_wgrad_kind{1};
+
+void set_wgrad_kernel(int kind) {
+    if (kind < 0 || kind > 1) fail(VAPOR_INVALID_ARGUMENT, "weight-gradient kernel: 0 or 1");
+    g_wgrad_kind.store(kind);
+}
+
 void launch_conv3_wgrad(const WGradArgs& a, cudaStream_t s) {
     const long V = long(a.D) * a.H * a.W;
+    if (g_wgrad_kind.load() == 1 && a.cin <= 96 && a.cout % 16 == 0 && a.cin % 16 == 0 &&
+        a.g_stride % 8 == 0 && a.g_offset % 8 == 0 && a.x_stride % 8 == 0) {
+        // voxel ranges: about two waves of CTAs over the tap groups and
+        // output-channel chunks, at least one stage of voxels each
+        const int others = 4 * (a.cout / 16);
+        const long target = std::max<long>(1, (2L * device_sm_count() + others - 1) / others);
+        const long chunk = std::max<long>(WGradTc::kK, ((V + target - 1) / target + WGradTc::kK - 1) /
+                                                           WGradTc::kK * WGradTc::kK);
+        const dim3 grid(unsigned((V + chunk - 1) / chunk), 4, unsigned(a.cout / 16));
+        count_launch();
+        k_conv3_wgrad_tc<<<grid, 256, WGradTc::smem(a.cin), s>>>(a, chunk);
+        return;
+    }
     const int chunks = int(std::max<long>(1, std::min<long>(V / 4096, 256)));
     const dim3 grid(chunks, 27, (a.cout / 16) * (a.cin / 16));
     count_launch();
