@@ -577,6 +577,47 @@ vapor_status vapor_mac2d_midpoint_projection(vapor_mac2d *sim, vapor_projection_
  * summed in the reference's order, max |velocity|, max |div|. */
 vapor_status vapor_mac2d_diagnostics(vapor_mac2d *sim, vapor_fluid_diagnostics *out);
 
+/* ---- MAC 2D reflection solver (src/solvers/mac2d/ReflectionMacFluidSolver2D.hpp) ----
+ * The reference's compatibility solver for the historical 2D plume (unit
+ * box, n in 2..512): semi-Lagrangian velocity, semi-Lagrangian or MacCormack
+ * smoke with its in-place 3x3 limiter, FP32 red-black SOR with a fixed
+ * iteration count, buoyancy d^1/4 split onto both faces of a cell, emitter
+ * with optional random stirring, midpoint reflection every step
+ * (ReflectionMacFluidSolver2D.hpp:32-45, 309-425). Layout as vapor_mac2d;
+ * the pressure is n^2 FP32. Each call waits for its work. */
+typedef struct vapor_mac2d_refl vapor_mac2d_refl;
+/* The solver's public fields (ReflectionMacFluidSolver2D.hpp:19-22, 57-71). */
+typedef struct vapor_mac2d_refl_params {
+    int32_t mac_cormack_smoke;     /* 1: MacCormack smoke, 0: semi-Lagrangian */
+    float source_strength;
+    float buoyancy;
+    float smoke_decay;             /* per second; the step uses exp(-decay / 60) per frame */
+    int32_t project_iterations;    /* red-black SOR iterations, half of them per projection */
+    float emitter_radius;          /* fraction of the box */
+    float emitter_center_x, emitter_center_y;
+    float emitter_kick_multiplier;
+    float stir_strength;           /* random inlet stirring; 0 keeps the historical replay */
+    float sor_omega;
+    uint32_t random_seed;          /* stirring stream, applied at creation and reset */
+} vapor_mac2d_refl_params;
+/* The struct's defaults (MC smoke, 60 iterations, radius .08). */
+vapor_status vapor_mac2d_refl_default_params(vapor_mac2d_refl_params *out);
+/* The solver built from an advection method (ReflectionMacFluidSolver2D.hpp:77-85:
+ * radius .04, 120 iterations; method VAPOR_SEMI_LAGRANGIAN or
+ * VAPOR_MACCORMACK); its resolution is 128. */
+vapor_status vapor_mac2d_refl_app_params(int32_t method, vapor_mac2d_refl_params *out);
+vapor_status vapor_mac2d_refl_create(int32_t n, const vapor_mac2d_refl_params *params, vapor_mac2d_refl **out);
+vapor_status vapor_mac2d_refl_destroy(vapor_mac2d_refl *sim);
+vapor_status vapor_mac2d_refl_get_params(const vapor_mac2d_refl *sim, vapor_mac2d_refl_params *out);
+vapor_status vapor_mac2d_refl_set_params(vapor_mac2d_refl *sim, const vapor_mac2d_refl_params *params);
+vapor_status vapor_mac2d_refl_advance(vapor_mac2d_refl *sim, float dt);
+/* resetState(): zero fields, stirring stream back to the seed. */
+vapor_status vapor_mac2d_refl_reset(vapor_mac2d_refl *sim);
+/* Host arrays; any pointer may be NULL to skip it (pressure: download only). */
+vapor_status vapor_mac2d_refl_upload(vapor_mac2d_refl *sim, const float *smoke, const float *u, const float *v);
+vapor_status vapor_mac2d_refl_download(vapor_mac2d_refl *sim, float *smoke, float *u, float *v, float *pressure);
+vapor_status vapor_mac2d_refl_diagnostics(vapor_mac2d_refl *sim, vapor_fluid_diagnostics *out);
+
 #ifdef __cplusplus
 }
 #endif

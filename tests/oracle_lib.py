@@ -381,6 +381,19 @@ def _ref2d_lib():
         f("ref2_last_projection", None, _vp, C.POINTER(ProjectionResult))
         f("ref2_midpoint_projection", None, _vp, C.POINTER(ProjectionResult))
         f("ref2_diagnostics", None, _vp, C.POINTER(FluidDiagnostics))
+        from vapor_b200.abi import Mac2DReflParams
+        R = C.POINTER(Mac2DReflParams)
+        f("ref2r_create", _vp, C.c_int, R)
+        f("ref2r_create_app", _vp, C.c_int)
+        f("ref2r_destroy", None, _vp)
+        f("ref2r_resolution", C.c_int, _vp)
+        f("ref2r_get_params", None, _vp, R)
+        f("ref2r_set_params", None, _vp, R)
+        f("ref2r_reset", None, _vp)
+        f("ref2r_set_fields", None, _vp, _vp, _vp, _vp)
+        f("ref2r_advance", C.c_int, _vp, C.c_float)
+        f("ref2r_get_fields", None, _vp, _vp, _vp, _vp, _vp)
+        f("ref2r_diagnostics", None, _vp, C.POINTER(FluidDiagnostics))
         _ref2d = lib
     return _ref2d
 
@@ -425,4 +438,58 @@ class RefSim2D:
     def diagnostics(self):
         d = FluidDiagnostics()
         self.lib.ref2_diagnostics(self.h, C.byref(d))
+        return d
+
+
+class RefReflection2D:
+    """The reference's ReflectionMacFluidSolver2D (CPU): resolution n with the
+    given fields, or (n None) the solver built from an advection method."""
+
+    def __init__(self, n, params=None, method=None):
+        from vapor_b200.abi import field_shapes_2d
+        self.lib = _ref2d_lib()
+        if n is None:
+            self.h = self.lib.ref2r_create_app(int(method))
+        else:
+            self.h = self.lib.ref2r_create(int(n), None if params is None else C.byref(params))
+        if not self.h:
+            raise ValueError("the reference rejected the reflection solver")
+        self.n = self.lib.ref2r_resolution(self.h)
+        self.shapes = field_shapes_2d(self.n) + ((self.n, self.n),)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref2r_destroy(self.h)
+            self.h = None
+
+    @property
+    def params(self):
+        from vapor_b200.abi import Mac2DReflParams
+        p = Mac2DReflParams()
+        self.lib.ref2r_get_params(self.h, C.byref(p))
+        return p
+
+    @params.setter
+    def params(self, p):
+        self.lib.ref2r_set_params(self.h, C.byref(p))
+
+    def reset(self):
+        self.lib.ref2r_reset(self.h)
+
+    def set_fields(self, smoke=None, u=None, v=None):
+        keep = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (smoke, u, v)]
+        self.lib.ref2r_set_fields(self.h, *[None if a is None else a.ctypes.data for a in keep])
+
+    def advance(self, dt):
+        return self.lib.ref2r_advance(self.h, dt)
+
+    def fields(self):
+        """smoke, u, v, pressure."""
+        out = [np.zeros(s, np.float32) for s in self.shapes]
+        self.lib.ref2r_get_fields(self.h, *[a.ctypes.data for a in out])
+        return out
+
+    def diagnostics(self):
+        d = FluidDiagnostics()
+        self.lib.ref2r_diagnostics(self.h, C.byref(d))
         return d

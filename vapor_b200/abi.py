@@ -184,6 +184,16 @@ class Mac2DParams(C.Structure):
                 ("smoke_decay", C.c_float), ("sor_omega", C.c_float), ("project_iterations", C.c_int32)]
 
 
+class Mac2DReflParams(C.Structure):
+    """vapor_mac2d_refl_params (the public fields of ReflectionMacFluidSolver2D,
+    ReflectionMacFluidSolver2D.hpp:19-22, 57-71)."""
+    _fields_ = [("mac_cormack_smoke", C.c_int32), ("source_strength", C.c_float), ("buoyancy", C.c_float),
+                ("smoke_decay", C.c_float), ("project_iterations", C.c_int32), ("emitter_radius", C.c_float),
+                ("emitter_center_x", C.c_float), ("emitter_center_y", C.c_float),
+                ("emitter_kick_multiplier", C.c_float), ("stir_strength", C.c_float), ("sor_omega", C.c_float),
+                ("random_seed", C.c_uint32)]
+
+
 def field_shapes_2d(n):
     """numpy shapes (y, x) of density, u, v of the MAC 2D state (MacGridState2D.hpp:7)."""
     return (n, n), (n, n + 1), (n + 1, n)

@@ -17,9 +17,9 @@
 //     kinetic energy likewise;
 //   - the emitter's Gaussian weights exp(-3.5 q) and the decay exp(-dt k)
 //     are evaluated on the host with the C library, as the reference does;
-//   - buoyancy's d^(1/4) is the correctly rounded value (two FP64 square
-//     roots, then one rounding to FP32), which the C library's powf returns
-//     except in rare near-halfway cases.
+//   - buoyancy's d^(1/4) is the C library's powf(d, .25f) bit for bit
+//     (powf_quarter.cuh: the correctly rounded root corrected by a table of
+//     the library's one-ulp differences).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "powf_quarter.cuh"
 
 namespace vb {
 namespace {
@@ -118,12 +119,11 @@ __global__ void k2_decay(long count, float decay, const float* __restrict__ next
 
 // Buoyancy on the interior v faces (MacGridFluidSolver2D.cpp:75-86):
 // v += (dt buoyancy) (.5 (d_below^1/4 + d_above^1/4)).
-__device__ __forceinline__ float quarter_power(float d) { return float(sqrt(sqrt(double(d)))); }
 __global__ void k2_buoyancy(int n, float dt_buoyancy, const float* __restrict__ d, float* __restrict__ v) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= long(n) * (n - 1)) return;
     const int y = int(i / n) + 1, x = int(i - long(y - 1) * n);
-    const float smoke = .5f * (quarter_power(d[x + size_t(n) * (y - 1)]) + quarter_power(d[x + size_t(n) * y]));
+    const float smoke = .5f * (powf_quarter(d[x + size_t(n) * (y - 1)]) + powf_quarter(d[x + size_t(n) * y]));
     v[x + size_t(n) * y] += dt_buoyancy * smoke;
 }
 
