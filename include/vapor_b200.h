@@ -618,6 +618,100 @@ vapor_status vapor_mac2d_refl_upload(vapor_mac2d_refl *sim, const float *smoke, 
 vapor_status vapor_mac2d_refl_download(vapor_mac2d_refl *sim, float *smoke, float *u, float *v, float *pressure);
 vapor_status vapor_mac2d_refl_diagnostics(vapor_mac2d_refl *sim, vapor_fluid_diagnostics *out);
 
+/* ---- Simplicial 3D compute stages (src/solvers/simplicial3d/SimplicialCompute3D.hpp:7-13) ----
+ * The reference's optional compute backend of SimplicialFluidSolver3D
+ * (its OpenGL GpuSimplicial3D, gpu/GpuSimplicial3D.cpp) on the device, FP64:
+ * the circulation advection (trace every dual vertex by the midpoint rule,
+ * integrate the dual edges, sum each primal edge's dual face), the smoke
+ * advection with decay (trace every primal vertex, interpolate the vertex
+ * smoke) and the flux recovery (CG on the Dirichlet potential operator of
+ * SimplicialFluidSolver3D::laplacian, preconditioned as the CPU solver
+ * preconditions it: its IC(0) factor or its diagonal). The sampling
+ * keeps the CPU solver's operation order: traces, velocities, circulations
+ * and smoke equal the CPU's bit for bit (box nearest-site search by a scan;
+ * the descent search and general domains follow the same arithmetic).
+ * vapor_b200/host/VaporSimplicial3D.hpp flattens a solver into this struct
+ * and implements SimplicialCompute3D on these calls. Each call waits for
+ * its work. */
+typedef struct vapor_simplicial3d vapor_simplicial3d;
+typedef struct vapor_simplicial3d_mesh {
+    int32_t box_domain;              /* Mesh::boxDomain: Voronoi-cell interpolation; 0: subdivision */
+    int32_t bins;                    /* spatial bins per axis (0: none, one list of all items) */
+    double size;                     /* Mesh::size */
+    int32_t n_primal, n_dual, n_nodes, n_edges, n_dual_edges, n_tets, n_faces;
+    int32_t n_planes, n_corners, n_cones, n_subtets;
+    const double *dual_position;     /* 3 n_dual: dual vertices */
+    const double *node_position;     /* 3 n_nodes: box: the primal vertices; domain: subdivision nodes */
+    const double *tet_geometry;      /* 12 n_tets: vertex 0, barycentric gradients 1..3 */
+    const int32_t *tet_vertices;     /* 4 n_tets */
+    const int32_t *dual_hint;        /* n_dual: a tet near each dual vertex, or -1 */
+    const int32_t *primal_hint;      /* n_primal: a tet of each primal vertex */
+    const int32_t *bin_offsets;      /* max(1, bins^3) + 1 */
+    const int32_t *bin_items;        /* tets per bin */
+    const int32_t *wall_offsets;     /* max(1, bins^3) + 1 */
+    const int32_t *wall_items;       /* boundary faces per bin */
+    const double *wall_geometry;     /* 6 n_faces: outward area normal, first vertex */
+    const int32_t *wall_owner;       /* n_faces: the tet on the inner side */
+    const double *box_planes;        /* 4 n_planes: Voronoi cell planes (normal, offset) */
+    const int32_t *cell_corners;     /* n_primal + 1 */
+    const int32_t *corner_vertices;  /* n_corners: dual vertex of each cell corner */
+    const int32_t *corner_cones;     /* n_corners + 1 */
+    const int32_t *cone_planes;      /* 3 n_cones */
+    const int32_t *neighbor_offsets; /* n_primal + 1: Delaunay neighbours */
+    const int32_t *neighbors;
+    const int32_t *sub_offsets;      /* n_tets + 1: circumcentric subtets (domain) */
+    const int32_t *sub_nodes;        /* 4 n_subtets */
+    const double *sub_gradients;     /* 9 n_subtets */
+    const int32_t *loop_offsets;     /* n_edges + 1: each primal edge's dual face */
+    const int32_t *loop_items;       /* sign * (dual edge + 1) */
+    const int32_t *dual_edges;       /* 2 n_dual_edges */
+    /* the Dirichlet potential operator */
+    const int32_t *face_edges;       /* 3 n_faces */
+    const int32_t *face_signs;       /* 3 n_faces */
+    const int32_t *edge_vertices;    /* 2 n_edges */
+    const uint8_t *edge_boundary;    /* n_edges */
+    const uint8_t *vertex_boundary;  /* n_primal */
+    const double *star0;             /* n_primal */
+    const double *star1;             /* n_edges */
+    const double *star2;             /* n_faces */
+    /* the preconditioner of SimplicialFluidSolver3D::solve: its IC(0) factor
+     * when it has one (general domains), else its diagonal (Jacobi) */
+    const double *jacobi_diagonal;   /* n_edges; NULL: the assembled operator's diagonal */
+    const int32_t *ic_offsets;       /* n_edges + 1, or NULL: no factor */
+    const int32_t *ic_columns;       /* strictly lower entries, ascending per row */
+    const double *ic_values;
+    const double *ic_diagonal;       /* n_edges */
+} vapor_simplicial3d_mesh;
+/* Uploads the mesh. site_search: 0 automatic (a scan of all sites up to
+ * 4096 primal vertices, else the descent), 1 scan, 2 descent over Delaunay
+ * neighbours from the sample's tet. dot_order: 0 automatic (index order up
+ * to 262144 edges), 1 index order on one thread (std::inner_product's: the
+ * recovery's iterates equal the CPU solver's bit for bit), 2 a parallel
+ * tree (faster on large meshes; equal to rounding). */
+vapor_status vapor_simplicial3d_create(const vapor_simplicial3d_mesh *mesh, int32_t site_search,
+                                       int32_t dot_order, vapor_simplicial3d **out);
+vapor_status vapor_simplicial3d_destroy(vapor_simplicial3d *stages);
+/* advectCirculation: omega (n_edges) from the dual velocities (3 n_dual) and,
+ * on general domains, the node samples (3 n_nodes; NULL on boxes). */
+vapor_status vapor_simplicial3d_advect_circulation(vapor_simplicial3d *stages, double dt,
+                                                   const double *dual_velocity, const double *node_samples,
+                                                   double *omega);
+/* advectDensity: the vertex smoke (n_primal) traced back by dt, times decay
+ * (the caller's exp(-smokeDecay dt)). */
+vapor_status vapor_simplicial3d_advect_density(vapor_simplicial3d *stages, double dt, double decay,
+                                               const double *dual_velocity, const double *node_samples,
+                                               const float *vertex_density, float *density_out);
+/* recover: x (n_edges) with A x = rhs from x0 (the CPU solver starts from
+ * zero on boxes and from the current potential on general domains),
+ * boundary edges held at zero; stops when the infinity norm of the
+ * residual is at most max(absolute, relative * |rhs|_inf) or after
+ * `iterations`; the final residual is recomputed from x. Invalid controls:
+ * VAPOR_INVALID_ARGUMENT; a non-finite rhs or a lost positive definiteness:
+ * VAPOR_RUNTIME_ERROR (the reference's messages). */
+vapor_status vapor_simplicial3d_recover(vapor_simplicial3d *stages, const double *rhs, const double *x0,
+                                        int32_t iterations, double absolute_tolerance, double relative_tolerance,
+                                        double *x, vapor_linear_solve_result *result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,11 +3,14 @@
 // the header-only ReflectionMacFluidSolver2D.hpp, compiled from where they lie
 // by oracle/Makefile into _ref/libvapor_ref2d.so), so that the tests can step
 // the reference's CPU solvers beside the device ones on the same state and
-// parameters.
+// parameters; and over the reference's historical 2D plume
+// (tests/fixtures/Ba20987Smoke2D.hpp), which its Historical2DTests.cpp
+// replays against the reflection solver.
 #include "../include/vapor_b200.h"
 
 #include "solvers/mac2d/MacGridFluidSolver2D.hpp"
 #include "solvers/mac2d/ReflectionMacFluidSolver2D.hpp"
+#include "fixtures/Ba20987Smoke2D.hpp"
 
 #include <algorithm>
 #include <exception>
@@ -169,4 +172,25 @@ REF2_EXPORT void ref2r_diagnostics(void* h, vapor_fluid_diagnostics* out) {
     out->kinetic_energy = d.kineticEnergy;
     out->max_velocity = d.maxVelocity;
     out->max_divergence = d.maxDivergence;
+}
+
+// ---- the historical plume (Ba20987Smoke2D.hpp), closed walls ----
+// Random stirring is off: the fixture's stirring stream is one process-wide
+// state, so only the first instance of a process could replay it.
+REF2_EXPORT void* ref2h_create(int n) {
+    auto* s = new ba20987::SmokeSim2D(n);
+    s->stirStrength = 0.f;
+    s->openLeft = s->openRight = s->openTop = s->openBottom = false;
+    return s;
+}
+REF2_EXPORT void ref2h_destroy(void* h) { delete static_cast<ba20987::SmokeSim2D*>(h); }
+REF2_EXPORT void ref2h_step(void* h, float dt, float buoyancy, float dissipation, float strength, int iterations) {
+    static_cast<ba20987::SmokeSim2D*>(h)->step(dt, buoyancy, dissipation, strength, iterations);
+}
+REF2_EXPORT void ref2h_get_fields(void* h, float* s, float* u, float* v, float* pressure) {
+    const ba20987::SmokeSim2D& r = *static_cast<ba20987::SmokeSim2D*>(h);
+    std::copy(r.smoke.begin(), r.smoke.end(), s);
+    std::copy(r.vx.begin(), r.vx.end(), u);
+    std::copy(r.vy.begin(), r.vy.end(), v);
+    std::copy(r.pressure.begin(), r.pressure.end(), pressure);
 }

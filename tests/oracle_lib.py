@@ -394,6 +394,10 @@ def _ref2d_lib():
         f("ref2r_advance", C.c_int, _vp, C.c_float)
         f("ref2r_get_fields", None, _vp, _vp, _vp, _vp, _vp)
         f("ref2r_diagnostics", None, _vp, C.POINTER(FluidDiagnostics))
+        f("ref2h_create", _vp, C.c_int)
+        f("ref2h_destroy", None, _vp)
+        f("ref2h_step", None, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int)
+        f("ref2h_get_fields", None, _vp, _vp, _vp, _vp, _vp)
         _ref2d = lib
     return _ref2d
 
@@ -493,3 +497,176 @@ class RefReflection2D:
         d = FluidDiagnostics()
         self.lib.ref2r_diagnostics(self.h, C.byref(d))
         return d
+
+
+class RefHistorical2D:
+    """The reference's historical 2D plume (tests/fixtures/Ba20987Smoke2D.hpp)
+    with closed walls and no stirring, as its Historical2DTests.cpp runs it."""
+
+    def __init__(self, n):
+        from vapor_b200.abi import field_shapes_2d
+        self.lib = _ref2d_lib()
+        self.n = int(n)
+        self.h = self.lib.ref2h_create(self.n)
+        self.shapes = field_shapes_2d(self.n) + ((self.n, self.n),)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref2h_destroy(self.h)
+            self.h = None
+
+    def step(self, dt, buoyancy, dissipation, strength, iterations):
+        self.lib.ref2h_step(self.h, dt, buoyancy, dissipation, strength, iterations)
+
+    def fields(self):
+        """smoke, u, v, pressure."""
+        out = [np.zeros(s, np.float32) for s in self.shapes]
+        self.lib.ref2h_get_fields(self.h, *[a.ctypes.data for a in out])
+        return out
+
+
+# ---- the reference's simplicial 3D solver with the drop-in backend
+#      (oracle/_ref/libvapor_ref_simplicial.so) ----
+
+SIMPLICIAL_SO = os.path.join(ROOT, "oracle", "_ref", "libvapor_ref_simplicial.so")
+SIMPLICIAL_MESHES = os.path.join(ROOT, "oracle", "_ref", "meshes")
+_simplicial = None
+
+
+def simplicial_available():
+    return os.path.exists(SIMPLICIAL_SO) and os.path.isdir(SIMPLICIAL_MESHES)
+
+
+def _simplicial_lib():
+    global _simplicial
+    if _simplicial is None:
+        lib = C.CDLL(SIMPLICIAL_SO)
+
+        def f(name, res, *args):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = list(args)
+        f("rs_error", C.c_char_p)
+        f("rs_create", _vp, C.c_char_p, C.c_int, C.c_double)
+        f("rs_destroy", None, _vp)
+        f("rs_attach", C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp)
+        f("rs_counts", None, _vp, _vp)
+        f("rs_set_potential", C.c_int, _vp, _vp)
+        f("rs_advect_vorticity", C.c_int, _vp, C.c_double)
+        f("rs_advance", C.c_int, _vp, C.c_float)
+        f("rs_set_box_size", C.c_int, _vp, C.c_float)
+        f("rs_reset", C.c_int, _vp)
+        f("rs_set_parameters", None, _vp, C.c_int, C.c_float, C.c_int, C.c_double, C.c_double)
+        for name in ("rs_vorticity", "rs_potential", "rs_flux", "rs_vertex_density", "rs_density",
+                     "rs_edge_midpoints", "rs_diagnostics"):
+            f(name, None, _vp, _vp)
+        f("rs_last_recovery", None, _vp, _vp, _vp, _vp, _vp)
+        f("rs_smoke_center", None, _vp, _vp)
+        f("rs_substeps", C.c_int, _vp)
+        _simplicial = lib
+    return _simplicial
+
+
+class RefSimplicial:
+    """The reference's SimplicialFluidSolver3D on one of its example meshes,
+    with a compute backend: 0 the CPU path, 1 the CUDA stages, 2 the stages'
+    arithmetic on the host with `partner`'s recovery, 3 the CUDA advection
+    with `partner`'s recovery. search: 0 automatic, 1 scan, 2 descent; dots:
+    the recovery's dot order, 0 automatic, 1 index order, 2 tree."""
+
+    CPU, DEVICE, HOST_ADVECTION, DEVICE_ADVECTION = 0, 1, 2, 3
+
+    def __init__(self, mesh="box.tet", box=True, size=1.0):
+        self.lib = _simplicial_lib()
+        self.h = self.lib.rs_create(os.path.join(SIMPLICIAL_MESHES, mesh).encode(), 1 if box else 0, size)
+        if not self.h:
+            raise ValueError(self.lib.rs_error().decode())
+        c = (C.c_int * 5)()
+        self.lib.rs_counts(self.h, c)
+        self.n_vertices, self.n_edges, self.n_faces, self.n_tets, self.n_dual = list(c)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.rs_destroy(self.h)
+            self.h = None
+
+    def _ok(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.rs_error().decode())
+
+    def attach(self, mode, search=0, partner=None, dots=0):
+        self._ok(self.lib.rs_attach(self.h, mode, search, dots, partner.h if partner is not None else None))
+
+    def set_parameters(self, emitter=True, decay=0.08, cg_iterations=600, abs_tol=1e-10, rel_tol=1e-9):
+        self.lib.rs_set_parameters(self.h, 1 if emitter else 0, decay, cg_iterations, abs_tol, rel_tol)
+
+    def set_potential(self, phi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        self._ok(self.lib.rs_set_potential(self.h, phi.ctypes.data))
+
+    def advect_vorticity(self, dt):
+        self._ok(self.lib.rs_advect_vorticity(self.h, dt))
+
+    def advance(self, dt):
+        self._ok(self.lib.rs_advance(self.h, dt))
+
+    def set_box_size(self, size):
+        self._ok(self.lib.rs_set_box_size(self.h, size))
+
+    def reset(self):
+        self._ok(self.lib.rs_reset(self.h))
+
+    def _get(self, name, count, dtype):
+        out = np.zeros(count, dtype)
+        getattr(self.lib, name)(self.h, out.ctypes.data)
+        return out
+
+    def vorticity(self):
+        return self._get("rs_vorticity", self.n_edges, np.float64)
+
+    def potential(self):
+        return self._get("rs_potential", self.n_edges, np.float64)
+
+    def flux(self):
+        return self._get("rs_flux", self.n_faces, np.float64)
+
+    def vertex_density(self):
+        return self._get("rs_vertex_density", self.n_vertices, np.float32)
+
+    def density(self):
+        return self._get("rs_density", self.n_tets, np.float32)
+
+    def edge_ends(self):
+        return self._get("rs_edge_midpoints", 6 * self.n_edges, np.float64).reshape(-1, 2, 3)
+
+    def diagnostics(self):
+        names = ("max_divergence", "max_boundary_flux", "kinetic_energy", "max_speed", "recovery_curl_error",
+                 "smoke_mass")
+        return dict(zip(names, self._get("rs_diagnostics", 6, np.float64)))
+
+    def substeps(self):
+        """CFL substeps of the last advance."""
+        return self.lib.rs_substeps(self.h)
+
+    def smoke_center(self):
+        """(centre height, mass) of the tet smoke."""
+        out = self._get("rs_smoke_center", 2, np.float64)
+        return float(out[0]), float(out[1])
+
+    def last_recovery(self):
+        it, cv = C.c_int(), C.c_int()
+        a, b = C.c_double(), C.c_double()
+        self.lib.rs_last_recovery(self.h, C.byref(it), C.byref(cv), C.byref(a), C.byref(b))
+        return {"iterations": it.value, "converged": bool(cv.value), "initial": a.value, "final": b.value}
+
+
+def sine_potential(ref):
+    """The seeded potential of the reference's GPU simplicial test
+    (SimplicialGpu3DTests.cpp): sin(pi x/L) sin(pi y/L) sin(pi z/L) (b_z - a_z)
+    at each edge's midpoint."""
+    ends = ref.edge_ends()
+    a, b = ends[:, 0], ends[:, 1]
+    p = (a + b) * .5
+    size = max(float(ends.max()), 1e-30)
+    s = np.sin(np.pi * p / size)
+    return s[:, 0] * s[:, 1] * s[:, 2] * (b[:, 2] - a[:, 2])

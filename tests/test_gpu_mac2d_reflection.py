@@ -13,7 +13,7 @@ import pytest
 import vapor_b200 as vb
 from vapor_b200.mac2d import (MACCORMACK, SEMI_LAGRANGIAN, ReflectionSimulation2D, reflection_app_params,
                               reflection_default_params)
-from oracle_lib import RefReflection2D, ref2d_available
+from oracle_lib import RefHistorical2D, RefReflection2D, ref2d_available
 
 needs_ref = pytest.mark.skipif(not ref2d_available(), reason="reference 2D build (oracle/_ref) missing")
 DT = 1.0 / 60.0
@@ -137,6 +137,25 @@ def test_reset_equals_the_reference_reset():
     sim.reset()
     ref.reset()
     _compare(sim, ref, 5, "after reset")
+    sim.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("n,frames", [(24, 24), (64, 60)])
+def test_frames_equal_the_historical_plume(n, frames):
+    """Historical2DTests.cpp's replay with the device in place of the
+    reflection solver: the historical plume (closed walls, no stirring,
+    step(1/60, .8, .995, 1, 60)) and the device solver with the member
+    initialisers give the same smoke, u, v and pressure every frame."""
+    old = RefHistorical2D(n)
+    sim = ReflectionSimulation2D(n, reflection_default_params())
+    for frame in range(1, frames + 1):
+        old.step(DT, .8, .995, 1.0, 60)
+        sim.advance(DT)
+        for name, got, want in zip(FIELDS, sim.download(), old.fields()):
+            assert np.all(np.isfinite(want))
+            assert _bits_equal(got, want), f"frame {frame} {name}"
     sim.close()
 
 
