@@ -293,6 +293,22 @@ vapor_status vapor_mac3d_upload(vapor_mac3d *sim, const float *density, const fl
                                 const float *v, const float *w);
 vapor_status vapor_mac3d_download(vapor_mac3d *sim, float *density, float *u, float *v,
                                   float *w);
+/* Streamed transfers, for hosts that exchange the state every step.
+ * vapor_mac3d_upload_async stages a host snapshot on a copy stream and
+ * returns; the next vapor_mac3d_advance takes it in at the start of its step
+ * (a device-to-device copy), so the copy overlaps whatever runs before.
+ * vapor_mac3d_download_async snapshots the fields after the steps issued so
+ * far (on the step stream) and copies the snapshot to the host on another
+ * stream, overlapping the steps issued after it. Host arrays (pinned memory
+ * for full overlap) must stay valid and unchanged, and downloaded arrays
+ * unread, until vapor_mac3d_wait_transfers returns. A synchronous upload
+ * replaces a staged upload that no step took in yet. The byte counters count
+ * both forms. */
+vapor_status vapor_mac3d_upload_async(vapor_mac3d *sim, const float *density, const float *u,
+                                      const float *v, const float *w);
+vapor_status vapor_mac3d_download_async(vapor_mac3d *sim, float *density, float *u, float *v,
+                                        float *w);
+vapor_status vapor_mac3d_wait_transfers(vapor_mac3d *sim);
 /* uploadedBytes/downloadedBytes (GpuMacSimulation3D.hpp:25-26). */
 vapor_status vapor_mac3d_byte_counters(const vapor_mac3d *sim, uint64_t *uploaded,
                                        uint64_t *downloaded);

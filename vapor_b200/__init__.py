@@ -90,6 +90,9 @@ def _declare(lib):
     f("vapor_render_volume", _vp, C.c_int32, C.c_float, C.POINTER(abi.RenderParams), _vp, _vp)
     f("vapor_mac3d_upload", _vp, _vp, _vp, _vp, _vp)
     f("vapor_mac3d_download", _vp, _vp, _vp, _vp, _vp)
+    f("vapor_mac3d_upload_async", _vp, _vp, _vp, _vp, _vp)
+    f("vapor_mac3d_download_async", _vp, _vp, _vp, _vp, _vp)
+    f("vapor_mac3d_wait_transfers", _vp)
     f("vapor_mac3d_byte_counters", _vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
     f("vapor_mac3d_device_fields", _vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp))
     f("vapor_mac3d_stream", _vp, C.POINTER(_vp))
@@ -218,6 +221,7 @@ class MacSimulation3D:
             n = n_or_algorithm
             params = params if params is not None else default_params()
         self.n = int(n)
+        self._in_flight = []  # host arrays of streamed transfers not yet waited for
         h = _vp()
         check(lib.vapor_mac3d_create(self.n, float(box), C.byref(params), C.byref(h)))
         self._h = h
@@ -313,6 +317,31 @@ class MacSimulation3D:
         ptrs = [_host(a, s, writable=True) for a, s in zip(out, sizes)]
         check(library().vapor_mac3d_download(self._h, *ptrs))
         return out
+
+    def upload_async(self, density, u, v, w):
+        """Stage a host snapshot on a copy stream; the next advance takes it
+        in. The arrays (pinned for full overlap) are kept referenced and must
+        stay unchanged until wait_transfers()."""
+        sizes = field_sizes(self.n)
+        arrays = (density, u, v, w)
+        ptrs = [_host(a, s) for a, s in zip(arrays, sizes)]
+        check(library().vapor_mac3d_upload_async(self._h, *ptrs))
+        self._in_flight.extend(arrays)
+
+    def download_async(self, out):
+        """Snapshot the state after the steps issued so far and copy it into
+        `out` (four float32 arrays, pinned for full overlap) on a copy stream;
+        read `out` only after wait_transfers()."""
+        sizes = field_sizes(self.n)
+        ptrs = [_host(a, s, writable=True) for a, s in zip(out, sizes)]
+        check(library().vapor_mac3d_download_async(self._h, *ptrs))
+        self._in_flight.extend(out)
+        return out
+
+    def wait_transfers(self):
+        """Block until every staged upload and download has finished."""
+        check(library().vapor_mac3d_wait_transfers(self._h))
+        self._in_flight = []
 
     def byte_counters(self):
         up, down = C.c_uint64(), C.c_uint64()

@@ -229,6 +229,14 @@ VB_API vapor_status vapor_mac3d_upload(vapor_mac3d* sim, const float* d, const f
 VB_API vapor_status vapor_mac3d_download(vapor_mac3d* sim, float* d, float* u, float* v, float* w) {
     SIM_GUARD(require(d && u && v && w, "null field"); sim->sim.download(d, u, v, w));
 }
+VB_API vapor_status vapor_mac3d_upload_async(vapor_mac3d* sim, const float* d, const float* u, const float* v,
+                                             const float* w) {
+    SIM_GUARD(require(d && u && v && w, "null field"); sim->sim.upload_async(d, u, v, w));
+}
+VB_API vapor_status vapor_mac3d_download_async(vapor_mac3d* sim, float* d, float* u, float* v, float* w) {
+    SIM_GUARD(require(d && u && v && w, "null field"); sim->sim.download_async(d, u, v, w));
+}
+VB_API vapor_status vapor_mac3d_wait_transfers(vapor_mac3d* sim) { SIM_GUARD(sim->sim.wait_transfers()); }
 VB_API vapor_status vapor_mac3d_byte_counters(const vapor_mac3d* sim, uint64_t* up, uint64_t* down) {
     SIM_GUARD(if (up) *up = sim->sim.uploaded; if (down) *down = sim->sim.downloaded);
 }

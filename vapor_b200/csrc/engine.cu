@@ -694,6 +694,10 @@ Simulation::Simulation(int n, float box, const vapor_mac3d_params& p) : params(p
 }
 
 Simulation::~Simulation() {
+    cudaStreamSynchronize(h2d_.s);
+    cudaStreamSynchronize(d2h_.s);
+    for (cudaEvent_t e : {in_ready_, in_taken_, out_ready_, out_done_})
+        if (e) cudaEventDestroy(e);
     cudaStreamSynchronize(ws_.stream());
     release_graphs();
     if (warm_) warm_->use_own_stream();  // the networks outlive this simulation's stream
@@ -926,6 +930,7 @@ void Simulation::record_step_for_batch(float dt) {
 
 void Simulation::advance(float dt) {
     prepare_step(dt);
+    take_staged_upload();
     cudaStream_t s = ws_.stream();
     if (!use_graphs_ || ws_.timer().enabled()) {
         record_step(dt);
@@ -1072,6 +1077,9 @@ std::vector<uint8_t> Simulation::step_key(float dt) const {
 }
 
 void Simulation::upload(const float* d, const float* u, const float* v, const float* w) {
+    // a synchronous upload replaces a staged one that no step took in yet
+    VB_CUDA(cudaStreamSynchronize(h2d_.s));
+    pending_in_ = false;
     cudaStream_t s = ws_.stream();
     const size_t cells = dens_[0].n, faces = vel_[0][0].n;
     VB_CUDA(cudaMemcpyAsync(dens_[cur_].p, d, cells * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -1091,6 +1099,69 @@ void Simulation::download(float* d, float* u, float* v, float* w) {
     VB_CUDA(cudaMemcpyAsync(w, vel_[S_][2].p, faces * sizeof(float), cudaMemcpyDeviceToHost, s));
     VB_CUDA(cudaStreamSynchronize(s));
     downloaded += (cells + 3 * faces) * sizeof(float);
+}
+
+namespace {
+void ensure_event(cudaEvent_t& e) {
+    if (!e) VB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+void ensure_stage(DevArray<float>* stage, size_t cells, size_t faces) {
+    if (stage[0].n != cells) stage[0].allocate(cells);
+    for (int c = 1; c < 4; ++c)
+        if (stage[c].n != faces) stage[c].allocate(faces);
+}
+}  // namespace
+
+void Simulation::upload_async(const float* d, const float* u, const float* v, const float* w) {
+    const size_t cells = dens_[0].n, faces = vel_[0][0].n;
+    ensure_stage(in_stage_, cells, faces);
+    for (cudaEvent_t* e : {&in_ready_, &in_taken_}) ensure_event(*e);
+    // the staging copy is reused once the previous staged upload was taken in
+    if (in_taken_recorded_) VB_CUDA(cudaStreamWaitEvent(h2d_.s, in_taken_, 0));
+    const float* src[4] = {d, u, v, w};
+    for (int c = 0; c < 4; ++c)
+        VB_CUDA(cudaMemcpyAsync(in_stage_[c].p, src[c], in_stage_[c].bytes(), cudaMemcpyHostToDevice, h2d_.s));
+    VB_CUDA(cudaEventRecord(in_ready_, h2d_.s));
+    pending_in_ = true;
+    uploaded += (cells + 3 * faces) * sizeof(float);
+}
+
+// At the start of a step: the staged snapshot becomes the state.
+void Simulation::take_staged_upload() {
+    if (!pending_in_) return;
+    cudaStream_t s = ws_.stream();
+    VB_CUDA(cudaStreamWaitEvent(s, in_ready_, 0));
+    float* dst[4] = {dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p};
+    for (int c = 0; c < 4; ++c)
+        VB_CUDA(cudaMemcpyAsync(dst[c], in_stage_[c].p, in_stage_[c].bytes(), cudaMemcpyDeviceToDevice, s));
+    VB_CUDA(cudaEventRecord(in_taken_, s));
+    in_taken_recorded_ = true;
+    pending_in_ = false;
+}
+
+void Simulation::download_async(float* d, float* u, float* v, float* w) {
+    const size_t cells = dens_[0].n, faces = vel_[0][0].n;
+    ensure_stage(out_stage_, cells, faces);
+    for (cudaEvent_t* e : {&out_ready_, &out_done_}) ensure_event(*e);
+    cudaStream_t s = ws_.stream();
+    // the snapshot is rewritten once the previous one reached the host
+    if (out_done_recorded_) VB_CUDA(cudaStreamWaitEvent(s, out_done_, 0));
+    const float* src[4] = {dens_[cur_].p, vel_[S_][0].p, vel_[S_][1].p, vel_[S_][2].p};
+    for (int c = 0; c < 4; ++c)
+        VB_CUDA(cudaMemcpyAsync(out_stage_[c].p, src[c], out_stage_[c].bytes(), cudaMemcpyDeviceToDevice, s));
+    VB_CUDA(cudaEventRecord(out_ready_, s));
+    VB_CUDA(cudaStreamWaitEvent(d2h_.s, out_ready_, 0));
+    float* dst[4] = {d, u, v, w};
+    for (int c = 0; c < 4; ++c)
+        VB_CUDA(cudaMemcpyAsync(dst[c], out_stage_[c].p, out_stage_[c].bytes(), cudaMemcpyDeviceToHost, d2h_.s));
+    VB_CUDA(cudaEventRecord(out_done_, d2h_.s));
+    out_done_recorded_ = true;
+    downloaded += (cells + 3 * faces) * sizeof(float);
+}
+
+void Simulation::wait_transfers() {
+    VB_CUDA(cudaStreamSynchronize(h2d_.s));
+    VB_CUDA(cudaStreamSynchronize(d2h_.s));
 }
 
 void Simulation::synchronize() { (void)last_projection(); }

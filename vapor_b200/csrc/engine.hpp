@@ -226,6 +226,16 @@ public:
     }
     void upload(const float* d, const float* u, const float* v, const float* w);
     void download(float* d, float* u, float* v, float* w);
+    // Streamed host transfers. upload_async copies a host snapshot into a
+    // device staging copy on its own stream and returns; the next advance
+    // takes it in (one device-to-device copy at the start of the step).
+    // download_async snapshots the fields on the step's stream and copies
+    // the snapshot to the host on another stream. Both overlap the
+    // neighbouring steps' compute; wait_transfers blocks until every staged
+    // copy has finished (host buffers stay untouched and valid until then).
+    void upload_async(const float* d, const float* u, const float* v, const float* w);
+    void download_async(float* d, float* u, float* v, float* w);
+    void wait_transfers();
     void synchronize();
     vapor_projection_result last_projection();
     void diagnostics(vapor_fluid_diagnostics* out);
@@ -285,6 +295,13 @@ private:
     bool use_graphs_ = true;
     unet::UNet* warm_ = nullptr;
     unet::UNet* coarse_ = nullptr;
+
+    // streamed transfers
+    void take_staged_upload();
+    Stream h2d_, d2h_;
+    DevArray<float> in_stage_[4], out_stage_[4];
+    cudaEvent_t in_ready_ = nullptr, in_taken_ = nullptr, out_ready_ = nullptr, out_done_ = nullptr;
+    bool pending_in_ = false, in_taken_recorded_ = false, out_done_recorded_ = false;
 
     Stream stream_;
     Workspace ws_;
