@@ -1213,17 +1213,23 @@ void set_sor_planes(int n, int planes) {
     else g_sor_planes[n] = planes;
 }
 
-// Planes per thread of the z-marching sweep: the tuned value, else about 2.5
-// waves of blocks (at 256^3: 4 planes, 2048 blocks; measured 5 % faster per
-// launch than 2 planes).
+// Planes per thread of the z-marching sweep: the tuned value; else, when
+// it is at least 2 and at most 16, the largest count whose full-length
+// chunks still fit one wave of resident blocks (148 SMs x 5), so that only
+// the short last chunk runs after the wave; else about 2.5 waves. At 256^3
+// this gives 11 planes (768 blocks: 23.4 us per colour launch, against
+// 25.2 us at 4 planes / 2048 blocks and 25.0 us at 12 planes / 704 blocks).
 static int sor_planes(int n, int blocks_x) {
     {
         std::lock_guard<std::mutex> lock(g_tuning_mutex);
         const auto it = g_sor_planes.find(n);
         if (it != g_sor_planes.end()) return std::max(1, std::min(it->second, n));
     }
-    const long target_blocks = 148L * 5 * 5 / 2;
+    const long slots = 148L * 5;
     const long per_plane = long(blocks_x);
+    const long one_wave = (per_plane * n) / slots;
+    if (one_wave >= 2 && one_wave <= 16) return int(one_wave);
+    const long target_blocks = slots * 5 / 2;
     int zb = int(std::max(1L, (per_plane * n) / target_blocks));
     return std::min(zb, 8);
 }
