@@ -1215,17 +1215,18 @@ void set_sor_planes(int n, int planes) {
 
 // Planes per thread of the z-marching sweep: the tuned value; else, when
 // it is at least 2 and at most 16, the largest count whose full-length
-// chunks still fit one wave of resident blocks (148 SMs x 5), so that only
+// chunks still fit one wave of resident blocks (148 SMs x 5, or x 4 for the
+// variants that also reduce a residual or dot products), so that only
 // the short last chunk runs after the wave; else about 2.5 waves. At 256^3
 // this gives 11 planes (768 blocks: 23.4 us per colour launch, against
 // 25.2 us at 4 planes / 2048 blocks and 25.0 us at 12 planes / 704 blocks).
-static int sor_planes(int n, int blocks_x) {
+static int sor_planes(int n, int blocks_x, int blocks_per_sm = 5) {
     {
         std::lock_guard<std::mutex> lock(g_tuning_mutex);
         const auto it = g_sor_planes.find(n);
         if (it != g_sor_planes.end()) return std::max(1, std::min(it->second, n));
     }
-    const long slots = 148L * 5;
+    const long slots = 148L * blocks_per_sm;
     const long per_plane = long(blocks_x);
     const long one_wave = (per_plane * n) / slots;
     if (one_wave >= 2 && one_wave <= 16) return int(one_wave);
@@ -1240,7 +1241,7 @@ int launch_sor_color_dot(const ProjectionArgs& a, int parity, float* x, const fl
     const RBLayout L = rb_layout(n);
     if (!sor_fuses_measure(n) || a.diag != nullptr || n % 2 != 0) return 0;
     const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
-    const int zb = sor_planes(n, bx);
+    const int zb = sor_planes(n, bx, 4);
     const dim3 grid(bx, (n + zb - 1) / zb);
     const int blocks = int(grid.x * grid.y);
     if (2 * blocks > partial_capacity) return 0;
@@ -1263,7 +1264,7 @@ void launch_sor_color(const ProjectionArgs& a, int parity, float* x, const float
     count_launch();
     if (sor_fuses_measure(n)) {
         const int bx = (L.hw / 4 * n + kThreads - 1) / kThreads;
-        const int zb = sor_planes(n, bx);
+        const int zb = sor_planes(n, bx, measure ? 4 : 5);
         const dim3 grid(bx, (n + zb - 1) / zb);
         const bool plain = a.diag == nullptr && n % 2 == 0;
 #define VB_SOR_RBZ(E, R, Z, P)                                                                                \
