@@ -374,14 +374,17 @@ vapor_status vapor_stage_set_solver_kind(vapor_stage *stage, int32_t kind);
  * solid cell are closed (velocity 0 before and after the projection), solid
  * cells are not unknowns (pressure 0, excluded from the residual), the
  * diagonal of a fluid cell counts its fluid neighbours, and the right-hand-side
- * and pressure means run over fluid cells. Needs VAPOR_SOLVER_MIXED_REFINEMENT;
- * a mask without fluid cells is VAPOR_INVALID_ARGUMENT. */
+ * and pressure means run over fluid cells. Needs VAPOR_SOLVER_MIXED_REFINEMENT
+ * or VAPOR_SOLVER_FPCG (masked operator, smoothing and coarse correction; the
+ * coarse network's mask channel stays zero); a mask without fluid cells is
+ * VAPOR_INVALID_ARGUMENT. */
 vapor_status vapor_stage_set_solid(vapor_stage *stage, const uint8_t *mask);
 /* The same obstacle mask (extension) for every later projection of a
  * resident simulation's steps: solid cells carry no pressure and the faces
  * touching them are closed; advection, forcing and smoke are unchanged.
- * Needs solver_kind VAPOR_SOLVER_MIXED_REFINEMENT (the step fails otherwise);
- * mask NULL removes it. Waits for the simulation's stream. */
+ * Needs solver_kind VAPOR_SOLVER_MIXED_REFINEMENT or VAPOR_SOLVER_FPCG (the
+ * step fails otherwise); mask NULL removes it. Waits for the simulation's
+ * stream. */
 vapor_status vapor_mac3d_set_solid(vapor_mac3d *sim, const uint8_t *mask);
 vapor_status vapor_stage_stream(vapor_stage *stage, void **stream);
 

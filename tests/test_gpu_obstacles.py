@@ -132,10 +132,94 @@ def test_resident_steps_with_an_obstacle_match_the_oracle():
         errs[name] = float(np.abs(x - y).max() / max(1e-30, float(np.abs(y).max())))
     print("32^3 plume with obstacle, 3 steps vs oracle, max relative difference:", errs)
     assert max(errs.values()) <= 1e-4, errs
-    # the learned solver has no obstacle form: a clear error, not a wrong answer
-    p.solver_kind = vb.abi.SOLVER_FPCG
+    # the plain red-black SOR has no obstacle form: a clear error, not a wrong answer
+    p.solver_kind = vb.abi.SOLVER_RED_BLACK_SOR
     sim.set_parameters(p)
     with pytest.raises(vb.VaporError):
         sim.advance(DT)
         sim.synchronize()
+
+
+def _fpcg_stage(n, mask, net=None):
+    st = vb.StageBackend(n, 1.0)
+    st.set_solver_kind(vb.abi.SOLVER_FPCG)
+    st.set_solid(mask)
+    if net is not None:
+        st.set_preconditioner(net)
+    return st
+
+
+@pytest.mark.parametrize("n,learned", [(32, False), (64, True)])
+def test_fpcg_with_an_obstacle_matches_the_oracle(n, learned):
+    """The FPCG solver with a sphere obstacle (masked operator, smoothing and
+    coarse correction; the coarse network where given, whose mask channel
+    stays zero) solves the same masked system as the oracle's mixed-precision
+    solver: fields and pressure to the projection test's 1e-5 relative, solid
+    pressure zero, the faces touching the obstacle closed."""
+    from vapor_b200.learned import WarmStartNet, COARSE_WEIGHTS
+    mask = sphere_mask(n, (0.5, 0.45, 0.55), 0.22)
+    _, u, v, w = random_fields(n, seed=90 + n)
+    opts = _opts(1e-8)
+    st, ro, ue, ve, we, pe = oracle_project(n, 1.0, u, v, w, 0.01, 1.9, 6.0, opts, solver_kind=1, solid=mask)
+    assert st == 0 and ro.linear_solve.converged
+    net = WarmStartNet.load(COARSE_WEIGHTS) if learned else None
+    stage = _fpcg_stage(n, mask, net)
+    ug, vg, wg = [a.copy() for a in (u, v, w)]
+    r, pg = stage.project(ug, vg, wg, ProjectionOptions(0.01, 1.9, opts), 6.0, want_pressure=True)
+    ls = r.linear_solve
+    assert ls.converged and ls.final_residual <= 1e-8 * ls.initial_residual
+    print(f"FPCG with obstacle at {n}^3 (learned={learned}): {ls.iterations} CG steps, "
+          f"oracle mixed solver {ro.linear_solve.iterations} sweeps")
+    for a, b in ((ug, ue), (vg, ve), (wg, we), (pg, pe)):
+        assert np.abs(a - b).max() <= 1e-5 * max(1.0, float(np.abs(b).max()))
+    s = mask.astype(bool)
+    assert np.all(pg[s] == 0)
+    assert np.all(ug[:, :, :-1][s] == 0) and np.all(ug[:, :, 1:][s] == 0)
+    assert np.all(vg[:, :-1, :][s] == 0) and np.all(vg[:, 1:, :][s] == 0)
+    assert np.all(wg[:-1][s] == 0) and np.all(wg[1:][s] == 0)
+    stage.close()
+    if net is not None:
+        net.close()
+
+
+def test_resident_fpcg_steps_with_an_obstacle_match_the_oracle():
+    """Whole resident steps of the 64^3 plume with a sphere obstacle and the
+    learned FPCG solver (to 1e-7) against the oracle's mixed-precision steps
+    with the same mask: within the resident obstacle test's 1e-4 after two
+    steps, faces touching the obstacle closed."""
+    from oracle_lib import OracleSim
+    from vapor_b200.learned import WarmStartNet, COARSE_WEIGHTS
+    from vapor_b200.plume import DT, scene_params, swirl_fields
+    n = 64
+    mask = sphere_mask(n, (0.5, 0.5, 0.55), 0.18)
+    p = scene_params(vb.default_params(), n, rel=1e-7, max_iterations=20000)
+    fields = [np.asarray(a, np.float32) for a in swirl_fields(n, seed=9)]
+    p.solver_kind = vb.abi.SOLVER_FPCG
+    net = WarmStartNet.load(COARSE_WEIGHTS)
+    sim = vb.MacSimulation3D(n, 1.0, p)
+    sim.upload(*fields)
+    sim.set_solid(mask)
+    sim.set_preconditioner(net)
+    p_ref = scene_params(vb.default_params(), n, rel=1e-7, max_iterations=20000)
+    p_ref.solver_kind = vb.abi.SOLVER_MIXED_REFINEMENT
+    ref = OracleSim(n, 1.0)
+    ref.params = p_ref
+    ref.set_fields(*fields)
+    ref.set_solid(mask)
+    s = mask.astype(bool)
+    for _ in range(2):
+        assert ref.advance(DT) == 0
+        sim.advance(DT)
+        assert sim.last_projection().linear_solve.converged
+        d, u, v, w = sim.download()
+        assert np.all(u[:, :, :-1][s] == 0) and np.all(u[:, :, 1:][s] == 0)
+        assert np.all(v[:, :-1, :][s] == 0) and np.all(v[:, 1:, :][s] == 0)
+        assert np.all(w[:-1][s] == 0) and np.all(w[1:][s] == 0)
+    errs = {}
+    for name, x, y in zip(("density", "u", "v", "w"), sim.download(), ref.fields()):
+        errs[name] = float(np.abs(x - y).max() / max(1e-30, float(np.abs(y).max())))
+    print("64^3 plume with obstacle, learned FPCG, 2 steps vs oracle, max relative difference:", errs)
+    assert max(errs.values()) <= 1e-4, errs
+    sim.close()
+    net.close()
     sim.close()

@@ -362,7 +362,11 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     float* r = r32_.p;
     const FpcgSmoothing sm = fpcg_smoothing();
     const int sweeps = sm.sweeps;
-    const ProjectionArgs smooth{a.g, a.dt, sm.omega, 0.0f, a.options};
+    // the smoothing sweeps keep the projection's obstacle mask, if any
+    ProjectionArgs smooth = a;
+    smooth.omega = sm.omega;
+    smooth.diagonal_floor = 0.0f;
+    const uint8_t* mask = a.diag;
     if (warm) warm->infer_into(n_, b_.p, ctrl_, nullptr, x64_[0].p);
     else VB_CUDA(cudaMemsetAsync(x64_[0].p, 0, x64_[0].bytes(), s));
     t.begin(VAPOR_PHASE_RESIDUAL);
@@ -385,13 +389,13 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         if (coarse) {
             t.begin(VAPOR_PHASE_COARSE);
-            launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st);
+            launch_restrict_residual(n_, r, cg_z_.p, cg_rows_.p, cg_rc_.p, st, mask);
             if (coarse_log_)
                 launch_log_coarse(cg_rc_.p, cg_rc_.n, coarse_log_, coarse_log_capacity_, coarse_log_counter_, st);
             coarse->set_stream(st);
             const float* zc = coarse->precondition(n_ / 4, cg_rc_.p);
             coarse->set_stream(s);
-            launch_coarse_correction(n_, cg_z_.p, zc, cg_rc_.p, cg_partials_.p, cg_, st);
+            launch_coarse_correction(n_, cg_z_.p, zc, cg_rc_.p, cg_partials_.p, cg_, st, mask);
             t.end(VAPOR_PHASE_COARSE, 0);
         }
         t.begin(VAPOR_PHASE_SOR);
@@ -406,10 +410,10 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
         t.end(VAPOR_PHASE_SOR, 2 * sweeps);
         return dot_blocks;
     };
-    // n % 8 == 0: the direction update, A p and the deferred error update run
-    // as one pass (launch_cg_direction_apply), with the direction in two
-    // buffers; same values as the separate passes
-    const bool fused = n_ % 8 == 0;
+    // n % 8 == 0 and no obstacles: the direction update, A p and the
+    // deferred error update run as one pass (launch_cg_direction_apply), with
+    // the direction in two buffers; same values as the separate passes
+    const bool fused = n_ % 8 == 0 && mask == nullptr;
     float* const pbuf[2] = {cg_p_.p, cg_p2_.p};
     auto recentre_group = [&](cudaStream_t st) {
         if (fused) launch_cg_fold(count, e, pbuf, cg_, ctrl_, st);
@@ -424,7 +428,7 @@ void Workspace::project_fpcg(const ProjectionArgs& a, unet::UNet* warm, unet::UN
     auto iteration = [&](cudaStream_t st) {
         t.begin(VAPOR_PHASE_KRYLOV);
         if (fused) launch_cg_direction_apply(n_, cg_z_.p, pbuf, e, cg_q_.p, cg_partials_.p, cg_, st);
-        else launch_apply_A_alpha(n_, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st);
+        else launch_apply_A_alpha(n_, cg_p_.p, cg_q_.p, cg_partials_.p, cg_, st, mask);
         t.end(VAPOR_PHASE_KRYLOV, 2);
         t.begin(VAPOR_PHASE_RESIDUAL);
         if (graph) {
@@ -470,8 +474,9 @@ void Workspace::project(const float* ui, const float* vi, const float* wi, float
                         unet::UNet* coarse, const float* rhs_field) {
     ProjectionArgs a{grid(), dt, omega, diagonal_floor, o};
     if (fluid_ > 0.0) {
-        if (solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT)
-            fail(VAPOR_INVALID_ARGUMENT, "solid obstacles need the mixed-precision solver (VAPOR_SOLVER_MIXED_REFINEMENT)");
+        if (solver_kind != VAPOR_SOLVER_MIXED_REFINEMENT && solver_kind != VAPOR_SOLVER_FPCG)
+            fail(VAPOR_INVALID_ARGUMENT,
+                 "solid obstacles need the mixed-precision or the FPCG solver (VAPOR_SOLVER_MIXED_REFINEMENT, VAPOR_SOLVER_FPCG)");
         a.diag = solid_diag_.p;
         a.solid = solid_.p;
         a.fluid = fluid_;

@@ -265,7 +265,8 @@ public:
     // null: smoothing-only preconditioner). Needs n divisible by 16.
     void set_preconditioner(unet::UNet* net);
     // Obstacle mask (n^3, x fastest, nonzero = solid; null clears) for every
-    // later projection of this simulation; needs the mixed-precision solver.
+    // later projection of this simulation; needs the mixed-precision or the
+    // FPCG solver.
     void set_solid(const uint8_t* mask);
     unet::UNet* preconditioner() const { return coarse_; }
     Workspace& workspace() { return ws_; }

@@ -258,7 +258,9 @@ void launch_cg_rho(size_t count, const float* z, const float* r, double* partial
 void launch_cg_alpha(size_t count, const float* p, const float* q, double* partials, CgControl* cg,
                      cudaStream_t s);
 // q = A p and cg->alpha = rho / p.q in one pass over p (two launches).
-void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s);
+// diag: the solid-obstacle mask (split-layout fluid-neighbour counts), or null.
+void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s,
+                          const uint8_t* diag = nullptr);
 // e += alpha p; r -= alpha q; then count the iteration and decide the FP64
 // re-centring (ctrl->recentre, and the graph if-condition when active).
 void launch_cg_update(size_t count, float* e, float* r, const float* p, const float* q, const CgControl* cg,
@@ -285,13 +287,14 @@ void launch_cg_update_r(size_t count, float* r, const float* q, const CgControl*
 void launch_cg_fold(size_t count, float* e, float* const* p, CgControl* cg, const ProjControl* ctrl, cudaStream_t s);
 // rc = 4^3 block sums of r - A z on the (n/4)^3 grid (natural layout); n % 4 == 0.
 // `rows` holds n^3 / 4 floats of scratch.
-void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s);
+void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s,
+                              const uint8_t* diag = nullptr);
 // Appends the coarse right-hand side (cells floats) to a device ring of
 // `capacity` records: record *counter % capacity, then ++*counter.
 void launch_log_coarse(const float* rc, size_t cells, float* log, int capacity, int* counter, cudaStream_t s);
 // z += gamma (P zc - mean zc), gamma by the Galerkin condition on the coarse grid.
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
-                              cudaStream_t s);
+                              cudaStream_t s, const uint8_t* diag = nullptr);
 
 // ---- headless rendering (kernels_render.cu) ----
 void render_volume(const float* density, int n, float box, const vapor_render_params& p, float* rgb, cudaStream_t s);

@@ -61,6 +61,39 @@ __global__ void __launch_bounds__(kThreads) k_apply_A(int n, const float* __rest
     }
 }
 
+// Solid obstacles: `diag` holds each slot's fluid-neighbour count, 0 for a
+// solid cell (the mixed solver's split-layout mask). The solver keeps every
+// vector at 0 on solid cells, so a solid neighbour adds nothing to a sum;
+// the operator's diagonal is the fluid-neighbour count and its row is 0 on a
+// solid cell (the rules of the mixed solver's masked sweep and residual).
+__global__ void __launch_bounds__(kThreads) k_apply_A_masked(int n, const float* __restrict__ ps,
+                                                             const uint8_t* __restrict__ diag,
+                                                             float* __restrict__ qs) {
+    const RBLayout L = rb_layout(n);
+    const size_t count = 2 * L.stride;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x) {
+        const int colour = int(i / L.stride);
+        const size_t rem = i - size_t(colour) * L.stride;
+        const int slot = int(rem % L.hw);
+        const size_t row = rem / L.hw;
+        const int y = int(row % n), z = int(row / n);
+        const int x = 2 * slot + ((y + z + colour) & 1);
+        float out = 0.f;
+        const int d = diag[i];
+        if (x < n && d > 0) {
+            float ax = float(d) * ps[i];
+            if (x > 0) ax -= ps[rb_index(L, x - 1, y, z)];
+            if (x + 1 < n) ax -= ps[rb_index(L, x + 1, y, z)];
+            if (y > 0) ax -= ps[rb_index(L, x, y - 1, z)];
+            if (y + 1 < n) ax -= ps[rb_index(L, x, y + 1, z)];
+            if (z > 0) ax -= ps[rb_index(L, x, y, z - 1)];
+            if (z + 1 < n) ax -= ps[rb_index(L, x, y, z + 1)];
+            out = ax;
+        }
+        qs[i] = out;
+    }
+}
+
 // Row-pair access (n % 8 == 0): thread t owns slots 4j..4j+3 of both colours
 // in row (y, z), i.e. the 8 cells x = 8j .. 8j+7. In that row the cells with
 // even x have colour (y + z) & 1, those with odd x the other colour, so the
@@ -534,6 +567,39 @@ __global__ void __launch_bounds__(kThreads) k_restrict_rows(int n, const float* 
     }
 }
 
+// k_restrict_rows with obstacles: solid cells contribute nothing (their r
+// and z are 0), fluid cells r - A z with the masked operator.
+__global__ void __launch_bounds__(kThreads) k_restrict_rows_masked(int n, const float* __restrict__ r,
+                                                                   const float* __restrict__ zs,
+                                                                   const uint8_t* __restrict__ diag,
+                                                                   float* __restrict__ rows) {
+    const RBLayout L = rb_layout(n);
+    const int nc = n >> 2;
+    const long total = long(n) * n * nc;
+    for (long t = long(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const int cx = int(t % nc);
+        const long yz = t / nc;
+        const int y = int(yz % n), z = int(yz / n);
+        float acc = 0.f;
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+            const int x = 4 * cx + dx;
+            const size_t me = rb_index(L, x, y, z);
+            const int d = diag[me];
+            if (d == 0) continue;
+            float ax = float(d) * zs[me];
+            if (x > 0) ax -= zs[rb_index(L, x - 1, y, z)];
+            if (x + 1 < n) ax -= zs[rb_index(L, x + 1, y, z)];
+            if (y > 0) ax -= zs[rb_index(L, x, y - 1, z)];
+            if (y + 1 < n) ax -= zs[rb_index(L, x, y + 1, z)];
+            if (z > 0) ax -= zs[rb_index(L, x, y, z - 1)];
+            if (z + 1 < n) ax -= zs[rb_index(L, x, y, z + 1)];
+            acc += r[me] - ax;
+        }
+        rows[t] = acc;
+    }
+}
+
 // Pass 2: rc[C] = sum of the 4 x 4 (y, z) row sums of C, fixed order.
 __global__ void __launch_bounds__(kThreads) k_restrict_blocks(int n, const float* __restrict__ rows,
                                                               float* __restrict__ rc) {
@@ -631,6 +697,29 @@ __global__ void __launch_bounds__(kThreads) k_prolong_add(int n, float* __restri
     }
 }
 
+// k_prolong_add on fluid cells only (solid cells keep z = 0).
+__global__ void __launch_bounds__(kThreads) k_prolong_add_masked(int n, float* __restrict__ zs,
+                                                                 const float* __restrict__ zc,
+                                                                 const uint8_t* __restrict__ diag,
+                                                                 const CgControl* __restrict__ cg) {
+    const RBLayout L = rb_layout(n);
+    const int nc = n >> 2;
+    const float g = float(cg->gamma), m = float(cg->zc_mean);
+    const size_t count = 2 * L.stride;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x) {
+        if (diag[i] == 0) continue;
+        const int colour = int(i / L.stride);
+        const size_t rem = i - size_t(colour) * L.stride;
+        const int slot = int(rem % L.hw);
+        const size_t row = rem / L.hw;
+        const int y = int(row % n), z = int(row / n);
+        const int x = 2 * slot + ((y + z + colour) & 1);
+        if (x >= n) continue;
+        const size_t coarse = (size_t(z >> 2) * nc + (y >> 2)) * nc + (x >> 2);
+        zs[i] = zs[i] + g * (zc[coarse] - m);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_log_coarse(const float* __restrict__ rc, size_t cells,
                                                          float* __restrict__ log, int capacity,
                                                          const int* __restrict__ counter) {
@@ -685,7 +774,14 @@ void launch_cg_alpha(size_t count, const float* p, const float* q, double* parti
     k_alpha_finish<<<1, 1024, 0, s>>>(partials, blocks, cg);
 }
 
-void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s) {
+void launch_apply_A_alpha(int n, const float* p, float* q, double* partials, CgControl* cg, cudaStream_t s,
+                          const uint8_t* diag) {
+    if (diag) {
+        count_launch();
+        k_apply_A_masked<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, p, diag, q);
+        launch_cg_alpha(rb_count(n), p, q, partials, cg, s);
+        return;
+    }
     if (n % 8 != 0) {
         launch_apply_A(n, p, q, s);
         launch_cg_alpha(rb_count(n), p, q, partials, cg, s);
@@ -759,10 +855,12 @@ void launch_cg_fold(size_t count, float* e, float* const* p, CgControl* cg, cons
     k_fold_clear<<<1, 1, 0, s>>>(cg, ctrl);
 }
 
-void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s) {
+void launch_restrict_residual(int n, const float* r, const float* z, float* rows, float* rc, cudaStream_t s,
+                              const uint8_t* diag) {
     const int nc = n / 4;
     count_launch();
-    if (n % 16 == 0) k_restrict_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, r, z, rows);
+    if (diag) k_restrict_rows_masked<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, diag, rows);
+    else if (n % 16 == 0) k_restrict_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, r, z, rows);
     else k_restrict_rows<<<blocks_for(size_t(n) * n * nc), kThreads, 0, s>>>(n, r, z, rows);
     count_launch();
     k_restrict_blocks<<<blocks_for(size_t(nc) * nc * nc), kThreads, 0, s>>>(n, rows, rc);
@@ -776,7 +874,7 @@ void launch_log_coarse(const float* rc, size_t cells, float* log, int capacity, 
 }
 
 void launch_coarse_correction(int n, float* z, const float* zc, const float* rc, double* partials, CgControl* cg,
-                              cudaStream_t s) {
+                              cudaStream_t s, const uint8_t* diag) {
     const int nc = n / 4;
     const size_t cells = size_t(nc) * nc * nc;
     const int blocks = blocks_for(cells);
@@ -785,7 +883,8 @@ void launch_coarse_correction(int n, float* z, const float* zc, const float* rc,
     count_launch();
     k_coarse_finish<<<1, 1024, 0, s>>>(partials, blocks, double(cells), cg);
     count_launch();
-    if (n % 16 == 0) k_prolong_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, z, zc, cg);
+    if (diag) k_prolong_add_masked<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, diag, cg);
+    else if (n % 16 == 0) k_prolong_pairs<<<pair_grid(n), kThreads, 0, s>>>(n, z, zc, cg);
     else k_prolong_add<<<blocks_for(rb_count(n)), kThreads, 0, s>>>(n, z, zc, cg);
 }
 
