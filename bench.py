@@ -459,20 +459,23 @@ def main():
     peak, peak_kind = measured_peaks()
     cells = n ** 3
 
-    def sor_roofline(ph, sweeps):
+    def sor_roofline(ph, sweeps, dot_launches=0.0):
         """The red-black sweep phase of one eager step covering `sweeps`
         red+black iterations: per-launch algorithmic bytes over the average
         launch time. One red+black iteration reads x and b and writes x,
         12 B/cell, so a one-colour launch is charged half of that, 6 B/cell
         (the other colour's half of x, written by the previous launch, is
         mostly read back from L2); a temporally blocked launch of several
-        iterations reads x and b and writes x once, 12 B/cell."""
+        iterations reads x and b and writes x once, 12 B/cell. In the FPCG
+        preconditioner the last sweep of each CG step (`dot_launches` of
+        them) also reads r of the other colour and q of both, 6 B/cell
+        more."""
         sor = ph["sor"]
         launches = max(1, sor["launches"])
         launch_ms = sor["ms"] / launches
         per_launch = sweeps / launches
         blocked = per_launch >= 1.5
-        nbytes = (12.0 if blocked else 6.0) * cells
+        nbytes = (12.0 if blocked else 6.0) * cells * (1.0 + dot_launches / launches)
         achieved = nbytes / (launch_ms * 1e-3) / 1e9
         line = {"bound": "hbm", "kernel": (f"k_sor_blocked ({per_launch:.0f} red+black iterations per launch)"
                                            if blocked else "k_sor_rbz (red-black colour sweep)"),
@@ -526,7 +529,7 @@ def main():
         "sweep_ratio_vs_plain": plain["iterations"] / max(1e-9, per_app * (learned["iterations"] + 2)),
         "gpu_launches": launches,
         "gpu_launches_note": "kernels per step counted on the eager replay of the same step, times steps",
-        "roofline": sor_roofline(phases, per_app * (eager_its + 2.0) * roof_steps),
+        "roofline": sor_roofline(phases, per_app * (eager_its + 2.0) * roof_steps, eager_its * roof_steps),
         "roofline_tensor": {"bound": "tensor", "kernel": "coarse U-Net forward (k_conv3_zm and k_conv3_tc, 10 convolutions)",
                             "achieved": tflops, "peak": tpeak, "unit": "TFLOP/s", "frac": tflops / tpeak,
                             "peak_kind": "measured sustained", "flops_per_application": net_flops,
