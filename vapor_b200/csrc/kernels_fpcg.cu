@@ -186,7 +186,10 @@ __global__ void __launch_bounds__(kThreads) k_apply_A_dot(int n, const float* __
     }
 }
 
-// Fused direction step on row pairs (n % 8 == 0), grid as k_apply_A_dot:
+// Fused direction step on row pairs (n % 8 == 0), grid as k_apply_A_dot.
+// Capped at 64 registers (4 resident blocks per SM instead of 3; a few
+// bytes spill): the pass is bound by the latency of its neighbour-row
+// loads, and the higher occupancy measured 0.3 ms per 256^3 step faster.
 // with po = p[p_cur] and pn the other buffer, e += alpha_pending po (when an
 // update is pending), pn = z + beta po (a copy of z for the first direction),
 // q = A pn and FP64 block partials of pn.q. The stencil reads pn at the
@@ -209,7 +212,7 @@ __device__ __forceinline__ RowEO dir_eo(const float* __restrict__ z, const float
     return r;
 }
 
-__global__ void __launch_bounds__(kThreads) k_direction_apply(int n, const float* __restrict__ zs, float* P0, float* P1,
+__global__ void __launch_bounds__(kThreads, 4) k_direction_apply(int n, const float* __restrict__ zs, float* P0, float* P1,
                                                               float* __restrict__ es, float* __restrict__ qs,
                                                               const CgControl* __restrict__ cg,
                                                               double* __restrict__ partials) {
