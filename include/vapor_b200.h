@@ -706,9 +706,12 @@ typedef struct vapor_simplicial3d_mesh {
  * neighbours from the sample's tet. dot_order: 0 automatic (index order up
  * to 262144 edges), 1 index order on one thread (std::inner_product's: the
  * recovery's iterates equal the CPU solver's bit for bit), 2 a parallel
- * tree (faster on large meshes; equal to rounding). */
+ * tree (faster on large meshes; equal to rounding). preconditioner: 0 the
+ * CPU solver's (its IC(0) factor where it has one, else its diagonal), 1
+ * always the diagonal (Jacobi, the OpenGL backend's choice: no sequential
+ * triangular solves, more iterations, not the CPU's iterates). */
 vapor_status vapor_simplicial3d_create(const vapor_simplicial3d_mesh *mesh, int32_t site_search,
-                                       int32_t dot_order, vapor_simplicial3d **out);
+                                       int32_t dot_order, int32_t preconditioner, vapor_simplicial3d **out);
 vapor_status vapor_simplicial3d_destroy(vapor_simplicial3d *stages);
 /* advectCirculation: omega (n_edges) from the dual velocities (3 n_dual) and,
  * on general domains, the node samples (3 n_nodes; NULL on boxes). */

@@ -213,14 +213,15 @@ HX void* rs_create(const char* path, int box, double size) {
 HX void rs_destroy(void* h) { delete static_cast<Solver*>(h); }
 
 // Installs backend `mode` (see the header) with nearest-site search `search`
-// and the recovery's dot-product order `dot_order` (vapor_simplicial3d_create).
-HX int rs_attach(void* h, int mode, int search, int dot_order, void* partner) {
+// and the recovery's dot-product order `dot_order` and preconditioner
+// (vapor_simplicial3d_create).
+HX int rs_attach(void* h, int mode, int search, int dot_order, int preconditioner, void* partner) {
     return guarded([&] {
         Solver& s = S(h);
         s.solver->setComputeBackend(nullptr);
         s.backend.reset();
         if (mode == 1) {
-            auto gpu = std::make_unique<GpuSimplicial3D>(search, dot_order);
+            auto gpu = std::make_unique<GpuSimplicial3D>(search, dot_order, preconditioner);
             gpu->initialize(*s.solver);
             s.backend = std::move(gpu);
         } else if (mode == 2) {
@@ -336,3 +337,20 @@ HX void rs_smoke_center(void* h, double* out) {
 }
 // CFL substeps of the last advance (SimplicialTimings3D::substeps).
 HX int rs_substeps(void* h) { return S(h).solver->timings().substeps; }
+// Dependency levels of the forward solve of the solver's IC(0) factor (0
+// when it has none): the sequential steps of the preconditioner on a GPU.
+HX int rs_ic_levels(void* h) {
+    vapor_b200::SimplicialPacked k;
+    GpuSimplicial3D::packSolver(*S(h).solver, k);
+    if (k.ic_offsets.empty()) return 0;
+    const int n = int(k.ic_offsets.size()) - 1;
+    std::vector<int> level(n, 0);
+    int levels = 0;
+    for (int i = 0; i < n; ++i) {
+        int l = 0;
+        for (int j = k.ic_offsets[i]; j < k.ic_offsets[i + 1]; ++j) l = std::max(l, level[k.ic_columns[j]] + 1);
+        level[i] = l;
+        levels = std::max(levels, l + 1);
+    }
+    return levels;
+}

@@ -549,7 +549,7 @@ def _simplicial_lib():
         f("rs_error", C.c_char_p)
         f("rs_create", _vp, C.c_char_p, C.c_int, C.c_double)
         f("rs_destroy", None, _vp)
-        f("rs_attach", C.c_int, _vp, C.c_int, C.c_int, C.c_int, _vp)
+        f("rs_attach", C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp)
         f("rs_counts", None, _vp, _vp)
         f("rs_set_potential", C.c_int, _vp, _vp)
         f("rs_advect_vorticity", C.c_int, _vp, C.c_double)
@@ -594,8 +594,9 @@ class RefSimplicial:
         if rc != 0:
             raise RuntimeError(self.lib.rs_error().decode())
 
-    def attach(self, mode, search=0, partner=None, dots=0):
-        self._ok(self.lib.rs_attach(self.h, mode, search, dots, partner.h if partner is not None else None))
+    def attach(self, mode, search=0, partner=None, dots=0, jacobi=False):
+        self._ok(self.lib.rs_attach(self.h, mode, search, dots, 1 if jacobi else 0,
+                                    partner.h if partner is not None else None))
 
     def set_parameters(self, emitter=True, decay=0.08, cg_iterations=600, abs_tol=1e-10, rel_tol=1e-9):
         self.lib.rs_set_parameters(self.h, 1 if emitter else 0, decay, cg_iterations, abs_tol, rel_tol)

@@ -111,6 +111,23 @@ def test_device_backend_tree_order_stays_within_rounding():
         assert _max_error(cpu.flux(), gpu.flux()) <= 1e-9, k + 1
 
 
+@pytest.mark.gpu
+@needs_ref
+def test_device_backend_jacobi_option_within_the_reference_bound():
+    """The Jacobi preconditioner on a general domain (the OpenGL backend's
+    choice; not the CPU's iterates): the recovery converges and flux and
+    smoke stay within the reference's GPU-backend bounds over 20 steps."""
+    cpu = RefSimplicial("bunny-fluid.tet", False, 2.0)
+    gpu = RefSimplicial("bunny-fluid.tet", False, 2.0)
+    gpu.attach(RefSimplicial.DEVICE, dots=2, jacobi=True)
+    for k in range(20):
+        cpu.advance(1 / 30)
+        gpu.advance(1 / 30)
+        assert gpu.last_recovery()["converged"]
+        assert _max_error(cpu.flux(), gpu.flux()) <= 1e-5, k + 1
+        assert _max_error(cpu.vertex_density(), gpu.vertex_density()) <= 1e-3, k + 1
+
+
 def _max_error(a, b):
     return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max())
 

@@ -12,8 +12,9 @@
 //                       vertex smoke at the foot, decay, round to float
 //   recover             CG on the CSR Dirichlet potential operator with the
 //                       CPU solver's preconditioner (its IC(0) factor by two
-//                       level-scheduled triangular solves in one block, each
-//                       row in the CPU's operation order, or its diagonal);
+//                       level-scheduled triangular solves in one block, the
+//                       vector in shared memory when it fits, each row in
+//                       the CPU's operation order, or its diagonal);
 //                       the operator applied matrix-free by gather kernels
 //                       in the CPU's summation order and the dot products
 //                       summed in index order (std::inner_product's), so the
@@ -257,6 +258,9 @@ struct Precond {
     const int* b_level_offsets;
     const int* b_columns;
     int b_levels;
+    // the same rows in level order as (row, first entry, end) for one load
+    const int4* f_table;
+    const int4* b_table;
 };
 
 // r = b - A x (zero on boundary edges, as the CPU solver sets it); partials
@@ -316,6 +320,112 @@ __global__ void __launch_bounds__(1024) ks_ic_solve(Precond m, const double* __r
         }
         __syncthreads();
     }
+}
+// ks_ic_solve with the vector in shared memory (n doubles) and one warp per
+// row. The lanes hold a row's entries (up to 32 at a time) and form its
+// products in parallel; one lane then subtracts them from the row's value in
+// the CPU's order. The entries of a warp's row in the
+// next level do not depend on the solve, so they are fetched before the
+// barrier that ends the current level and arrive while it waits: a level
+// costs the shared-memory gathers, the shuffles and the barrier, not round
+// trips to L2. Same operations in the same order as the thread-per-row form.
+struct IcRowFetch {
+    int row, beg, end;  // row < 0: none
+    int column;
+    double value, init;
+};
+__device__ __forceinline__ IcRowFetch ic_fetch(int k, int k_end, const int4* __restrict__ table,
+                                               const int* __restrict__ columns, const double* __restrict__ values,
+                                               const double* init_global, int lane) {
+    IcRowFetch f;
+    f.row = -1;
+    f.beg = f.end = 0;
+    f.column = 0;
+    f.value = 0.0;
+    f.init = 0.0;
+    if (k < k_end) {
+        const int4 t = table[k];
+        f.row = t.x;
+        f.beg = t.y;
+        f.end = t.z;
+        const int j = f.beg + lane;
+        if (j < f.end) {
+            f.column = columns[j];
+            f.value = values[j];
+        }
+        if (init_global) f.init = init_global[f.row];
+    }
+    return f;
+}
+// acc minus the row's products in order (the fetched first 32, then the
+// rest): the lanes form the products into the warp's shared-memory slots and
+// lane 0 subtracts them one after the other (its result is the one kept).
+__device__ __forceinline__ double ic_apply(const IcRowFetch& f, double acc, const int* __restrict__ columns,
+                                           const double* __restrict__ values, const double* zs, double* stage,
+                                           int lane) {
+    stage[lane] = f.beg + lane < f.end ? f.value * zs[f.column] : 0.0;
+    __syncwarp();
+    if (lane == 0) {
+        const int count = min(32, f.end - f.beg);
+        for (int t = 0; t < count; ++t) acc -= stage[t];
+    }
+    __syncwarp();
+    for (int base = f.beg + 32; base < f.end; base += 32) {
+        const int j = base + lane;
+        stage[lane] = j < f.end ? values[j] * zs[columns[j]] : 0.0;
+        __syncwarp();
+        if (lane == 0) {
+            const int count = min(32, f.end - base);
+            for (int t = 0; t < count; ++t) acc -= stage[t];
+        }
+        __syncwarp();
+    }
+    return acc;
+}
+// One triangular solve over `levels` levels: each warp's first row of a level
+// is fetched two levels ahead (its table entry, entries and initial value do
+// not depend on the solve); further rows of the level are fetched in place.
+__device__ __forceinline__ void ic_sweep(int levels, const int* __restrict__ level_offsets,
+                                         const int4* __restrict__ table, const int* __restrict__ columns,
+                                         const double* __restrict__ values, const double* __restrict__ diagonal,
+                                         const double* init_global, double* zs, double* stage, int lane, int warp,
+                                         int warps) {
+    auto fetch = [&](int level) {
+        if (level >= levels) return IcRowFetch{-1, 0, 0, 0, 0.0, 0.0};
+        return ic_fetch(level_offsets[level] + warp, level_offsets[level + 1], table, columns, values, init_global,
+                        lane);
+    };
+    IcRowFetch a = fetch(0), b = fetch(1);
+    for (int level = 0; level < levels; ++level) {
+        const IcRowFetch cur = a;
+        a = b;
+        b = fetch(level + 2);
+        if (cur.row >= 0) {
+            const double acc = ic_apply(cur, init_global ? cur.init : zs[cur.row], columns, values, zs, stage, lane);
+            if (lane == 0) zs[cur.row] = acc / diagonal[cur.row];
+        }
+        for (int k = level_offsets[level] + warp + warps; k < level_offsets[level + 1]; k += warps) {
+            const IcRowFetch f = ic_fetch(k, k + 1, table, columns, values, init_global, lane);
+            const double acc = ic_apply(f, init_global ? f.init : zs[f.row], columns, values, zs, stage, lane);
+            if (lane == 0) zs[f.row] = acc / diagonal[f.row];
+        }
+        __syncthreads();
+    }
+}
+__global__ void __launch_bounds__(1024, 1) ks_ic_solve_shared(Precond m, int n, const double* __restrict__ r,
+                                                              double* __restrict__ z, const double* status) {
+    if (status[kDone] != 0) return;
+    extern __shared__ double zs[];
+    __shared__ double stages[32 * 32];  // per warp, the products of one row chunk
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    double* stage = stages + 32 * warp;
+    // forward: zs[i] = (r[i] - sum L_ij zs[j]) / D_i
+    ic_sweep(m.f_levels, m.f_level_offsets, m.f_table, m.l_columns, m.l_values, m.l_diagonal, r, zs, stage, lane,
+             warp, warps);
+    // backward: zs[c] = (zs[c] - sum over later rows i of L_ic zs[i]) / D_c
+    ic_sweep(m.b_levels, m.b_level_offsets, m.b_table, m.t_rows, m.t_values, m.l_diagonal, nullptr, zs, stage, lane,
+             warp, warps);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) z[i] = zs[i];
 }
 // rz of the start
 __global__ void ks_cg_take_rz(double* status) {
@@ -412,7 +522,7 @@ long check_offsets(const int32_t* off, long owners, const char* what) {
 
 class SimplicialStages {
 public:
-    SimplicialStages(const vapor_simplicial3d_mesh& m, int site_search, int dot_order) {
+    SimplicialStages(const vapor_simplicial3d_mesh& m, int site_search, int dot_order, int preconditioner) {
         validate(m);
         cudaStream_t s = st_.s;
         v_ = View{};
@@ -482,7 +592,7 @@ public:
         v_.loop_items = iptr(loop_items_);
         v_.dual_edges = iptr(dual_edges_);
         setup_operator(m);
-        setup_preconditioner(m);
+        setup_preconditioner(m, preconditioner == 1);
         dual_velocity_.allocate(3L * m.n_dual);
         samples_.allocate(3L * m.n_nodes);
         traced_.allocate(3L * m.n_dual);
@@ -708,7 +818,9 @@ private:
     // z = M^-1 r on the stream (skipped once the iteration is done).
     void precondition() {
         cudaStream_t s = st_.s;
-        if (pc_.ic)
+        if (pc_.ic && ic_shared_bytes_)
+            ks_ic_solve_shared<<<1, 1024, ic_shared_bytes_, s>>>(pc_, v_.n_edges, r_.p, z_.p, status_.p);
+        else if (pc_.ic)
             ks_ic_solve<<<1, 1024, 0, s>>>(pc_, r_.p, z_.p, status_.p);
         else
             ks_jacobi<<<cg_blocks_, kT, 0, s>>>(v_.n_edges, r_.p, pc_.jacobi, z_.p, status_.p);
@@ -716,7 +828,7 @@ private:
 
     // The CPU solver's preconditioner: its IC(0) factor, with the level sets
     // of both triangular solves, or its diagonal.
-    void setup_preconditioner(const vapor_simplicial3d_mesh& m) {
+    void setup_preconditioner(const vapor_simplicial3d_mesh& m, bool jacobi_only) {
         const int n = m.n_edges;
         cudaStream_t s = st_.s;
         pc_ = Precond{};
@@ -726,9 +838,10 @@ private:
             upload(jacobi_, m.jacobi_diagonal, n, s);
             pc_.jacobi = jacobi_.p;
         } else {
-            require_s(m.ic_offsets != nullptr, "the preconditioner needs the Jacobi diagonal or the IC factor");
+            require_s(m.ic_offsets != nullptr && !jacobi_only,
+                      "the preconditioner needs the Jacobi diagonal or the IC factor");
         }
-        if (!m.ic_offsets) return;
+        if (!m.ic_offsets || jacobi_only) return;
         const long nnz = check_offsets(m.ic_offsets, n, "IC factor offsets");
         require_s(m.ic_diagonal && (nnz == 0 || (m.ic_columns && m.ic_values)), "IC factor arrays");
         for (int i = 0; i < n; ++i) {
@@ -791,6 +904,15 @@ private:
         upload(t_values_, t_values.data(), t_values.size(), s);
         upload_i(b_level_offsets_, b_off.data(), b_off.size(), s);
         upload_i(b_columns_, b_cols.data(), b_cols.size(), s);
+        std::vector<int32_t> f_tab, b_tab;
+        for (int k = 0; k < n; ++k) {
+            const int i = f_rows[k];
+            f_tab.insert(f_tab.end(), {i, m.ic_offsets[i], m.ic_offsets[i + 1], 0});
+            const int c = b_cols[k];
+            b_tab.insert(b_tab.end(), {c, t_off[c], t_off[c + 1], 0});
+        }
+        upload_i(f_table_, f_tab.data(), f_tab.size(), s);
+        upload_i(b_table_, b_tab.data(), b_tab.size(), s);
         VB_CUDA(cudaStreamSynchronize(s));
         pc_.ic = 1;
         pc_.l_offsets = iptr(ic_offsets_);
@@ -806,6 +928,18 @@ private:
         pc_.b_level_offsets = iptr(b_level_offsets_);
         pc_.b_columns = iptr(b_columns_);
         pc_.b_levels = b_levels;
+        pc_.f_table = reinterpret_cast<const int4*>(f_table_.p);
+        pc_.b_table = reinterpret_cast<const int4*>(b_table_.p);
+        // the shared-memory form when the vector fits the block's shared memory
+        int device = 0, limit = 0;
+        VB_CUDA(cudaGetDevice(&device));
+        VB_CUDA(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        const size_t need = sizeof(double) * size_t(n);
+        ic_shared_bytes_ = 0;
+        if (need + sizeof(double) * 32 * 32 <= size_t(limit)) {
+            VB_CUDA(cudaFuncSetAttribute(ks_ic_solve_shared, cudaFuncAttributeMaxDynamicSharedMemorySize, int(need)));
+            ic_shared_bytes_ = need;
+        }
     }
 
     void put_velocity(const double* dual_velocity, const double* samples) {
@@ -850,9 +984,10 @@ private:
     std::vector<uint8_t> edge_boundary_;
     int cg_blocks_ = 1;
     Precond pc_{};
+    size_t ic_shared_bytes_ = 0;
     DevArray<double> jacobi_, ic_values_, ic_diagonal_, t_values_;
     DevArray<uint32_t> ic_offsets_, ic_columns_, f_level_offsets_, f_rows_, t_offsets_, t_rows_, b_level_offsets_,
-        b_columns_;
+        b_columns_, f_table_, b_table_;
 };
 
 }  // namespace vb
@@ -861,19 +996,21 @@ private:
 
 struct vapor_simplicial3d {
     vb::SimplicialStages stages;
-    vapor_simplicial3d(const vapor_simplicial3d_mesh& m, int search, int dots) : stages(m, search, dots) {}
+    vapor_simplicial3d(const vapor_simplicial3d_mesh& m, int search, int dots, int precond)
+        : stages(m, search, dots, precond) {}
 };
 
 #define VB_APIS extern "C" __attribute__((visibility("default")))
 
 VB_APIS vapor_status vapor_simplicial3d_create(const vapor_simplicial3d_mesh* mesh, int32_t site_search,
-                                               int32_t dot_order, vapor_simplicial3d** out) {
+                                               int32_t dot_order, int32_t preconditioner, vapor_simplicial3d** out) {
     return vb::guard([&] {
         if (!out || !mesh) vb::fail(VAPOR_INVALID_ARGUMENT, "null mesh or output");
         *out = nullptr;
         if (site_search < 0 || site_search > 2) vb::fail(VAPOR_INVALID_ARGUMENT, "site_search must be 0, 1 or 2");
         if (dot_order < 0 || dot_order > 2) vb::fail(VAPOR_INVALID_ARGUMENT, "dot_order must be 0, 1 or 2");
-        *out = new vapor_simplicial3d(*mesh, site_search, dot_order);
+        if (preconditioner < 0 || preconditioner > 1) vb::fail(VAPOR_INVALID_ARGUMENT, "preconditioner must be 0 or 1");
+        *out = new vapor_simplicial3d(*mesh, site_search, dot_order, preconditioner);
     });
 }
 VB_APIS vapor_status vapor_simplicial3d_destroy(vapor_simplicial3d* stages) {

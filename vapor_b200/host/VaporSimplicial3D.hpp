@@ -56,8 +56,10 @@ struct SimplicialPacked {
 class GpuSimplicial3D final : public SimplicialCompute3D {
 public:
     // site_search: 0 automatic, 1 scan of all sites, 2 descent; dot_order: 0
-    // automatic, 1 index order, 2 tree (vapor_simplicial3d_create).
-    explicit GpuSimplicial3D(int site_search = 0, int dot_order = 0) : search_(site_search), dots_(dot_order) {}
+    // automatic, 1 index order, 2 tree; preconditioner: 0 the CPU solver's,
+    // 1 Jacobi (vapor_simplicial3d_create).
+    explicit GpuSimplicial3D(int site_search = 0, int dot_order = 0, int preconditioner = 0)
+        : search_(site_search), dots_(dot_order), precond_(preconditioner) {}
     ~GpuSimplicial3D() override { release(); }
     GpuSimplicial3D(const GpuSimplicial3D&) = delete;
     GpuSimplicial3D& operator=(const GpuSimplicial3D&) = delete;
@@ -67,7 +69,7 @@ public:
         if (stages_ && key_ == mesh.tets.data() && size_ == mesh.size) return;
         release();
         packSolver(solver, packed_);
-        vapor_b200::check(vapor_simplicial3d_create(&packed_.mesh, search_, dots_, &stages_));
+        vapor_b200::check(vapor_simplicial3d_create(&packed_.mesh, search_, dots_, precond_, &stages_));
         key_ = mesh.tets.data();
         size_ = mesh.size;
     }
@@ -308,6 +310,7 @@ private:
 
     int search_ = 0;
     int dots_ = 0;
+    int precond_ = 0;
     vapor_simplicial3d* stages_ = nullptr;
     const void* key_ = nullptr;
     double size_ = 0;
