@@ -109,6 +109,18 @@ public:
         if (s.n != resolution() || s.box != boxSize()) throw std::invalid_argument("GPU snapshot box mismatch");
         check(vapor_mac3d_download(handle_, s.density.data(), s.u.data(), s.v.data(), s.w.data()));
     }
+    // Streamed transfers (vapor_mac3d_upload_async / _download_async): the
+    // snapshot must stay alive and unchanged, and a downloaded one unread,
+    // until waitTransfers() returns.
+    void uploadAsync(const HostState& s) {
+        if (s.n != resolution() || s.box != boxSize()) throw std::invalid_argument("GPU snapshot box mismatch");
+        check(vapor_mac3d_upload_async(handle_, s.density.data(), s.u.data(), s.v.data(), s.w.data()));
+    }
+    void downloadAsync(HostState& s) {
+        if (s.n != resolution() || s.box != boxSize()) throw std::invalid_argument("GPU snapshot box mismatch");
+        check(vapor_mac3d_download_async(handle_, s.density.data(), s.u.data(), s.v.data(), s.w.data()));
+    }
+    void waitTransfers() { check(vapor_mac3d_wait_transfers(handle_)); }
     std::uint64_t uploadedBytes() const {
         uint64_t up, down;
         check(vapor_mac3d_byte_counters(handle_, &up, &down));
