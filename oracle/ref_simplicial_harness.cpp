@@ -354,3 +354,19 @@ HX int rs_ic_levels(void* h) {
     }
     return levels;
 }
+// The rotating stir force and the emitter position/strength/radius.
+HX void rs_set_stir(void* h, float strength, float radius, float frequency) {
+    auto& p = S(h).solver->parameters();
+    p.stirStrength = strength;
+    p.stirRadius = radius;
+    p.stirFrequency = frequency;
+}
+HX void rs_set_emitter(void* h, float x, float y, float z, float strength, float radius, float buoyancy) {
+    auto& p = S(h).solver->parameters();
+    p.emitterX = x;
+    p.emitterY = y;
+    p.emitterZ = z;
+    p.sourceStrength = strength;
+    p.emitterRadius = radius;
+    p.buoyancy = buoyancy;
+}

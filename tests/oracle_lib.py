@@ -563,6 +563,8 @@ def _simplicial_lib():
         f("rs_last_recovery", None, _vp, _vp, _vp, _vp, _vp)
         f("rs_smoke_center", None, _vp, _vp)
         f("rs_substeps", C.c_int, _vp)
+        f("rs_set_stir", None, _vp, C.c_float, C.c_float, C.c_float)
+        f("rs_set_emitter", None, _vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float)
         _simplicial = lib
     return _simplicial
 
@@ -600,6 +602,12 @@ class RefSimplicial:
 
     def set_parameters(self, emitter=True, decay=0.08, cg_iterations=600, abs_tol=1e-10, rel_tol=1e-9):
         self.lib.rs_set_parameters(self.h, 1 if emitter else 0, decay, cg_iterations, abs_tol, rel_tol)
+
+    def set_stir(self, strength, radius=.18, frequency=1.0):
+        self.lib.rs_set_stir(self.h, strength, radius, frequency)
+
+    def set_emitter(self, x, y, z, strength=4.0, radius=.12, buoyancy=3.0):
+        self.lib.rs_set_emitter(self.h, x, y, z, strength, radius, buoyancy)
 
     def set_potential(self, phi):
         phi = np.ascontiguousarray(phi, np.float64)
