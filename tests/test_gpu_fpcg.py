@@ -1,6 +1,6 @@
-"""Flexible PCG solver (VAPOR_SOLVER_FPCG): the plain FP64 residual test is the
-judge, so its projections are compared with the oracle's mixed-precision SOR
-solve at a matched relative residual."""
+"""Flexible PCG solver (VAPOR_SOLVER_FPCG): the plain FP64 residual test
+decides convergence, so its projections are compared with the oracle's
+mixed-precision SOR solve at a matched relative residual."""
 import numpy as np
 import pytest
 
